@@ -1,0 +1,439 @@
+#!/usr/bin/env python
+"""Benchmark of the Parareal T2S4 CC-CFV solver on B200.
+
+Workload (default): periodic unit square, solid-body rotation
+u = -2 pi (y - 1/2), v = 2 pi (x - 1/2), nu = 1e-3, Gaussian hump sigma 0.05
+at (0.5, 0.75), T = 1 (one revolution), N^2 = 2048^2 cells, fine dt at
+CFL ~0.8 (Nt = 4N), 64 time slices, coarse dt = 8 x fine, Parareal iterated
+to a relative update < 1e-10 (or the iteration cap).  One benchmark step is
+one full Parareal solve; the metric is the effective rate N^2 * Nt / time
+(cell-updates/s of the serial fine solve that Parareal replaces).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one rank per GPU): every rank solves its own instance
+(instances are independent: weak scaling, no collective on the data path);
+the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "parareal-cc-cfv-split-gpu_b200"
+sys.path.insert(0, str(PKG))
+
+BYTES_PER_FINE_CELL_SWEEP = 16  # FP64: 8 B read + 8 B written per cell per sweep
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-device", default="cpu", choices=["cpu", "gpu"],
+                    help="reference arm: the oracle port on the host cores (cpu) or the "
+                         "reference binary's own GPU step (gpu)")
+    ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--slices", type=int, default=64)
+    ap.add_argument("--ratio", type=int, default=8)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--kmax", type=int, default=24)
+    ap.add_argument("--coarse", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--form", default="delta", choices=["standard", "delta"])
+    ap.add_argument("--cpu-sample-s", type=float, default=8.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(a):
+    N = a.n
+    nt = 4 * N
+    return dict(N=N, T=1.0, nt=nt, slices=a.slices, ratio=a.ratio, tol=a.tol, kmax=a.kmax,
+                nu=1e-3, omega=2 * np.pi, center=(0.5, 0.5), hump=(0.5, 0.75), sigma=0.05)
+
+
+def workload_name(w, a):
+    return (f"periodic unit square {w['N']}^2, solid-body rotation (one revolution, T=1), "
+            f"nu={w['nu']}, Gaussian sigma={w['sigma']} at {w['hump']}, Nt={w['nt']} fine steps, "
+            f"{w['slices']} slices, coarse dt = {w['ratio']} x fine ({a.coarse} coarse, {a.form} "
+            f"form), Parareal to relative update < {w['tol']:g} (cap {w['kmax']})")
+
+
+def initial_field(w, device):
+    """Cell averages (3x3 Simpson, as T2S4_Parareal.cu:118-140) of the
+    Gaussian hump with its periodic images; synthetic input data."""
+    import torch
+    N = w["N"]
+    h = 1.0 / N
+    den = 2.0 * w["sigma"] ** 2
+    x = (torch.arange(N, dtype=torch.float64, device=device) + 0.5) * h
+    X, Y = torch.meshgrid(x, x, indexing="ij")
+    acc = torch.zeros_like(X)
+    wts = {-1: 1.0, 0: 4.0, 1: 1.0}
+    for dxs in (-1, 0, 1):
+        for dys in (-1, 0, 1):
+            wgt = wts[dxs] * wts[dys]
+            px, py = X + 0.5 * h * dxs, Y + 0.5 * h * dys
+            for ix in (-1, 0, 1):
+                for iy in (-1, 0, 1):
+                    acc += wgt * torch.exp(-((px - w["hump"][0] + ix) ** 2 +
+                                             (py - w["hump"][1] + iy) ** 2) / den)
+    return (acc / 36.0).contiguous()
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.lines: list[str] = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons, pw = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [v.strip() for v in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+                pw.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(mx),
+                "power_w_max": max(pw) if pw else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def dist_setup(a):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl"
+        try:
+            import torch
+            if not torch.cuda.is_available():
+                backend = "gloo"
+        except Exception:
+            backend = "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def reduce_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(N):
+    """Per-launch DRAM traffic of the fine sweep from a committed ncu summary
+    (profiles/sweep_traffic.json), scaled to this workload's cells."""
+    p = ROOT / "profiles" / "sweep_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return float(d["bytes_per_cell_sweep"])
+    except Exception:
+        return None
+
+
+def cpu_baseline(w, sample_s):
+    """The oracle (CPU restatement of the reference step) on all host cores:
+    serial fine steps of the same workload, bounded to ~sample_s seconds."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    cores = O.cpu_count()
+    N = w["N"]
+    g = O.grid(N, bc=O.BC_PERIODIC, vel=O.VEL_ROTATION, vp=(w["omega"], 0.5, 0.5), K=w["nu"],
+               threads=cores, scheme=O.SCHEME_CONSISTENT)
+    den = 2 * w["sigma"] ** 2
+    x = (np.arange(N) + 0.5) / N
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    C = np.exp(-((X - w["hump"][0]) ** 2 + (Y - w["hump"][1]) ** 2) / den)
+    dt = w["T"] / w["nt"]
+    t0 = time.perf_counter()
+    C = O.run(g, C, 0.0, dt, 1)
+    t1 = time.perf_counter() - t0
+    n = max(1, min(200, int(sample_s / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    O.run(g, C, dt, dt, n)
+    el = time.perf_counter() - t0
+    return {"value": N * N * n / el, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+            "sample": f"{n} serial fine steps of the {N}^2 workload (oracle, OpenMP over lines)"}
+
+
+def run_reference(a, w, ws, rank):
+    """Reference arm: the reference path's serial fine time-stepping, on the
+    host cores (oracle port: the reference has no CPU implementation of its
+    own) or, with --ref-device gpu, the reference binary's GpuOneStep on the
+    GPU (oracle/_ref).  Rank 0 only."""
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    N = w["N"]
+    dt = w["T"] / w["nt"]
+    if a.ref_device == "gpu":
+        if not O.ref_available():
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "reference binary not built (make -C oracle ref)"}))
+            return
+        x = -1.0 + (np.arange(N) + 0.5) * (2.0 / N)
+        X, Y = np.meshgrid(x, x, indexing="ij")
+        C0 = np.exp(-((X + 0.35) ** 2 + Y ** 2) / 0.005)
+        nst = max(2, int(2e8 / (N * N)))
+        vals = []
+        for i in range(a.warmup + a.steps):
+            _, ms = O.ref_time_run(N, w["nu"], 0.0, dt, nst, C0)
+            if i >= a.warmup:
+                vals.append(N * N * nst / (ms * 1e-3))
+        v = statistics.median(vals)
+        line = dict(metric="parareal_cell_updates_per_s", value=v, unit="cell-updates/s",
+                    impl="reference", n_gpus=1, steps=a.steps, warmup=a.warmup,
+                    ms_per_step=N * N * nst / v * 1e3, higher_is_better=True, scaling="weak",
+                    vs_baseline=None, dtype="f64", data="synthetic",
+                    config={"workload": f"reference binary GpuOneStep, {N}^2, {nst} serial fine "
+                                        "steps per sample (reference domain and velocity)"},
+                    cpu_baseline=None,
+                    e2e={"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0})
+        print(json.dumps(line))
+        return
+    cores = O.cpu_count()
+    g = O.grid(N, bc=O.BC_PERIODIC, vel=O.VEL_ROTATION, vp=(w["omega"], 0.5, 0.5), K=w["nu"],
+               threads=cores, scheme=O.SCHEME_CONSISTENT)
+    den = 2 * w["sigma"] ** 2
+    x = (np.arange(N) + 0.5) / N
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    C = np.exp(-((X - w["hump"][0]) ** 2 + (Y - w["hump"][1]) ** 2) / den)
+    t0 = time.perf_counter()
+    O.run(g, C, 0.0, dt, 1)
+    t1 = time.perf_counter() - t0
+    nst = max(1, int(min(a.cpu_sample_s, 20.0) / max(t1, 1e-6)))
+    vals = []
+    for i in range(a.warmup + a.steps):
+        t0 = time.perf_counter()
+        C = O.run(g, C, 0.0, dt, nst)
+        el = time.perf_counter() - t0
+        if i >= a.warmup:
+            vals.append(N * N * nst / el)
+    v = statistics.median(vals)
+    sample = f"{nst} serial fine steps of the {N}^2 workload per step (oracle port, OpenMP)"
+    line = dict(metric="parareal_cell_updates_per_s", value=v, unit="cell-updates/s",
+                impl="reference", n_gpus=ws, steps=a.steps, warmup=a.warmup,
+                ms_per_step=N * N * nst / v * 1e3, higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="f64", data="synthetic",
+                config={"workload": workload_name(w, a) + "; reference arm: serial fine "
+                                                          "time-stepping on the host cores"},
+                cpu_baseline={"value": v, "unit": "cell-updates/s", "cores": cores,
+                              "kind": "port", "sample": sample},
+                e2e={"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                     "d2h_bytes_per_step": 0})
+    print(json.dumps(line))
+
+
+def run_ours(a, w, ws, rank, local):
+    import torch
+    import ccfv
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    N, nt = w["N"], w["nt"]
+    grid = ccfv.make_grid(N, bc=ccfv.BC_PERIODIC, velocity=ccfv.VEL_ROTATION,
+                          vel_params=(w["omega"], *w["center"]), K=w["nu"],
+                          scheme=ccfv.SCHEME_CONSISTENT)
+    solver = ccfv.Solver(grid, local)
+    C0 = initial_field(w, dev)
+    out = torch.empty_like(C0)
+    prec = ccfv.FP32 if a.coarse == "fp32" else ccfv.FP64
+    form = ccfv.FORM_DELTA if a.form == "delta" else ccfv.FORM_STANDARD
+    kw = dict(t0=0.0, t1=w["T"], nt_fine=nt, n_slices=w["slices"], coarse_ratio=w["ratio"],
+              tol=w["tol"], kmax=w["kmax"], coarse_precision=prec, form=form)
+    stream = torch.cuda.current_stream()
+
+    for _ in range(a.warmup):
+        solver.parareal(C0, out, **kw)
+    torch.cuda.synchronize()
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = ccfv.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    ev0.record(stream)
+    for _ in range(a.steps):
+        _, st = solver.parareal(C0, out, **kw)
+        stats.append(st)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = ccfv.kernel_launches() - l0
+    ck = clocks.stop()
+    barrier(ws)
+    ms = ev0.elapsed_time(ev1)
+    ms_max = reduce_max(ms, ws)
+    value = ws * (N * N * nt) * a.steps / (ms_max * 1e-3)
+
+    # e2e: the same solve through the C ABI with pinned host buffers (H2D of
+    # the initial field and D2H of the result inside every timed step)
+    h_in = torch.empty(N, N, dtype=torch.float64, pin_memory=True)
+    h_in.copy_(C0.cpu())
+    h_out = torch.empty(N, N, dtype=torch.float64, pin_memory=True)
+    hin_np, hout_np = h_in.numpy(), h_out.numpy()
+    solver.parareal(hin_np, hout_np, **kw)
+    torch.cuda.synchronize()
+    barrier(ws)
+    e0 = time.perf_counter()
+    for _ in range(a.steps):
+        solver.parareal(hin_np, hout_np, **kw)
+    torch.cuda.synchronize()
+    e_s = reduce_max(time.perf_counter() - e0, ws)
+    e2e_value = ws * (N * N * nt) * a.steps / e_s
+
+    # live roofline of the dominant kernel (the fine sweep) from the F-phase
+    # device time of the timed solves
+    f_ms = sum(s["fine_ms"] for s in stats)
+    f_launch = sum(s["fine_sweep_launches"] for s in stats)
+    f_cells = sum(s["fine_sweep_cells"] for s in stats)
+    peak, peak_kind = measured_peak()
+    achieved = f_cells * BYTES_PER_FINE_CELL_SWEEP / (f_ms * 1e-3) / 1e9 if f_ms > 0 else None
+    tpc = ncu_traffic(N)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None,
+            "traffic": (tpc * f_cells / f_launch) if (tpc and f_launch) else None,
+            "kernel": "sweep_kernel<double> (fused x/y sweep, F phase)",
+            "bytes_per_launch": f_cells * BYTES_PER_FINE_CELL_SWEEP / max(f_launch, 1),
+            "avg_launch_us": f_ms * 1e3 / max(f_launch, 1), "peak_source": peak_kind}
+
+    # accuracy of the benchmarked solve against the serial fine solve (untimed)
+    err = None
+    plain = None
+    if rank == 0:
+        fine = C0.clone()
+        e_a, e_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_a.record(stream)
+        solver.run(fine, 0.0, w["T"] / nt, nt)
+        e_b.record(stream)
+        torch.cuda.synchronize()
+        plain = N * N * nt / (e_a.elapsed_time(e_b) * 1e-3)
+        err = float(torch.linalg.norm(out - fine) / torch.linalg.norm(fine))
+
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(w, a.cpu_sample_s)
+
+    if rank == 0:
+        st = stats[-1]
+        line = dict(
+            metric="parareal_cell_updates_per_s", value=value, unit="cell-updates/s",
+            n_gpus=ws, steps=a.steps, warmup=a.warmup, ms_per_step=ms_max / a.steps,
+            higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
+            data="synthetic",
+            config={"workload": workload_name(w, a), "N": N, "nt_fine": nt,
+                    "n_slices": w["slices"], "coarse_ratio": w["ratio"],
+                    "coarse_precision": a.coarse, "form": a.form,
+                    "l2_flush": "working set (slice states) > L2: "
+                                f"{(2 * w['slices'] + 2) * N * N * 8 / 1e9:.1f} GB",
+                    "parallelism": f"{ws} independent instance(s), one per GPU"},
+            iterations=st["iterations"], converged=st["converged"],
+            final_update=st["update"][-1] if st["update"] else None,
+            l2_err_vs_serial_fine=err,
+            executed_cell_updates_per_s=ws * (st["fine_cell_updates"] +
+                                              st["coarse_cell_updates"]) * a.steps /
+            (ms_max * 1e-3),
+            plain_serial_fine_cell_updates_per_s=plain,
+            e2e={"value": e2e_value, "unit": "cell-updates/s",
+                 "h2d_bytes_per_step": 8 * N * N, "d2h_bytes_per_step": 8 * N * N},
+            roofline=roof, cpu_baseline=cpu, clocks=ck, gpu_launches=launches)
+        print(json.dumps(line))
+
+
+def main():
+    a = parse()
+    w = workload(a)
+    ws, rank, local = dist_setup(a)
+    try:
+        if a.impl == "reference":
+            run_reference(a, w, ws, rank)
+        else:
+            run_ours(a, w, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -60,6 +60,17 @@ enum ccfv_velocity {
                             v = -sin^2(pi y) sin(2 pi x) cos(pi t / p0)     */
 };
 
+/* Which field the third sweep differentiates at the characteristic feet. */
+enum ccfv_scheme {
+  CCFV_SCHEME_REFERENCE = 0,  /* the remapped field, as the reference does
+                                 (dcdx_bar_on_gpu(v_d_Cnphf_bar_x, ...),
+                                 T2S4_Parareal.cu:929-932): bit-compatible
+                                 with the reference, first order in time    */
+  CCFV_SCHEME_CONSISTENT = 1  /* the sweep input, like the first two sweeps
+                                 (T2S4:834-837, 882-885): 4th order in space,
+                                 2nd order in time                          */
+};
+
 enum ccfv_precision { CCFV_FP64 = 0, CCFV_FP32 = 1 };
 enum ccfv_mem { CCFV_MEM_DEVICE = 0, CCFV_MEM_HOST = 1 };
 enum ccfv_form {
@@ -77,6 +88,7 @@ typedef struct ccfv_grid {
   int velocity;                /* enum ccfv_velocity                       */
   double vel_params[4];        /* see enum ccfv_velocity                   */
   double K;                    /* diffusivity (reference config key "K")   */
+  int scheme;                  /* enum ccfv_scheme (0 = reference)         */
 } ccfv_grid;
 
 typedef struct ccfv_ctx ccfv_ctx;
@@ -136,6 +148,10 @@ typedef struct ccfv_stats {
   double fine_cell_updates;              /* executed fine cell-updates     */
   double coarse_cell_updates;            /* executed coarse cell-updates   */
   double ms;                             /* device time of the solve       */
+  double fine_ms;                        /* device time of the F phases    */
+  double coarse_ms;                      /* device time of the G phases    */
+  long long fine_sweep_launches;         /* sweep launches in the F phases */
+  long long fine_sweep_cells;            /* cells swept in the F phases    */
 } ccfv_stats;
 
 /* Parareal solve of C0 over [t0,t1]; the final state goes to C_T.
@@ -149,6 +165,9 @@ int ccfv_parareal(ccfv_ctx *ctx, const ccfv_parareal_opts *opts, const double *C
 /* ---- library info ---------------------------------------------------- */
 /* Number of kernels this library launched since load (all contexts). */
 uint64_t ccfv_kernel_launches(void);
+
+/* Text of the last error recorded on `ctx` ("" if none). */
+const char *ccfv_last_error(ccfv_ctx *ctx);
 
 #ifdef __cplusplus
 }

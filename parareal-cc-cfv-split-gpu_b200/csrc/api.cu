@@ -1,0 +1,170 @@
+// api.cu -- the extern "C" boundary of libccfv (declared in include/ccfv.h).
+#include <cstring>
+#include <new>
+
+#include "engine.h"
+
+using namespace ccfv;
+
+namespace {
+
+bool grid_ok(const ccfv_grid *g) {
+  if (!g) return false;
+  if (g->nx < 4 || g->ny < 4) return false;
+  if (!(g->x_max > g->x_min) || !(g->y_max > g->y_min)) return false;
+  if (g->bc != CCFV_BC_COMPAT && g->bc != CCFV_BC_PERIODIC) return false;
+  if (g->velocity < CCFV_VEL_REF_ROT4 || g->velocity > CCFV_VEL_SWIRL) return false;
+  if (g->velocity == CCFV_VEL_SWIRL && g->vel_params[0] == 0.0) return false;
+  if (g->scheme != CCFV_SCHEME_REFERENCE && g->scheme != CCFV_SCHEME_CONSISTENT) return false;
+  if (!(g->K >= 0.0)) return false;
+  return true;
+}
+
+int use_device(ccfv_ctx *ctx) {
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return set_error(ctx, CCFV_ERR_CUDA, cudaGetErrorString(e));
+  return CCFV_OK;
+}
+
+int last_launch(ccfv_ctx *ctx) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(ctx, CCFV_ERR_CUDA, cudaGetErrorString(e));
+  return CCFV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *ccfv_strerror(int status) {
+  switch (status) {
+    case CCFV_OK: return "ok";
+    case CCFV_ERR_INVALID: return "invalid argument";
+    case CCFV_ERR_CUDA: return "CUDA error";
+    case CCFV_ERR_NOMEM: return "out of device memory";
+    case CCFV_ERR_UNSUPPORTED: return "unsupported configuration";
+    case CCFV_ERR_HALO: return "characteristic foot outside the staged halo";
+    case CCFV_ERR_BUDGET: return "request exceeds the HBM budget";
+    case CCFV_ERR_NOT_FOUND: return "unknown ticket";
+    case CCFV_ERR_CANCELLED: return "cancelled";
+    case CCFV_ERR_TIMEOUT: return "timed out";
+  }
+  return "unknown status";
+}
+
+int ccfv_create(ccfv_ctx **out, const ccfv_grid *grid, int device) {
+  if (!out) return CCFV_ERR_INVALID;
+  *out = nullptr;
+  if (!grid_ok(grid)) return CCFV_ERR_INVALID;
+  ccfv_ctx *ctx = new (std::nothrow) ccfv_ctx();
+  if (!ctx) return CCFV_ERR_NOMEM;
+  ctx->grid = *grid;
+  ctx->device = device;
+  int rc = use_device(ctx);
+  if (rc) { delete ctx; return rc; }
+  if (ctx->status.alloc(sizeof(unsigned) * 4) != cudaSuccess ||
+      ctx->partial.alloc(sizeof(double) * 2 * RED_BLOCKS_MAX) != cudaSuccess ||
+      ctx->counter.alloc(sizeof(unsigned) * 4) != cudaSuccess) {
+    delete ctx;
+    return CCFV_ERR_NOMEM;
+  }
+  if (cudaMemset(ctx->status.p, 0, sizeof(unsigned) * 4) != cudaSuccess ||
+      cudaMemset(ctx->counter.p, 0, sizeof(unsigned) * 4) != cudaSuccess) {
+    delete ctx;
+    return CCFV_ERR_CUDA;
+  }
+  *out = ctx;
+  return CCFV_OK;
+}
+
+int ccfv_destroy(ccfv_ctx *ctx) {
+  if (!ctx) return CCFV_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaDeviceSynchronize();
+  delete ctx;
+  return CCFV_OK;
+}
+
+int ccfv_check(ccfv_ctx *ctx, void *stream) {
+  if (!ctx) return CCFV_ERR_INVALID;
+  int rc = use_device(ctx);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned flag = 0;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaMemcpy(&flag, ctx->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_error(ctx, CCFV_ERR_CUDA, cudaGetErrorString(e));
+  if (flag) {
+    cudaMemset(ctx->status.p, 0, sizeof(unsigned));
+    return set_error(ctx, CCFV_ERR_HALO, "a characteristic foot left the staged halo");
+  }
+  return CCFV_OK;
+}
+
+int ccfv_step(ccfv_ctx *ctx, double *d_C, double tn, double dt, void *stream) {
+  if (!ctx || !d_C) return CCFV_ERR_INVALID;
+  int rc = use_device(ctx);
+  if (rc) return rc;
+  rc = steps(ctx, d_C, true, tn, dt, 1, (cudaStream_t)stream);
+  return rc ? rc : last_launch(ctx);
+}
+
+int ccfv_fine(ccfv_ctx *ctx, double *d_C, double tn, double DT, int J, void *stream) {
+  if (!ctx || !d_C || J < 1) return CCFV_ERR_INVALID;
+  int rc = use_device(ctx);
+  if (rc) return rc;
+  // FinePropagator: dt = DT / J, t_local = tn + j * dt (T2S4:979-982)
+  rc = steps(ctx, d_C, true, tn, DT / (double)J, J, (cudaStream_t)stream);
+  return rc ? rc : last_launch(ctx);
+}
+
+int ccfv_coarse(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, int precision,
+                void *stream) {
+  if (!ctx || !d_C || m < 1) return CCFV_ERR_INVALID;
+  if (precision != CCFV_FP64 && precision != CCFV_FP32) return CCFV_ERR_INVALID;
+  int rc = use_device(ctx);
+  if (rc) return rc;
+  if (precision == CCFV_FP64)
+    rc = steps(ctx, d_C, true, tn, DT / (double)m, m, (cudaStream_t)stream);
+  else
+    rc = coarse_fp32(ctx, d_C, tn, DT, m, (cudaStream_t)stream);
+  return rc ? rc : last_launch(ctx);
+}
+
+int ccfv_run(ccfv_ctx *ctx, double *C, int mem, double t0, double dt, int nsteps, void *stream) {
+  if (!ctx || !C || nsteps < 0) return CCFV_ERR_INVALID;
+  if (mem != CCFV_MEM_DEVICE && mem != CCFV_MEM_HOST) return CCFV_ERR_INVALID;
+  int rc = use_device(ctx);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t bytes = sizeof(double) * (size_t)ctx->grid.nx * ctx->grid.ny;
+  double *d = C;
+  if (mem == CCFV_MEM_HOST) {
+    if (ctx->io.alloc(bytes) != cudaSuccess) return set_error(ctx, CCFV_ERR_NOMEM, "io buffer");
+    d = ctx->io.as<double>();
+    cudaError_t e = cudaMemcpyAsync(d, C, bytes, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return set_error(ctx, CCFV_ERR_CUDA, cudaGetErrorString(e));
+  }
+  rc = steps(ctx, d, true, t0, dt, nsteps, st);
+  if (rc) return rc;
+  if (mem == CCFV_MEM_HOST) {
+    cudaError_t e = cudaMemcpyAsync(C, d, bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return set_error(ctx, CCFV_ERR_CUDA, cudaGetErrorString(e));
+  }
+  return last_launch(ctx);
+}
+
+int ccfv_parareal(ccfv_ctx *ctx, const ccfv_parareal_opts *opts, const double *C0, double *C_T,
+                  ccfv_stats *stats, void *stream) {
+  if (!ctx) return CCFV_ERR_INVALID;
+  int rc = use_device(ctx);
+  if (rc) return rc;
+  return parareal(ctx, opts, C0, C_T, stats, (cudaStream_t)stream);
+}
+
+uint64_t ccfv_kernel_launches(void) { return launches(); }
+
+const char *ccfv_last_error(ccfv_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+}  // extern "C"

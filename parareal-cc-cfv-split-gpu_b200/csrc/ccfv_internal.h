@@ -1,0 +1,80 @@
+// ccfv_internal.h -- device-side data structures and launchers shared by the
+// translation units of libccfv (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace ccfv {
+
+enum { BC_COMPAT = 0, BC_PERIODIC = 1 };
+enum { VEL_REF_ROT4 = 0, VEL_CONST = 1, VEL_ROTATION = 2, VEL_SWIRL = 3 };
+
+// Device status word bits (set by kernels, read by ccfv_check).
+enum : unsigned { STATUS_HALO = 1u };
+
+// Tile geometry of the fused sweep kernel.  A CTA owns LPG lines and a run
+// of consecutive cells (positions) of those lines; a thread-block cluster of
+// `cs` CTAs covers whole lines.  Lines sit in the fast (lane) index of the
+// shared-memory tile, positions in the slow index, so every phase of the
+// kernel reads shared memory without bank conflicts in both directions.
+constexpr int LPG = 16;          // lines per tile (x-sweeps: 128 B rows)
+constexpr int PITCH = LPG + 1;   // odd pitch: conflict-free column access
+constexpr int NW = 8;            // warps per CTA
+constexpr int NTH = NW * 32;     // threads per CTA
+constexpr int CPW = 32 / LPG;    // chunks per warp
+constexpr int NCH = NW * CPW;    // chunks per line per CTA
+constexpr int LC_MAX = 256;      // max positions per CTA
+constexpr int MAX_CLUSTER = 16;  // non-portable cluster size (lines <= 4096)
+
+// One field (one instance at one time slice) in one sweep launch.
+// x-sweep: lines are columns j (s_line = 1, s_pos = ny), positions i.
+// y-sweep: lines are rows i (s_line = ny, s_pos = 1), positions j.
+struct SweepField {
+  void *data;            // T[ny*nx], swept in place
+  long long s_pos;       // element stride between positions of a line
+  long long s_line;      // element stride between lines
+  int L;                 // cells per line
+  int M;                 // lines
+  int dir;               // 0: x-sweep, 1: y-sweep
+  int bc;                // BC_*
+  int vel;               // VEL_*
+  int group0;            // first tile index of this field in the launch
+  int groups;            // tiles of this field = ceil(M / LPG)
+  int dsrc;              // foot derivative of: 0 the sweep input, 1 the remapped field
+  int hd;                // dsrc = 1: halo (cells) of the remapped field
+  int uniform;           // 1: the velocity along the sweep depends only on the
+                         // transverse coordinate (every foot of a line has the
+                         // same displacement): stencil fast path
+  int pad1;
+  double vp[4];          // velocity parameters
+  double s_min, s_max, h;  // along-line edge coordinates: s_min + h*e
+  double t_min, ht;        // transverse edges: t_min + ht*line
+  double Dt;               // sub-step length
+  double ta_rel, tb_rel;   // foot-tracing interval relative to the launch time
+  double eps_remap;        // compat remap clamp (x: 1e-15, y: 1e-16)
+  double kb;               // 0.5*K*(Dt/h): RHS diffusion coefficient
+  double inv12h;           // 1/(12 h)
+  double sm_fac;           // periodic: a / gamma
+  double sm_inv_den;       // periodic: 1 / (1 + z0 + (a/gamma) z_{L-1})
+  const void *tab;         // T[3L]: alpha_k | g_k | z_k (solver factors)
+};
+
+// Shared-memory bytes of the sweep kernel for a launch.
+size_t sweep_smem_bytes(int lc_max, int halo, bool fp64);
+
+// Launches one fused sweep over all fields of `d_fields` (device array,
+// sorted by group0; tiles group_base .. group_base+groups_total-1).  All fields share the cluster size `cs`, their
+// max positions per CTA `lc_max` and the halo `halo`.  `toff` is added to
+// every field's ta_rel/tb_rel (the launch time); `data` (if non-null)
+// replaces fields[0].data (single-field launches).
+template <typename T>
+cudaError_t launch_sweep(const SweepField *d_fields, int nfields, int group_base,
+                         int groups_total, int cs, int lc_max, int halo, double toff, void *data,
+                         unsigned *d_status, cudaStream_t stream);
+
+// Counts kernel launches made by the library.
+void count_launch(uint64_t n = 1);
+uint64_t launches();
+
+}  // namespace ccfv

@@ -1,0 +1,587 @@
+// engine.cu -- solver context, line-invariant tridiagonal factors, step plans,
+// propagators and the Parareal engine of libccfv.
+#include "engine.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+
+namespace ccfv {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launch(uint64_t n) { g_launches += n; }
+uint64_t launches() { return g_launches.load(); }
+
+cudaError_t DevBuf::alloc(size_t b) {
+  if (p && bytes >= b) return cudaSuccess;
+  if (p) {
+    cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  if (b == 0) return cudaSuccess;
+  cudaError_t e = cudaMalloc(&p, b);
+  if (e == cudaSuccess) bytes = b;
+  else p = nullptr;
+  return e;
+}
+
+int set_error(ccfv_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->last_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return set_error(ctx, e_ == cudaErrorMemoryAllocation ? CCFV_ERR_NOMEM : CCFV_ERR_CUDA, \
+                       std::string(#call) + ": " + cudaGetErrorString(e_));            \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Line-invariant factors of the constant tridiagonal system
+//   a x_{k-1} + b x_k + a x_{k+1} = r_k,  a = 1/12 - 0.5 K Dt/h^2,
+//   b = 10/12 + K Dt/h^2  (x_A_LHS_on_gpu / y_A_LHS_on_gpu, T2S4:550-594).
+// LU in the reference's Thomas order (x_Thomas_on_gpu, T2S4:666-676):
+//   g_k = 1/(b_k - p_{k-1} a), p_k = a g_k, alpha_k = -a g_k,
+// so that forward q_k = g_k r_k + alpha_k q_{k-1} and backward
+// x_k = q_k + alpha_k x_{k+1}.  Periodic: Sherman-Morrison with gamma = -b,
+// b_0 -> b - gamma, b_{L-1} -> b - a^2/gamma, z = A'^{-1} (gamma,0..0,a).
+template <typename T>
+static void build_table(int L, double coA, double coB, int bc, std::vector<T> &out,
+                        double &sm_fac, double &sm_inv_den) {
+  const double coC = coA, gam = -coB;
+  std::vector<double> diag(L, coB), g(L), p(L), z(L, 0.0);
+  if (bc == BC_PERIODIC) {
+    diag[0] = coB - gam;
+    diag[L - 1] = coB - coA * coC / gam;
+  }
+  g[0] = 1.0 / diag[0];
+  p[0] = coC / diag[0];
+  for (int k = 1; k < L; ++k) {
+    g[k] = 1.0 / (diag[k] - p[k - 1] * coA);
+    p[k] = coC * g[k];
+  }
+  out.assign(3 * (size_t)L, T(0));
+  for (int k = 0; k < L; ++k) {
+    out[k] = T(-coA * g[k]);
+    out[L + k] = T(g[k]);
+  }
+  sm_fac = 0.0;
+  sm_inv_den = 0.0;
+  if (bc == BC_PERIODIC) {
+    std::vector<double> q(L);
+    for (int k = 0; k < L; ++k) {
+      double u = (k == 0) ? gam : (k == L - 1 ? coC : 0.0);
+      q[k] = g[k] * u + (k ? (-coA * g[k]) * q[k - 1] : 0.0);
+    }
+    z[L - 1] = q[L - 1];
+    for (int k = L - 2; k >= 0; --k) z[k] = q[k] - p[k] * z[k + 1];
+    for (int k = 0; k < L; ++k) out[2 * (size_t)L + k] = T(z[k]);
+    sm_fac = coA / gam;
+    sm_inv_den = 1.0 / (1.0 + z[0] + sm_fac * z[L - 1]);
+  }
+}
+
+static double spacing(const ccfv_grid &g, int dir) {
+  return dir == 0 ? (g.x_max - g.x_min) / g.nx : (g.y_max - g.y_min) / g.ny;
+}
+
+const SolverTable *get_table(ccfv_ctx *ctx, int dir, double Dt, bool fp64, int *status) {
+  auto key = std::make_tuple(dir, Dt, fp64 ? 1 : 0);
+  auto it = ctx->tables.find(key);
+  if (it != ctx->tables.end()) return it->second.get();
+  const ccfv_grid &g = ctx->grid;
+  const int L = dir == 0 ? g.nx : g.ny;
+  const double h = spacing(g, dir);
+  const double r2 = Dt / (h * h);
+  const double coA = 1.0 / 12 - 0.5 * g.K * r2;
+  const double coB = 10.0 / 12 + g.K * r2;
+  auto tab = std::make_unique<SolverTable>();
+  size_t bytes = 3 * (size_t)L * (fp64 ? 8 : 4);
+  if (tab->buf.alloc(bytes) != cudaSuccess) {
+    *status = set_error(ctx, CCFV_ERR_NOMEM, "solver table allocation failed");
+    return nullptr;
+  }
+  cudaError_t e;
+  if (fp64) {
+    std::vector<double> h_tab;
+    build_table(L, coA, coB, g.bc, h_tab, tab->sm_fac, tab->sm_inv_den);
+    e = cudaMemcpy(tab->buf.p, h_tab.data(), bytes, cudaMemcpyHostToDevice);
+  } else {
+    std::vector<float> h_tab;
+    build_table(L, coA, coB, g.bc, h_tab, tab->sm_fac, tab->sm_inv_den);
+    e = cudaMemcpy(tab->buf.p, h_tab.data(), bytes, cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    *status = set_error(ctx, CCFV_ERR_CUDA, cudaGetErrorString(e));
+    return nullptr;
+  }
+  const SolverTable *res = tab.get();
+  ctx->tables[key] = std::move(tab);
+  return res;
+}
+
+// Largest |velocity component along the sweep| over the domain (bounds the
+// characteristic displacement, hence the staged halo).
+static double wmax(const ccfv_grid &g, int dir) {
+  const double *p = g.vel_params;
+  switch (g.velocity) {
+    case CCFV_VEL_REF_ROT4:
+      return dir == 0 ? 4 * std::max(std::fabs(g.y_min), std::fabs(g.y_max))
+                      : 4 * std::max(std::fabs(g.x_min), std::fabs(g.x_max));
+    case CCFV_VEL_CONST: return std::fabs(dir == 0 ? p[0] : p[1]);
+    case CCFV_VEL_ROTATION:
+      return dir == 0 ? std::fabs(p[0]) * std::max(std::fabs(g.y_min - p[2]), std::fabs(g.y_max - p[2]))
+                      : std::fabs(p[0]) * std::max(std::fabs(g.x_min - p[1]), std::fabs(g.x_max - p[1]));
+    case CCFV_VEL_SWIRL: return 1.0;
+  }
+  return 0.0;
+}
+
+static int shift_cells(const ccfv_grid &g, int dir, double Dt) {
+  double s = std::fabs(Dt) * wmax(g, dir) / spacing(g, dir);
+  return (int)std::ceil(s + 1e-9);
+}
+
+SweepField make_field(const ccfv_grid &g, int dir, double Dt, double ta_rel, double tb_rel,
+                      void *data, const SolverTable *tab, int dsrc) {
+  SweepField f;
+  std::memset(&f, 0, sizeof(f));
+  const double dx = (g.x_max - g.x_min) / g.nx, dy = (g.y_max - g.y_min) / g.ny;
+  if (dir == 0) {
+    f.L = g.nx; f.M = g.ny; f.s_pos = g.ny; f.s_line = 1;
+    f.s_min = g.x_min; f.s_max = g.x_max; f.h = dx; f.t_min = g.y_min; f.ht = dy;
+    f.eps_remap = 1e-15;  // T2S4:323-324
+  } else {
+    f.L = g.ny; f.M = g.nx; f.s_pos = 1; f.s_line = g.ny;
+    f.s_min = g.y_min; f.s_max = g.y_max; f.h = dy; f.t_min = g.x_min; f.ht = dx;
+    f.eps_remap = 1e-16;  // T2S4:414-415
+  }
+  f.data = data;
+  f.dir = dir;
+  f.bc = g.bc;
+  f.vel = g.velocity;
+  for (int i = 0; i < 4; ++i) f.vp[i] = g.vel_params[i];
+  f.Dt = Dt;
+  f.ta_rel = ta_rel;
+  f.tb_rel = tb_rel;
+  f.kb = 0.5 * g.K * (Dt / f.h);
+  f.inv12h = 1.0 / (12.0 * f.h);
+  f.tab = tab->buf.p;
+  f.sm_fac = tab->sm_fac;
+  f.sm_inv_den = tab->sm_inv_den;
+  f.groups = (f.M + LPG - 1) / LPG;
+  f.dsrc = dsrc;
+  f.hd = dsrc ? shift_cells(g, dir, Dt) + 4 : 0;
+  f.uniform = (g.velocity == CCFV_VEL_REF_ROT4 || g.velocity == CCFV_VEL_CONST ||
+               g.velocity == CCFV_VEL_ROTATION) ? 1 : 0;
+  return f;
+}
+
+static LaunchGeom geom_for(const ccfv_grid &g, int dir, double Dt, int dsrc) {
+  LaunchGeom G;
+  const int L = dir == 0 ? g.nx : g.ny;
+  G.cs = (L + LC_MAX - 1) / LC_MAX;
+  G.lc_max = (L + G.cs - 1) / G.cs;
+  const int sh = shift_cells(g, dir, Dt);
+  G.halo = dsrc ? (sh + 4) + sh + 5 : sh + 5;
+  return G;
+}
+
+// Sub-steps of one split step: x(dt/2) over [t, t+dt/2], y(dt) over
+// [t, t+dt], x(dt/2) over [t+dt/2, t+dt] (GpuOneStep, T2S4:785-968).
+static void sweep_kind(int kind, double dt, int *dir, double *Dt, double *ta, double *tb) {
+  if (kind == 0) { *dir = 0; *Dt = 0.5 * dt; *ta = 0.0; *tb = 0.5 * dt; }
+  else if (kind == 1) { *dir = 1; *Dt = dt; *ta = 0.0; *tb = dt; }
+  else { *dir = 0; *Dt = 0.5 * dt; *ta = 0.5 * dt; *tb = dt; }
+}
+
+int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
+                    const std::vector<std::pair<void *, double>> &fields) {
+  const ccfv_grid &g = ctx->grid;
+  const int nf = (int)fields.size();
+  std::vector<SweepField> h(3 * (size_t)nf);
+  for (int kind = 0; kind < 3; ++kind) {
+    int dir;
+    double Dt, ta, tb;
+    sweep_kind(kind, dt, &dir, &Dt, &ta, &tb);
+    const int dsrc = (kind == 2 && g.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
+    int st = CCFV_OK;
+    const SolverTable *tab = get_table(ctx, dir, Dt, fp64, &st);
+    if (!tab) return st;
+    LaunchGeom G = geom_for(g, dir, Dt, dsrc);
+    if (G.cs > MAX_CLUSTER)
+      return set_error(ctx, CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
+    if (sweep_smem_bytes(G.lc_max, G.halo, fp64) > 227 * 1024)
+      return set_error(ctx, CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
+    for (int i = 0; i < nf; ++i) {
+      SweepField f = make_field(g, dir, Dt, ta + fields[i].second, tb + fields[i].second,
+                                fields[i].first, tab, dsrc);
+      f.group0 = i * f.groups;
+      h[(size_t)kind * nf + i] = f;
+      plan->groups_per_field[kind] = f.groups;
+    }
+    plan->geom[kind] = G;
+  }
+  plan->nf = nf;
+  CK(plan->fields.alloc(sizeof(SweepField) * h.size()));
+  CK(cudaMemcpy(plan->fields.p, h.data(), sizeof(SweepField) * h.size(), cudaMemcpyHostToDevice));
+  return CCFV_OK;
+}
+
+int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int count,
+                  double toff, void *data_override, cudaStream_t st) {
+  const SweepField *base = plan.fields.as<SweepField>();
+  unsigned *status = ctx->status.as<unsigned>();
+  for (int kind = 0; kind < 3; ++kind) {
+    const LaunchGeom &G = plan.geom[kind];
+    const int gpf = plan.groups_per_field[kind];
+    const SweepField *fk = base + (size_t)kind * plan.nf;
+    cudaError_t e =
+        fp64 ? launch_sweep<double>(fk, plan.nf, first * gpf, count * gpf, G.cs, G.lc_max,
+                                    G.halo, toff, data_override, status, st)
+             : launch_sweep<float>(fk, plan.nf, first * gpf, count * gpf, G.cs, G.lc_max, G.halo,
+                                   toff, data_override, status, st);
+    CK(e);
+  }
+  return CCFV_OK;
+}
+
+static StepPlan *single_plan(ccfv_ctx *ctx, double dt, bool fp64, int *status) {
+  auto key = std::make_tuple(dt, fp64 ? 1 : 0);
+  auto it = ctx->step_plans.find(key);
+  if (it != ctx->step_plans.end()) return it->second.get();
+  auto plan = std::make_unique<StepPlan>();
+  std::vector<std::pair<void *, double>> f{{nullptr, 0.0}};
+  int st = build_step_plan(ctx, plan.get(), dt, fp64, f);
+  if (st != CCFV_OK) {
+    *status = st;
+    return nullptr;
+  }
+  StepPlan *res = plan.get();
+  ctx->step_plans[key] = std::move(plan);
+  return res;
+}
+
+int steps(ccfv_ctx *ctx, void *d_C, bool fp64, double t0, double dt, int nsteps, cudaStream_t st) {
+  int status = CCFV_OK;
+  StepPlan *plan = single_plan(ctx, dt, fp64, &status);
+  if (!plan) return status;
+  for (int n = 0; n < nsteps; ++n) {
+    int rc = run_step_plan(ctx, *plan, fp64, 0, 1, t0 + n * dt, d_C, st);
+    if (rc) return rc;
+  }
+  return CCFV_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Element-wise kernels: precision conversion and the fused Parareal correction.
+
+template <typename S, typename D>
+__global__ void convert_kernel(const S *__restrict__ src, D *__restrict__ dst, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (D)src[i];
+}
+
+constexpr int RED_THREADS = 256;
+constexpr int RED_BLOCKS = 592;  // 4 x 148 SMs
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// U+[n+1] = G + (F - Gold)  (STANDARD; parareal_correction_kernel, T2S4:771-782)
+// U+[n+1] = F + G(e)        (DELTA)
+// fused with the update norms sum (U+ - U)^2 and sum U+^2, reduced
+// deterministically (fixed-order block partials, last block finishes).
+// STANDARD stores G into Gold; DELTA stores the new increment into W.
+template <typename TG>
+__global__ void __launch_bounds__(RED_THREADS)
+    correction_kernel(int form, long long n, double *__restrict__ U, const double *__restrict__ Fv,
+                      double *__restrict__ Gold, TG *__restrict__ W, double *__restrict__ partial,
+                      unsigned *__restrict__ counter, double *__restrict__ out) {
+  double se = 0.0, su = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double uo = U[i];
+    const double gw = (double)W[i];
+    double un;
+    if (form == CCFV_FORM_STANDARD) {
+      un = gw + (Fv[i] - Gold[i]);
+      Gold[i] = gw;
+    } else {
+      un = Fv[i] + gw;
+    }
+    const double d = un - uo;
+    U[i] = un;
+    if (form != CCFV_FORM_STANDARD) W[i] = (TG)d;
+    se += d * d;
+    su += un * un;
+  }
+  __shared__ double red[2][RED_THREADS / 32];
+  __shared__ bool last;
+  se = warp_sum(se);
+  su = warp_sum(su);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { red[0][w] = se; red[1][w] = su; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int k = 0; k < RED_THREADS / 32; ++k) { a += red[0][k]; b += red[1][k]; }
+    partial[2 * blockIdx.x] = a;
+    partial[2 * blockIdx.x + 1] = b;
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double a = 0, b = 0;
+    for (unsigned k = 0; k < gridDim.x; ++k) {
+      a += ((volatile double *)partial)[2 * k];
+      b += ((volatile double *)partial)[2 * k + 1];
+    }
+    out[0] = a;
+    out[1] = b;
+    *counter = 0;
+  }
+}
+
+static int grid_for(long long n) {
+  long long b = (n + RED_THREADS - 1) / RED_THREADS;
+  return (int)std::max(1LL, std::min<long long>(b, RED_BLOCKS));
+}
+
+template <typename S, typename D>
+static int convert(ccfv_ctx *ctx, const S *src, D *dst, long long n, cudaStream_t st) {
+  count_launch();
+  convert_kernel<S, D><<<grid_for(n), RED_THREADS, 0, st>>>(src, dst, n);
+  CK(cudaGetLastError());
+  return CCFV_OK;
+}
+
+template <typename TG>
+static int correction(ccfv_ctx *ctx, int form, long long n, double *U, const double *Fv,
+                      double *Gold, TG *W, double *out, cudaStream_t st) {
+  count_launch();
+  correction_kernel<TG><<<grid_for(n), RED_THREADS, 0, st>>>(
+      form, n, U, Fv, Gold, W, ctx->partial.as<double>(), ctx->counter.as<unsigned>(), out);
+  CK(cudaGetLastError());
+  return CCFV_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Parareal (T2S4_Parareal.cu:1249-1355, generalised).
+//
+// Slice states U[0..S], fine results F[1..S] (F[n+1] = F(U[n])), coarse work
+// field W in the coarse precision.  Iteration k (1-based) leaves slices
+// n < k exact, so only slices n >= k-1 are propagated and corrected.
+//   F-phase: all active slices advance J fine steps together, one launch per
+//            sweep over every slice (3 J launches).
+//   G-phase: sequential over slices, m coarse steps of the single field W,
+//            then the fused correction + norm kernel.
+
+template <typename TG>
+static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const double *C0,
+                         double *C_T, ccfv_stats *stats, cudaStream_t st) {
+  const ccfv_grid &g = ctx->grid;
+  const bool g64 = sizeof(TG) == 8;
+  const long long NN = (long long)g.nx * g.ny;
+  const int S = o->n_slices;
+  const int J = o->nt_fine / S;
+  const int m = o->coarse_ratio > 0 ? J / o->coarse_ratio : 1;
+  const double DT = (o->t1 - o->t0) / S;
+  const double dt = DT / (double)J;  // FinePropagator: dt = DT / J (T2S4:979)
+  const double dtc = DT / (double)m;
+  const size_t fb = sizeof(double) * NN;
+
+  CK(ctx->U.alloc(fb * (S + 1)));
+  CK(ctx->F.alloc(fb * (S + 1)));
+  if (o->form == CCFV_FORM_STANDARD) CK(ctx->Gold.alloc(fb * (S + 1)));
+  CK(ctx->W.alloc(sizeof(TG) * NN));
+  CK(ctx->norms.alloc(sizeof(double) * 2 * (S + 1)));
+  double *U = ctx->U.as<double>(), *F = ctx->F.as<double>();
+  double *Gold = o->form == CCFV_FORM_STANDARD ? ctx->Gold.as<double>() : nullptr;
+  TG *W = ctx->W.as<TG>();
+  double *norms = ctx->norms.as<double>();
+
+  // fine plan over all slices: field n = F[n+1], time origin t0 + n*DT
+  const double key[4] = {dt, o->t0, DT, (double)S};
+  if (!ctx->fine_plan || std::memcmp(key, ctx->fine_plan_key, sizeof(key)) != 0 ||
+      ctx->fine_plan_slices != S) {
+    auto plan = std::make_unique<StepPlan>();
+    std::vector<std::pair<void *, double>> fl;
+    for (int n = 0; n < S; ++n) fl.push_back({F + (size_t)(n + 1) * NN, o->t0 + n * DT});
+    int rc = build_step_plan(ctx, plan.get(), dt, true, fl);
+    if (rc) return rc;
+    ctx->fine_plan = std::move(plan);
+    std::memcpy(ctx->fine_plan_key, key, sizeof(key));
+    ctx->fine_plan_slices = S;
+  }
+  int status = CCFV_OK;
+  StepPlan *cplan = single_plan(ctx, dtc, g64, &status);
+  if (!cplan) return status;
+
+  cudaEvent_t ev0, ev1;
+  CK(cudaEventCreate(&ev0));
+  CK(cudaEventCreate(&ev1));
+  CK(cudaEventRecord(ev0, st));
+  const cudaMemcpyKind k_in = o->mem == CCFV_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  CK(cudaMemcpyAsync(U, C0, fb, k_in, st));
+
+  auto coarse_on_W = [&](int n) -> int {
+    for (int i = 0; i < m; ++i) {
+      int rc = run_step_plan(ctx, *cplan, g64, 0, 1, o->t0 + n * DT + i * dtc, W, st);
+      if (rc) return rc;
+    }
+    return CCFV_OK;
+  };
+
+  // k = 0: coarse sweep U[n+1] = G(U[n])  (T2S4:1271-1280)
+  for (int n = 0; n < S; ++n) {
+    int rc;
+    if (g64) CK(cudaMemcpyAsync(W, U + (size_t)n * NN, fb, cudaMemcpyDeviceToDevice, st));
+    else if ((rc = convert(ctx, U + (size_t)n * NN, W, NN, st))) return rc;
+    if ((rc = coarse_on_W(n))) return rc;
+    if (g64) CK(cudaMemcpyAsync(U + (size_t)(n + 1) * NN, W, fb, cudaMemcpyDeviceToDevice, st));
+    else if ((rc = convert(ctx, W, U + (size_t)(n + 1) * NN, NN, st))) return rc;
+    if (Gold) CK(cudaMemcpyAsync(Gold + (size_t)(n + 1) * NN, U + (size_t)(n + 1) * NN, fb,
+                                 cudaMemcpyDeviceToDevice, st));
+  }
+
+  std::vector<double> hn(2 * (size_t)(S + 1));
+  int iters = 0, converged = 0;
+  double fine_cu = 0, coarse_cu = (double)S * m * NN;
+  double fine_ms = 0, coarse_ms = 0;
+  long long fine_launches = 0, fine_cells = 0;
+  cudaEvent_t fa, fb_, gb;
+  CK(cudaEventCreate(&fa));
+  CK(cudaEventCreate(&fb_));
+  CK(cudaEventCreate(&gb));
+  for (int k = 1; k <= o->kmax; ++k) {
+    const int nlo = k - 1;
+    const int act = S - nlo;
+    // F-phase
+    CK(cudaMemcpyAsync(F + (size_t)(nlo + 1) * NN, U + (size_t)nlo * NN, fb * act,
+                       cudaMemcpyDeviceToDevice, st));
+    CK(cudaEventRecord(fa, st));
+    for (int j = 0; j < J; ++j) {
+      int rc = run_step_plan(ctx, *ctx->fine_plan, true, nlo, act, j * dt, nullptr, st);
+      if (rc) return rc;
+    }
+    CK(cudaEventRecord(fb_, st));
+    fine_cu += (double)act * J * NN;
+    fine_launches += 3LL * J;
+    fine_cells += 3LL * J * act * NN;
+    // G-phase + correction
+    CK(cudaMemsetAsync(norms, 0, sizeof(double) * 2 * (S + 1), st));
+    for (int n = nlo; n < S; ++n) {
+      int rc;
+      if (o->form == CCFV_FORM_STANDARD) {
+        CK(cudaMemcpyAsync(W, U + (size_t)n * NN, fb, cudaMemcpyDeviceToDevice, st));
+        if ((rc = coarse_on_W(n))) return rc;
+        coarse_cu += (double)m * NN;
+      } else if (n == nlo) {
+        CK(cudaMemsetAsync(W, 0, sizeof(TG) * NN, st));  // G(0) = 0
+      } else {
+        if ((rc = coarse_on_W(n))) return rc;
+        coarse_cu += (double)m * NN;
+      }
+      if ((rc = correction<TG>(ctx, o->form, NN, U + (size_t)(n + 1) * NN,
+                               F + (size_t)(n + 1) * NN,
+                               Gold ? Gold + (size_t)(n + 1) * NN : nullptr, W,
+                               norms + 2 * (n + 1), st)))
+        return rc;
+    }
+    CK(cudaEventRecord(gb, st));
+    CK(cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 2 * (S + 1), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    {
+      float a = 0, b = 0;
+      cudaEventElapsedTime(&a, fa, fb_);
+      cudaEventElapsedTime(&b, fb_, gb);
+      fine_ms += a;
+      coarse_ms += b;
+    }
+    double worst = 0.0;
+    for (int n = nlo + 1; n <= S; ++n) {
+      double e = std::sqrt(hn[2 * n]), u = std::sqrt(hn[2 * n + 1]);
+      double r = u > 0 ? e / u : e;
+      worst = std::max(worst, r);
+    }
+    iters = k;
+    if (stats && k - 1 < CCFV_MAX_ITERS) stats->update[k - 1] = worst;
+    if (o->tol > 0 && worst < o->tol) {
+      converged = 1;
+      break;
+    }
+  }
+  const cudaMemcpyKind k_out = o->mem == CCFV_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  CK(cudaMemcpyAsync(C_T, U + (size_t)S * NN, fb, k_out, st));
+  CK(cudaEventRecord(ev1, st));
+  CK(cudaStreamSynchronize(st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  cudaEventDestroy(fa);
+  cudaEventDestroy(fb_);
+  cudaEventDestroy(gb);
+  if (stats) {
+    stats->fine_ms = fine_ms;
+    stats->coarse_ms = coarse_ms;
+    stats->fine_sweep_launches = fine_launches;
+    stats->fine_sweep_cells = fine_cells;
+    stats->iterations = iters;
+    stats->converged = converged;
+    stats->fine_cell_updates = fine_cu;
+    stats->coarse_cell_updates = coarse_cu;
+    stats->ms = ms;
+  }
+  return CCFV_OK;
+}
+
+int parareal(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const double *C0, double *C_T,
+             ccfv_stats *stats, cudaStream_t st) {
+  if (!o || !C0 || !C_T) return set_error(ctx, CCFV_ERR_INVALID, "null argument");
+  if (o->n_slices < 1 || o->nt_fine < o->n_slices || o->nt_fine % o->n_slices)
+    return set_error(ctx, CCFV_ERR_INVALID, "nt_fine must be a positive multiple of n_slices");
+  const int J = o->nt_fine / o->n_slices;
+  if (o->coarse_ratio < 0 || (o->coarse_ratio > 0 && J % o->coarse_ratio))
+    return set_error(ctx, CCFV_ERR_INVALID, "coarse_ratio must divide nt_fine / n_slices");
+  if (o->kmax < 1 || o->kmax > CCFV_MAX_ITERS)
+    return set_error(ctx, CCFV_ERR_INVALID, "kmax out of range");
+  if (o->form != CCFV_FORM_STANDARD && o->form != CCFV_FORM_DELTA)
+    return set_error(ctx, CCFV_ERR_INVALID, "unknown Parareal form");
+  if (o->coarse_precision == CCFV_FP32 && o->form != CCFV_FORM_DELTA)
+    return set_error(ctx, CCFV_ERR_INVALID, "an FP32 coarse propagator needs the DELTA form");
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  int rc = o->coarse_precision == CCFV_FP32 ? parareal_impl<float>(ctx, o, C0, C_T, stats, st)
+                                            : parareal_impl<double>(ctx, o, C0, C_T, stats, st);
+  if (rc) return rc;
+  unsigned flag = 0;
+  CK(cudaMemcpy(&flag, ctx->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (flag) {
+    CK(cudaMemset(ctx->status.p, 0, sizeof(unsigned)));
+    return set_error(ctx, CCFV_ERR_HALO, "a characteristic foot left the staged halo");
+  }
+  return CCFV_OK;
+}
+
+int coarse_fp32(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, cudaStream_t st) {
+  const long long NN = (long long)ctx->grid.nx * ctx->grid.ny;
+  CK(ctx->C32.alloc(sizeof(float) * NN));
+  float *w = ctx->C32.as<float>();
+  int rc = convert(ctx, d_C, w, NN, st);
+  if (rc) return rc;
+  const double dtc = DT / (double)m;
+  if ((rc = steps(ctx, w, false, tn, dtc, m, st))) return rc;
+  return convert(ctx, w, d_C, NN, st);
+}
+
+}  // namespace ccfv

@@ -1,0 +1,82 @@
+// engine.h -- host-side solver context, plans and Parareal engine of libccfv.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/ccfv.h"
+#include "ccfv_internal.h"
+
+namespace ccfv {
+
+// Device memory owned by the library; freed on destruction.
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { if (p) cudaFree(p); }
+  cudaError_t alloc(size_t b);
+  template <typename T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+// Line-invariant LU factors of one constant tridiagonal system (device, T[3L]).
+struct SolverTable {
+  DevBuf buf;
+  double sm_fac = 0, sm_inv_den = 0;
+};
+
+// Launch geometry shared by all fields of one sweep launch.
+struct LaunchGeom {
+  int cs = 1, lc_max = 0, halo = 0, groups = 0;
+};
+
+// Three sweep launches (x dt/2, y dt, x dt/2) of one step over a set of fields.
+struct StepPlan {
+  DevBuf fields;          // SweepField[3][nf]
+  int nf = 0;
+  int groups_per_field[3] = {0, 0, 0};
+  LaunchGeom geom[3];
+};
+
+}  // namespace ccfv
+
+struct ccfv_ctx {
+  ccfv_grid grid;
+  int device = 0;
+  ccfv::DevBuf status;  // unsigned status word + partial-sum scratch
+  std::map<std::tuple<int, double, int>, std::unique_ptr<ccfv::SolverTable>> tables;
+  std::map<std::tuple<double, int>, std::unique_ptr<ccfv::StepPlan>> step_plans;
+  // Parareal slice states and scratch
+  ccfv::DevBuf U, F, Gold, W, C64, C32, norms, partial, counter, io;
+  size_t slices_cap = 0;
+  std::unique_ptr<ccfv::StepPlan> fine_plan;
+  double fine_plan_key[4] = {0, 0, 0, 0};
+  int fine_plan_slices = 0;
+  std::string last_error;
+};
+
+namespace ccfv {
+
+int set_error(ccfv_ctx *ctx, int code, const std::string &msg);
+const SolverTable *get_table(ccfv_ctx *ctx, int dir, double Dt, bool fp64, int *status);
+SweepField make_field(const ccfv_grid &g, int dir, double Dt, double ta_rel, double tb_rel,
+                      void *data, const SolverTable *tab, int dsrc);
+int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
+                    const std::vector<std::pair<void *, double>> &fields);
+int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int count,
+                  double toff, void *data_override, cudaStream_t st);
+int steps(ccfv_ctx *ctx, void *d_C, bool fp64, double t0, double dt, int nsteps, cudaStream_t st);
+int coarse_fp32(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, cudaStream_t st);
+int parareal(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const double *C0, double *C_T,
+             ccfv_stats *stats, cudaStream_t st);
+constexpr int RED_BLOCKS_MAX = 592;
+
+}  // namespace ccfv

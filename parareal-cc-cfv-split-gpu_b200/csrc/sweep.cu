@@ -1,0 +1,670 @@
+// sweep.cu -- the fused T2S4 CC-CFV sweep for sm_100a.
+//
+// One launch performs one directional sub-step (an x(dt/2) or y(dt) sweep of
+// GpuOneStep, T2S4_Parareal.cu:824-963) for any number of fields.  Per line
+// of cells it fuses what the reference spreads over ~11 kernels and ~40
+// N^2-sized global arrays:
+//   characteristic feet of the cell edges     (T2S4:203-258)
+//   PPM reconstruction + conservative remap   (T2S4:260-438)
+//   4th-order derivative at the edge feet     (T2S4:440-547)
+//   Crank-Nicolson RHS + compact mass matrix  (T2S4:550-654)
+//   tridiagonal solve                         (T2S4:657-719)
+// Each cell is read once from HBM and written once.
+//
+// Work decomposition.  A tile is LPG = 16 neighbouring lines.  A cluster of
+// cs CTAs covers the whole length of the tile's lines, each CTA a run of up
+// to LC_MAX consecutive positions plus a halo on both sides (loaded from
+// global memory; in place is safe because every store happens after a
+// cluster-wide barrier that follows all loads).  The shared tile is
+// [position][line] with an odd pitch: for x-sweeps global rows of 16
+// doubles (128 B) land in shared rows; for y-sweeps each line is a
+// contiguous global run written down a shared column.
+//
+// Thread mapping: lane % 16 = line, each thread owns a chunk of consecutive
+// positions of its line.  The constant-coefficient tridiagonal system is
+// solved as two first-order linear recurrences (LU forward / backward) with
+// line-invariant factors alpha_k, g_k precomputed per (L, dt, K): every
+// chunk runs its recurrence locally from a zero carry, the chunk maps
+// (prod alpha, local value) are composed across the CTA (shared memory) and
+// across the cluster (distributed shared memory), and a fix-up pass adds the
+// carried-in value times the running product.  The periodic (cyclic) system
+// adds a Sherman-Morrison rank-one correction with a line-invariant vector.
+#include <cooperative_groups.h>
+
+#include <climits>
+#include <cstdio>
+
+#include "ccfv_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace ccfv {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// velocity component along the sweep: x-sweep u(x=s, y=tau), y-sweep v(x=tau, y=s)
+__device__ __forceinline__ double vel_along(const SweepField &f, double s, double tau, double t) {
+  switch (f.vel) {
+    case VEL_REF_ROT4:  // Vx = -4y, Vy = 4x (T2S4_Parareal.cu:44-45)
+      return f.dir == 0 ? -4 * tau : 4 * tau;
+    case VEL_CONST:
+      return f.dir == 0 ? f.vp[0] : f.vp[1];
+    case VEL_ROTATION:
+      return f.dir == 0 ? -f.vp[0] * (tau - f.vp[2]) : f.vp[0] * (tau - f.vp[1]);
+    case VEL_SWIRL: {
+      double ss = sinpi(s);
+      double w = ss * ss * sinpi(2.0 * tau) * cospi(t / f.vp[0]);
+      return f.dir == 0 ? w : -w;
+    }
+  }
+  return 0.0;
+}
+
+// Heun foot of a cell corner (get_Lagrange_points_on_gpu, T2S4:203-229):
+// s* = s - Dt w(s, tb); foot = s - Dt/2 (w(s, tb) + w(s*, ta)).
+__device__ __forceinline__ double corner_foot(const SweepField &f, double s, double tau, double ta,
+                                              double tb) {
+  double w0 = vel_along(f, s, tau, tb);
+  double xs = s - f.Dt * w0;
+  return s - 0.5 * f.Dt * (w0 + vel_along(f, xs, tau, ta));
+}
+
+// Foot of edge e of a line = mean of its two corner feet
+// (intersection_point_vert_x / _hori_y, T2S4:231-258).
+__device__ __forceinline__ double edge_foot(const SweepField &f, int e, double tau0, double tau1,
+                                            double ta, double tb) {
+  double s = f.s_min + f.h * e;
+  return 0.5 * (corner_foot(f, s, tau0, ta, tb) + corner_foot(f, s, tau1, ta, tb));
+}
+
+// Bounds-checked view of one line in the shared tile, indexed by position.
+template <typename T>
+struct LineView {
+  const T *cs;
+  int base;   // row of position 0 = H - p0
+  int nrows;
+  unsigned *status;
+  __device__ __forceinline__ T operator()(int pos) const {
+    int row = pos + base;
+    if (row < 0 || row >= nrows) {
+      atomicOr(status, STATUS_HALO);
+      return T(0);
+    }
+    return cs[row * PITCH];
+  }
+};
+
+template <typename T>
+struct Ppm {
+  T CL, D, C6;
+};
+
+// PPM coefficients of cell i (x_step_ppm_coef_on_gpu, T2S4:260-304); ghost
+// cells are already in the tile (compat) or it holds wrapped cells (periodic).
+template <typename T>
+__device__ __forceinline__ Ppm<T> ppm(const LineView<T> &v, int i) {
+  const T one_twelfth = T(1.0 / 12.0), seven_twelfths = T(7.0 / 12.0);
+  T cm2 = v(i - 2), cm1 = v(i - 1), c0 = v(i), cp1 = v(i + 1), cp2 = v(i + 2);
+  T cl = seven_twelfths * (c0 + cm1) - one_twelfth * (cp1 + cm2);
+  T cr = seven_twelfths * (cp1 + c0) - one_twelfth * (cp2 + cm1);
+  Ppm<T> p;
+  p.CL = cl;
+  p.D = cr - cl;
+  p.C6 = T(6.0) * (c0 - T(0.5) * (cl + cr));
+  return p;
+}
+
+// PPM antiderivative in cell units (d_intC_ppm4th, T2S4:63-65).
+template <typename T>
+__device__ __forceinline__ T ppm_int(const Ppm<T> &p, T xi) {
+  T xi2 = xi * xi;
+  return T(-1.0 / 3) * p.C6 * (xi2 * xi) + T(0.5) * (p.D + p.C6) * xi2 + p.CL * xi;
+}
+
+// Neumaier-compensated sum of cells lo..hi.
+template <typename T>
+__device__ __forceinline__ T sum_cells(const LineView<T> &v, int lo, int hi) {
+  T s = T(0), comp = T(0);
+  for (int k = lo; k <= hi; ++k) {
+    T x = v(k);
+    T t = s + x;
+    comp += (fabs(s) >= fabs(x)) ? ((s - t) + x) : ((x - t) + s);
+    s = t;
+  }
+  return s + comp;
+}
+
+// Conservative remap of one cell over its departure interval [fL, fR].
+// compat: x_step_intC_ppm_on_gpu / y_step_intC_ppm_on_gpu (T2S4:306-438):
+// zero inflow from outside the domain, feet clamped by eps_remap.  The
+// reference's y-remap reads the next row's first cell when its right foot
+// is clamped onto the top edge (jR == Ny, an O(2^-53 * Ny) contribution);
+// here that term is zero.
+template <typename T>
+__device__ __forceinline__ T remap_cell(const SweepField &f, const LineView<T> &v, double fL,
+                                        double fR) {
+  const int L = f.L;
+  if (f.bc == BC_COMPAT) {
+    if (fL > f.s_max || fR < f.s_min || fL == fR) return T(0);
+    double xL = fmax(fL, f.s_min + f.eps_remap);
+    double xR = fmin(fR, f.s_max - f.eps_remap);
+    int iL = (int)floor((xL - f.s_min) / f.h);
+    int iR = (int)floor((xR - f.s_min) / f.h);
+    T xiL = (T)((xL - (f.s_min + f.h * iL)) / f.h);
+    T xiR = (T)((xR - (f.s_min + f.h * iR)) / f.h);
+    Ppm<T> z{T(0), T(0), T(0)};
+    Ppm<T> pL = (iL >= 0 && iL < L) ? ppm(v, iL) : z;
+    if (iR == iL) return ppm_int(pL, xiR) - ppm_int(pL, xiL);
+    Ppm<T> pR = (iR >= 0 && iR < L) ? ppm(v, iR) : z;
+    T IntCL = ppm_int(pL, T(1)) - ppm_int(pL, xiL);
+    T IntCR = ppm_int(pR, xiR);
+    T IntCM = T(0);
+    int hi = iR - 1 < L - 1 ? iR - 1 : L - 1;
+    for (int k = iL + 1; k <= hi; ++k) IntCM += v(k);
+    return IntCL + IntCM + IntCR;
+  } else {
+    double uL = (fL - f.s_min) / f.h, uR = (fR - f.s_min) / f.h;
+    double fkL = floor(uL), fkR = floor(uR);
+    int kL = (int)fkL, kR = (int)fkR;
+    T xiL = (T)(uL - fkL), xiR = (T)(uR - fkR);
+    Ppm<T> pL = ppm(v, kL);
+    if (kR == kL) return ppm_int(pL, xiR) - ppm_int(pL, xiL);
+    if (abs(kR - kL) > v.nrows) {  // cannot happen within the staged halo
+      atomicOr(v.status, STATUS_HALO);
+      return T(0);
+    }
+    Ppm<T> pR = ppm(v, kR);
+    if (kR > kL) return sum_cells(v, kL, kR - 1) + ppm_int(pR, xiR) - ppm_int(pL, xiL);
+    return -(sum_cells(v, kR, kL - 1) + ppm_int(pL, xiL) - ppm_int(pR, xiR));
+  }
+}
+
+// Fourth-order derivative at a foot (dcdx_bar_on_gpu / dcdy_bar_on_gpu,
+// T2S4:440-547).  compat keeps the reference's ghost selection at iL = L-2
+// (+2 tap reads C_{N+1}) and iL = 1 (-2 tap reads C_{-2}).
+template <typename T>
+__device__ __forceinline__ T foot_derivative(const SweepField &f, const LineView<T> &v, double fb) {
+  const int L = f.L;
+  int iL, pm2, pp2;
+  T xi;
+  if (f.bc == BC_COMPAT) {
+    if (!(fb >= f.s_min && fb <= f.s_max)) return T(0);
+    double ixb = fmin(fmax(fb, f.s_min + 1e-15), f.s_max - 1e-15);
+    iL = (int)floor((ixb - f.s_min) / f.h);
+    xi = (T)((ixb - (f.s_min + f.h * iL)) / f.h);
+    pm2 = (iL == 1) ? -2 : iL - 2;
+    pp2 = (iL == L - 2) ? L + 1 : iL + 2;
+  } else {
+    double u = (fb - f.s_min) / f.h, fk = floor(u);
+    iL = (int)fk;
+    xi = (T)(u - fk);
+    pm2 = iL - 2;
+    pp2 = iL + 2;
+  }
+  T Cim2 = v(pm2), Cim1 = v(iL - 1), Ci = v(iL), Cip1 = v(iL + 1), Cip2 = v(pp2);
+  T xi2 = xi * xi, xi3 = xi2 * xi;
+  return T(f.inv12h) * ((T(2.0) * xi3 - T(6.0) * xi2 + T(3.0) * xi + T(1.0)) * Cim2 +
+                        (T(-8.0) * xi3 + T(18.0) * xi2 + T(6.0) * xi - T(15.0)) * Cim1 +
+                        (T(12.0) * xi3 - T(18.0) * xi2 - T(24.0) * xi + T(15.0)) * Ci +
+                        (T(-8.0) * xi3 + T(6.0) * xi2 + T(18.0) * xi - T(1.0)) * Cip1 +
+                        (T(2.0) * xi3 - T(3.0) * xi) * Cip2);
+}
+
+// Compat ghost cells C_{-2}, C_{-1}, C_N, C_{N+1} of one line of a tile
+// (3-point extrapolation, T2S4:275-286), written where the tile's rows
+// [lo, hi) cover them.  base = row of position 0.
+template <typename T>
+__device__ __forceinline__ void compat_ghosts(T *c, int base, int lo, int hi, int L) {
+  const T one_eleventh = T(1.0 / 11.0);
+  if (lo <= -2 && hi > 2) {
+    T c0 = c[(base + 0) * PITCH], c1 = c[(base + 1) * PITCH], c2 = c[(base + 2) * PITCH];
+    c[(base - 1) * PITCH] = one_eleventh * (-c2 + T(3) * c1 + T(9) * c0);
+    c[(base - 2) * PITCH] = one_eleventh * (T(-15) * c2 + T(56) * c1 - T(30) * c0);
+  }
+  if (hi >= L + 2 && lo <= L - 3) {
+    T a = c[(base + L - 3) * PITCH], b = c[(base + L - 2) * PITCH], d = c[(base + L - 1) * PITCH];
+    c[(base + L) * PITCH] = one_eleventh * (-a + T(3) * b + T(9) * d);
+    c[(base + L + 1) * PITCH] = one_eleventh * (T(-15) * a + T(56) * b - T(30) * d);
+  }
+}
+
+// Shared-memory carve-up of the sweep kernel.
+template <typename T>
+struct Smem {
+  T *C;      // [(lc_max + 2H) * PITCH]  tile 0: the input cells
+  T *B;      // [(lc_max + 2H) * PITCH]  tile 1
+  // Both tiles are indexed by row = position - p0 + H.  Derivative of the
+  // input: b -> tile 1, q/x -> tile 0.  Derivative of the remapped field:
+  // remap -> tile 1, b -> tile 0, q/x -> tile 1.
+  T *tA;     // [lc_max]  alpha_k
+  T *tG;     // [lc_max]  g_k
+  T *tZ;     // [lc_max]  z_k (periodic)
+  T *aggA;   // [NCH * LPG] chunk products
+  T *aggF;   // [NCH * LPG] chunk forward values
+  T *aggR;   // [NCH * LPG] chunk backward values
+  T *xch;    // [8 * LPG] cluster exchange: fwdA fwdB bwdA bwdB y0 yL
+  SweepField *fd;
+};
+
+template <typename T>
+__device__ __forceinline__ Smem<T> carve(unsigned char *raw, int lc_max, int H) {
+  Smem<T> s;
+  s.fd = reinterpret_cast<SweepField *>(raw);
+  T *p = reinterpret_cast<T *>(raw + ((sizeof(SweepField) + 15) & ~size_t(15)));
+  s.C = p;
+  p += (lc_max + 2 * H) * PITCH;
+  s.B = p;
+  p += (lc_max + 2 * H) * PITCH;
+  s.tA = p;
+  p += lc_max;
+  s.tG = p;
+  p += lc_max;
+  s.tZ = p;
+  p += lc_max;
+  s.aggA = p;
+  p += NCH * LPG;
+  s.aggF = p;
+  p += NCH * LPG;
+  s.aggR = p;
+  p += NCH * LPG;
+  s.xch = p;
+  return s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NTH) sweep_kernel(const SweepField *__restrict__ fields,
+                                                    int nfields, int group_base, double toff,
+                                                    void *data_override, int lc_max, int H,
+                                                    unsigned *status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int cs = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  const int tile = blockIdx.x / cs + group_base;
+  Smem<T> S = carve<T>(smem_raw, lc_max, H);
+
+  // ---- descriptor of this tile's field (binary search on group0) ----
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = nfields - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (fields[mid].group0 <= tile) lo = mid; else hi = mid - 1;
+    }
+    *S.fd = fields[lo];
+    if (data_override) S.fd->data = data_override;
+  }
+  __syncthreads();
+  const SweepField &F = *S.fd;
+  const int L = F.L;
+  const int g = tile - F.group0;
+  const long long line0 = (long long)g * LPG;
+  const int Lc = (L + cs - 1) / cs;
+  const int p0 = min(L, rank * Lc);
+  const int p1 = min(L, p0 + Lc);
+  const int np = p1 - p0;
+  const int nrows = np + 2 * H;
+  const bool periodic = F.bc == BC_PERIODIC;
+  T *gdata = reinterpret_cast<T *>(F.data);
+
+  // ---- phase 0: stage the tile (+halo) and the solver factors ----
+  {
+    const int total = nrows * LPG;
+    const bool xs = (F.s_line == 1);
+    for (int e = threadIdx.x; e < total; e += NTH) {
+      int row, ln;
+      if (xs) { row = e / LPG; ln = e - row * LPG; }
+      else { ln = e / nrows; row = e - ln * nrows; }
+      int pos = p0 - H + row;
+      long long gl = line0 + ln;
+      T val = T(0);
+      if (gl < F.M) {
+        bool ok = true;
+        if (pos < 0 || pos >= L) {
+          if (periodic) { pos %= L; if (pos < 0) pos += L; }
+          else ok = false;
+        }
+        if (ok) val = gdata[(long long)pos * F.s_pos + gl * F.s_line];
+      }
+      S.C[row * PITCH + ln] = val;
+    }
+    const T *tab = reinterpret_cast<const T *>(F.tab);
+    for (int k = threadIdx.x; k < np; k += NTH) {
+      S.tA[k] = tab[p0 + k];
+      S.tG[k] = tab[L + p0 + k];
+      S.tZ[k] = periodic ? tab[2 * L + p0 + k] : T(0);
+    }
+  }
+  __syncthreads();
+  if (!periodic && threadIdx.x < LPG) compat_ghosts(S.C + threadIdx.x, H - p0, p0 - H, p1 + H, L);
+  __syncthreads();
+
+  // ---- thread -> (line, chunk) ----
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ln = lane % LPG;
+  const int c = warp * CPW + lane / LPG;
+  const long long gl = line0 + ln;
+  const int m = (np + NCH - 1) / NCH;
+  const int s = min(p1, p0 + c * m);
+  const int e = min(p1, s + m);
+  const int clast = (np - 1) / m;  // last non-empty chunk
+  LineView<T> v{S.C + ln, H - p0, nrows, status};
+
+  // ---- phase 1: feet, remap, foot derivative, RHS b ----
+  // b_k = remap_k + 0.5 K Dt/h (D_{k+1} - D_k) (x_b_RHS_on_gpu T2S4:564-580);
+  // the source f is identically zero (T2S4:59-61) and adds nothing.
+  T *bArr, *qArr;
+  {
+    int kb = s, ke = e;
+    if (c == 0 && (periodic || p0 > 0)) kb = p0 - 1;
+    if (c == clast && (periodic || p1 < L)) ke = p1 + 1;
+    const double tau0 = F.t_min + F.ht * (double)gl;
+    const double tau1 = F.t_min + F.ht * (double)(gl + 1);
+    const double ta = toff + F.ta_rel, tb = toff + F.tb_rel;
+    const T kbc = T(F.kb);
+    // Uniform displacement: every edge foot of this line sits at e - sigma
+    // (position units), -sigma = n0 + xi0.  Remap, foot derivative and RHS
+    // then reduce to fixed 6-tap stencils with weights depending on xi0 only:
+    //   remap_k = sum_t w_t C_{k+n0+t},  D_{k+1}-D_k = inv12h sum_t q_t C_{k+n0+t}
+    // (t = -2..3), the same PPM integral and cubic derivative weights as the
+    // per-cell formulas, so the fast and per-cell paths agree to rounding.
+    int n0 = 0, klo = 1, khi = 0;
+    T w[6], qd[6];
+    if (F.uniform) {
+      const double f0 = edge_foot(F, 0, tau0, tau1, ta, tb);
+      const double u = (f0 - F.s_min) / F.h;
+      const double fl = floor(u);
+      n0 = (int)fl;
+      const double x = u - fl, x2 = x * x, x3 = x2 * x;
+      const double A = x - 2.0 * x2 + x3, B = x3 - x2, Cc = 3.0 * x2 - 2.0 * x3;
+      w[0] = T(A / 12.0);
+      w[1] = T((B - 8.0 * A) / 12.0);
+      w[2] = T(1.0 - Cc - 2.0 * B / 3.0);
+      w[3] = T(Cc + 2.0 * A / 3.0);
+      w[4] = T((8.0 * B - A) / 12.0);
+      w[5] = T(-B / 12.0);
+      const double pm2 = 2.0 * x3 - 6.0 * x2 + 3.0 * x + 1.0;
+      const double pm1 = -8.0 * x3 + 18.0 * x2 + 6.0 * x - 15.0;
+      const double pz = 12.0 * x3 - 18.0 * x2 - 24.0 * x + 15.0;
+      const double pp1 = -8.0 * x3 + 6.0 * x2 + 18.0 * x - 1.0;
+      const double pp2 = 2.0 * x3 - 3.0 * x;
+      const double kq = F.kb * F.inv12h;
+      qd[0] = T(kq * -pm2);
+      qd[1] = T(kq * (pm2 - pm1));
+      qd[2] = T(kq * (pm1 - pz));
+      qd[3] = T(kq * (pz - pp1));
+      qd[4] = T(kq * (pp1 - pp2));
+      qd[5] = T(kq * pp2);
+      if (periodic) { klo = INT_MIN; khi = INT_MAX; }
+      else { klo = 2 - n0; khi = L - 4 - n0; }  // clear of clamps and ghost quirks
+    }
+    if (F.dsrc == 0) {
+      bArr = S.B;
+      qArr = S.C;
+      if (F.uniform) {
+        for (int k = kb; k < ke; ++k) {
+          T bk;
+          if (k >= klo && k <= khi) {
+            const int r = k + n0 + H - p0 - 2;
+            const T *cp = S.C + r * PITCH + ln;
+            if (r < 0 || r + 5 >= nrows) { atomicOr(status, STATUS_HALO); bk = T(0); }
+            else {
+              bk = T(0);
+#pragma unroll
+              for (int t = 0; t < 6; ++t) bk += (w[t] + qd[t]) * cp[t * PITCH];
+            }
+          } else {
+            double fa = edge_foot(F, k, tau0, tau1, ta, tb);
+            double fb = edge_foot(F, k + 1, tau0, tau1, ta, tb);
+            bk = remap_cell(F, v, fa, fb) + kbc * (foot_derivative(F, v, fb) - foot_derivative(F, v, fa));
+          }
+          bArr[(k - p0 + H) * PITCH + ln] = bk;
+        }
+      } else if (kb < ke) {
+        double fprev = edge_foot(F, kb, tau0, tau1, ta, tb);
+        T dprev = foot_derivative(F, v, fprev);
+        for (int k = kb; k < ke; ++k) {
+          double fnext = edge_foot(F, k + 1, tau0, tau1, ta, tb);
+          T dnext = foot_derivative(F, v, fnext);
+          T ic = remap_cell(F, v, fprev, fnext);
+          bArr[(k - p0 + H) * PITCH + ln] = ic + kbc * (dnext - dprev);
+          fprev = fnext;
+          dprev = dnext;
+        }
+      }
+    } else {
+      // The reference's third sweep differentiates the remapped field
+      // (dcdx_bar_on_gpu(v_d_Cnphf_bar_x, ...), T2S4:929-932): remap the
+      // cells p0-hd .. p1+hd-1 into tile 1 first, then differentiate it.
+      T *R = S.B;
+      int q0 = p0 - F.hd, q1 = p1 + F.hd;
+      if (!periodic) { q0 = max(q0, 0); q1 = min(q1, L); }
+      const int m1 = (q1 - q0 + NCH - 1) / NCH;
+      const int r0 = q0 + c * m1, r1 = min(q1, r0 + m1);
+      for (int k = r0; k < r1; ++k) {
+        T ik;
+        if (F.uniform && k >= klo && k <= khi) {
+          const int r = k + n0 + H - p0 - 2;
+          const T *cp = S.C + r * PITCH + ln;
+          if (r < 0 || r + 5 >= nrows) { atomicOr(status, STATUS_HALO); ik = T(0); }
+          else {
+            ik = T(0);
+#pragma unroll
+            for (int t = 0; t < 6; ++t) ik += w[t] * cp[t * PITCH];
+          }
+        } else {
+          double fa = edge_foot(F, k, tau0, tau1, ta, tb);
+          double fb = edge_foot(F, k + 1, tau0, tau1, ta, tb);
+          ik = remap_cell(F, v, fa, fb);
+        }
+        R[(k - p0 + H) * PITCH + ln] = ik;
+      }
+      __syncthreads();
+      if (!periodic && threadIdx.x < LPG) compat_ghosts(R + threadIdx.x, H - p0, q0 - 2, q1 + 2, L);
+      __syncthreads();
+      LineView<T> vr{R + ln, H - p0, nrows, status};
+      bArr = S.C;
+      qArr = S.B;
+      for (int k = kb; k < ke; ++k) {
+        T bk;
+        if (F.uniform && k >= klo && k <= khi) {
+          const int r = k + n0 + H - p0 - 2;
+          const T *rp = R + r * PITCH + ln;
+          if (r < 0 || r + 5 >= nrows) { atomicOr(status, STATUS_HALO); bk = T(0); }
+          else {
+            T acc = T(0);
+#pragma unroll
+            for (int t = 0; t < 6; ++t) acc += qd[t] * rp[t * PITCH];
+            bk = vr(k) + acc;
+          }
+        } else {
+          double fa = edge_foot(F, k, tau0, tau1, ta, tb);
+          double fb = edge_foot(F, k + 1, tau0, tau1, ta, tb);
+          bk = vr(k) + kbc * (foot_derivative(F, vr, fb) - foot_derivative(F, vr, fa));
+        }
+        bArr[(k - p0 + H) * PITCH + ln] = bk;
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 2: compact mass matrix + local forward recurrence ----
+  T *Cl = qArr + ln;
+  const int rb = H - p0;  // row of position 0 in both tiles
+  {
+    T A = T(1), q = T(0);
+    if (s < e) {
+      const T *Bl = bArr + ln;
+      T bm = Bl[(s - 1 + rb) * PITCH], bc = Bl[(s + rb) * PITCH];
+      for (int k = s; k < e; ++k) {
+        T bp = Bl[(k + 1 + rb) * PITCH];
+        T mb;
+        if (!periodic && k == 0) mb = (T(10.0) * bc + bp) / T(12.0);
+        else if (!periodic && k == L - 1) mb = (T(10.0) * bc + bm) / T(12.0);
+        else mb = (bp + T(10.0) * bc + bm) / T(12.0);
+        const T a = S.tA[k - p0];
+        q = S.tG[k - p0] * mb + a * q;
+        A *= a;
+        Cl[(k + rb) * PITCH] = q;
+        bm = bc;
+        bc = bp;
+      }
+    }
+    S.aggA[c * LPG + ln] = A;
+    S.aggF[c * LPG + ln] = q;
+  }
+  __syncthreads();
+
+  // ---- phase 3: forward carries (CTA prefix, then cluster prefix) ----
+  {
+    T PA = T(1), PB = T(0);  // composite of chunks 0..c-1
+    for (int j = 0; j < c; ++j) {
+      T a = S.aggA[j * LPG + ln], b = S.aggF[j * LPG + ln];
+      PB = a * PB + b;
+      PA = a * PA;
+    }
+    T cin = T(0);
+    if (cs > 1) {
+      T *xA = S.xch, *xB = S.xch + LPG;
+      if (c == NCH - 1) {
+        T a = S.aggA[c * LPG + ln], b = S.aggF[c * LPG + ln];
+        xA[ln] = a * PA;
+        xB[ln] = a * PB + b;
+      }
+      cluster.sync();
+      for (int r = 0; r < rank; ++r) {
+        const T *ra = cluster.map_shared_rank(xA, r);
+        const T *rbv = cluster.map_shared_rank(xB, r);
+        cin = ra[ln] * cin + rbv[ln];
+      }
+    }
+    const T carry = PA * cin + PB;
+    T P = T(1);
+    for (int k = s; k < e; ++k) {
+      P *= S.tA[k - p0];
+      Cl[(k + rb) * PITCH] += P * carry;
+    }
+    // ---- phase 4: local backward recurrence ----
+    T x = T(0);
+    for (int k = e - 1; k >= s; --k) {
+      x = Cl[(k + rb) * PITCH] + S.tA[k - p0] * x;
+      Cl[(k + rb) * PITCH] = x;
+    }
+    S.aggR[c * LPG + ln] = x;
+  }
+  __syncthreads();
+
+  // ---- phase 5: backward carries (CTA suffix, then cluster suffix) ----
+  {
+    T SA = T(1), SB = T(0);  // composite of chunks NCH-1 .. c+1
+    for (int j = NCH - 1; j > c; --j) {
+      T a = S.aggA[j * LPG + ln], b = S.aggR[j * LPG + ln];
+      SB = b + a * SB;
+      SA = a * SA;
+    }
+    T cin = T(0);
+    if (cs > 1) {
+      T *xA = S.xch + 2 * LPG, *xB = S.xch + 3 * LPG;
+      if (c == 0) {
+        T a = S.aggA[ln], b = S.aggR[ln];
+        xA[ln] = a * SA;
+        xB[ln] = b + a * SB;
+      }
+      cluster.sync();
+      for (int r = cs - 1; r > rank; --r) {
+        const T *ra = cluster.map_shared_rank(xA, r);
+        const T *rbv = cluster.map_shared_rank(xB, r);
+        cin = rbv[ln] + ra[ln] * cin;
+      }
+    }
+    const T carry = SB + SA * cin;
+    T P = T(1);
+    for (int k = e - 1; k >= s; --k) {
+      P *= S.tA[k - p0];
+      Cl[(k + rb) * PITCH] += P * carry;
+    }
+  }
+
+  // ---- phase 6: periodic rank-one (Sherman-Morrison) correction ----
+  if (periodic) {
+    T *y0 = S.xch + 4 * LPG, *yL = S.xch + 5 * LPG;
+    __syncthreads();
+    if (rank == 0 && threadIdx.x < LPG) y0[threadIdx.x] = qArr[(H)*PITCH + threadIdx.x];
+    if (rank == cs - 1 && threadIdx.x < LPG) yL[threadIdx.x] = qArr[(H + np - 1) * PITCH + threadIdx.x];
+    T a0, aL;
+    if (cs > 1) {
+      cluster.sync();
+      a0 = cluster.map_shared_rank(y0, 0)[ln];
+      aL = cluster.map_shared_rank(yL, cs - 1)[ln];
+    } else {
+      __syncthreads();
+      a0 = y0[ln];
+      aL = yL[ln];
+    }
+    const T fct = (a0 + T(F.sm_fac) * aL) * T(F.sm_inv_den);
+    for (int k = s; k < e; ++k) Cl[(k + rb) * PITCH] -= fct * S.tZ[k - p0];
+  }
+  __syncthreads();
+
+  // ---- phase 7: store ----
+  {
+    const int total = np * LPG;
+    const bool xs = (F.s_line == 1);
+    for (int q = threadIdx.x; q < total; q += NTH) {
+      int row, l2;
+      if (xs) { row = q / LPG; l2 = q - row * LPG; }
+      else { l2 = q / np; row = q - l2 * np; }
+      long long gl2 = line0 + l2;
+      if (gl2 < F.M)
+        gdata[(long long)(p0 + row) * F.s_pos + gl2 * F.s_line] = qArr[(row + H) * PITCH + l2];
+    }
+  }
+  if (cs > 1) cluster.sync();  // keep shared memory alive for remote readers
+}
+
+}  // namespace
+
+size_t sweep_smem_bytes(int lc_max, int halo, bool fp64) {
+  size_t el = fp64 ? 8 : 4;
+  size_t n = 2 * (size_t)(lc_max + 2 * halo) * PITCH +
+             3 * (size_t)lc_max + 3 * (size_t)NCH * LPG + 8 * (size_t)LPG;
+  return ((sizeof(SweepField) + 15) & ~size_t(15)) + n * el;
+}
+
+template <typename T>
+cudaError_t launch_sweep(const SweepField *d_fields, int nfields, int group_base,
+                         int groups_total, int cs, int lc_max, int halo, double toff, void *data,
+                         unsigned *d_status, cudaStream_t stream) {
+  const size_t smem = sweep_smem_bytes(lc_max, halo, sizeof(T) == 8);
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t err = cudaFuncSetAttribute(sweep_kernel<T>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (err != cudaSuccess) return err;
+    err = cudaFuncSetAttribute(sweep_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (err != cudaSuccess) return err;
+    configured = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(groups_total * cs), 1, 1);
+  cfg.blockDim = dim3(NTH, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  count_launch();
+  return cudaLaunchKernelEx(&cfg, sweep_kernel<T>, d_fields, nfields, group_base, toff, data,
+                            lc_max, halo, d_status);
+}
+
+template cudaError_t launch_sweep<double>(const SweepField *, int, int, int, int, int, int,
+                                          double, void *, unsigned *, cudaStream_t);
+template cudaError_t launch_sweep<float>(const SweepField *, int, int, int, int, int, int,
+                                         double, void *, unsigned *, cudaStream_t);
+
+}  // namespace ccfv

@@ -1,0 +1,62 @@
+"""Parareal engine through the C ABI against the oracle, the reference's
+golden Parareal run and the serial fine solve."""
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import periodic_field, rel_l2
+
+pytestmark = pytest.mark.gpu
+THREADS = min(32, os.cpu_count() or 1)
+
+
+def dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+def test_reference_schedule_matches_golden(ccfv):
+    """40 slices, 1 coarse step per slice, 3 fixed iterations, FP64 STANDARD:
+    the reference's own Parareal run (T2S4_Parareal.cu:1249-1355)."""
+    z = np.load(Path(__file__).parent / "golden" / "parareal_N24.npz")
+    meta = json.loads(str(z["meta"]))
+    s = ccfv.Solver(ccfv.make_grid(meta["N"], K=meta["K"]))
+    UT, st = s.parareal(z["C0"], t0=meta["T_min"], t1=meta["T_max"], nt_fine=meta["Nt"],
+                        n_slices=meta["n_slices"], kmax=meta["kmax"])
+    assert st["iterations"] == meta["kmax"]
+    assert rel_l2(UT, z["UT"]) < 1e-12
+    assert abs(np.abs(UT - z["uref"]).max() - z["err"][-1]) < 1e-12 * np.abs(z["uref"]).max()
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_parareal_matches_oracle(oracle, ccfv, form):
+    N, T, nt, S, ratio = 40, 0.25, 96, 12, 4
+    vp = (2 * np.pi, 0.5, 0.5)
+    C0 = periodic_field(N, 6)
+    g = oracle.grid(N, bc=1, vel=2, vp=vp, K=1e-3, threads=THREADS, scheme=1)
+    ref, it_o, upd_o = oracle.parareal(g, C0, t0=0.0, t1=T, nt_fine=nt, n_slices=S,
+                                       coarse_steps=(nt // S) // ratio, tol=0.0, kmax=4, form=form)
+    s = ccfv.Solver(ccfv.make_grid(N, bc=1, velocity=2, vel_params=vp, K=1e-3, scheme=1))
+    UT, st = s.parareal(dev(C0), t0=0.0, t1=T, nt_fine=nt, n_slices=S, coarse_ratio=ratio,
+                        tol=0.0, kmax=4, form=form)
+    assert rel_l2(UT.cpu().numpy(), ref) < 1e-12
+    np.testing.assert_allclose(st["update"], upd_o, rtol=1e-6)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_parareal_converges_to_serial_fine(oracle, ccfv, prec):
+    """Converged Parareal (FP64 or FP32 coarse) equals the serial fine
+    solve within its tolerance."""
+    N, T, nt, S, ratio, tol = 128, 1.0, 512, 16, 4, 1e-10
+    vp = (2 * np.pi, 0.5, 0.5)
+    den = 2 * 0.05 ** 2  # Gaussian hump, sigma 0.05 at (0.5, 0.75), one revolution
+    C0 = oracle.gaussians(oracle.grid(N, bc=1), [0.5], [0.75], [den], [1.0], img=1)
+    s = ccfv.Solver(ccfv.make_grid(N, bc=1, velocity=2, vel_params=vp, K=1e-3, scheme=1))
+    fine = s.run(C0, 0.0, T / nt, nt)
+    UT, st = s.parareal(dev(C0), t0=0.0, t1=T, nt_fine=nt, n_slices=S, coarse_ratio=ratio,
+                        tol=tol, kmax=S, coarse_precision=prec, form=ccfv.FORM_DELTA)
+    assert st["converged"], st
+    assert rel_l2(UT.cpu().numpy(), fine) < 10 * tol, st

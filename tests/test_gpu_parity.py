@@ -1,0 +1,152 @@
+"""CUDA path (through the C ABI) against the reference's golden vectors and
+the oracle.  Parity bar: 1e-12 relative L2 for FP64 (the oracle itself
+agrees with the reference binary to ~1e-13)."""
+import glob
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import periodic_field, rel_l2, seeded_field
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+THREADS = min(32, os.cpu_count() or 1)
+GOLDEN = sorted(glob.glob(str(Path(__file__).parent / "golden" / "*.npz")))
+
+
+def _load(f):
+    z = np.load(f)
+    return json.loads(str(z["meta"])), z
+
+
+def dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+@pytest.mark.parametrize("f", [g for g in GOLDEN if _load(g)[0]["kind"] in ("run", "ic_run")],
+                         ids=lambda p: Path(p).stem)
+def test_cuda_matches_reference_golden(ccfv, f):
+    """GpuOneStep through the reference-shaped binding, on the reference's
+    own outputs."""
+    meta, z = _load(f)
+    ctx = ccfv.GPUContext(meta["N"], K=meta["K"])
+    ctx.v_d_Cn.copy_(dev(z["C0"]))
+    for n in range(meta["nsteps"]):
+        ccfv.GpuOneStep(ctx, meta["t0"] + n * meta["dt"], meta["dt"])
+    ctx.solver.check()
+    assert rel_l2(host(ctx.v_d_Cn), z["out"]) < TOL
+
+
+def _compat_case(oracle, ccfv, nx, ny, K, dt, nsteps, seed, scheme=0):
+    C0 = seeded_field(nx, seed, ny=ny)
+    g = oracle.grid(nx, ny, K=K, threads=THREADS, scheme=scheme)
+    ref = oracle.run(g, C0, 0.0, dt, nsteps)
+    s = ccfv.Solver(ccfv.make_grid(nx, ny, K=K, scheme=scheme))
+    c = dev(C0)
+    s.run(c, 0.0, dt, nsteps)
+    s.check()
+    return host(c), ref
+
+
+@pytest.mark.parametrize("nx,ny", [(4, 4), (5, 9), (37, 37), (100, 60), (256, 256), (257, 257),
+                                   (300, 301), (600, 520), (1024, 1024)])
+def test_compat_matches_oracle_sizes(oracle, ccfv, nx, ny):
+    """Ragged sizes, tile tails (M % 16), cluster sizes 1..4."""
+    dx = 2.0 / max(nx, ny)
+    out, ref = _compat_case(oracle, ccfv, nx, ny, 1e-3, 0.1 * dx, 3, nx + ny)
+    assert rel_l2(out, ref) < TOL
+
+
+@pytest.mark.parametrize("N", [2048, 4096])
+def test_compat_matches_oracle_cluster_8_16(oracle, ccfv, N):
+    """Cluster sizes 8 and 16 (non-portable) for the longest lines."""
+    out, ref = _compat_case(oracle, ccfv, N, N, 1e-4, 0.2 / N, 1, 11)
+    assert rel_l2(out, ref) < TOL
+
+
+@pytest.mark.parametrize("scheme", [0, 1])
+@pytest.mark.parametrize("K,cfl", [(0.0, 0.5), (0.05, 0.5), (0.02, 3.3), (1.0, 1.0)])
+def test_compat_diffusion_and_cfl(oracle, ccfv, scheme, K, cfl):
+    """Both schemes, zero / strong diffusion, feet several cells away."""
+    N = 64
+    dt = cfl * (2.0 / N) / 4.0
+    out, ref = _compat_case(oracle, ccfv, N, N, K, dt, 4, 7, scheme)
+    assert rel_l2(out, ref) < TOL
+
+
+PERIODIC = [
+    ("const", 1, (1.0, -0.6)),
+    ("rotation", 2, (2 * np.pi, 0.5, 0.5)),
+    ("swirl", 3, (1.5,)),
+    ("refrot", 0, ()),
+]
+
+
+@pytest.mark.parametrize("name,vel,vp", PERIODIC, ids=[p[0] for p in PERIODIC])
+@pytest.mark.parametrize("nx,ny", [(64, 64), (96, 80), (512, 512)])
+def test_periodic_matches_oracle(oracle, ccfv, name, vel, vp, nx, ny):
+    K = 1e-3
+    dt = 0.8 / max(nx, ny) / 3.2
+    C0 = periodic_field(nx, 9, ny=ny)
+    g = oracle.grid(nx, ny, bc=1, vel=vel, vp=vp, K=K, threads=THREADS, scheme=1)
+    ref = oracle.run(g, C0, 0.3, dt, 3)
+    s = ccfv.Solver(ccfv.make_grid(nx, ny, bc=1, velocity=vel, vel_params=vp, K=K, scheme=1))
+    c = dev(C0)
+    s.run(c, 0.3, dt, 3)
+    s.check()
+    assert rel_l2(host(c), ref) < TOL
+
+
+def test_periodic_mass_conserved(oracle, ccfv):
+    N = 256
+    C0 = periodic_field(N, 4)
+    s = ccfv.Solver(ccfv.make_grid(N, bc=1, velocity=2, vel_params=(2 * np.pi, 0.5, 0.5),
+                                   K=1e-3, scheme=1))
+    c = dev(C0)
+    s.run(c, 0.0, 0.8 / N / np.pi, 64)
+    m0, m1 = oracle.sum_kahan(C0), oracle.sum_kahan(host(c))
+    assert abs(m1 - m0) / abs(m0) < 1e-13
+
+
+def test_propagators_match_oracle(oracle, ccfv):
+    N, K, tn, DT = 48, 2e-3, 0.05, 0.04
+    C0 = seeded_field(N, 3)
+    g = oracle.grid(N, K=K)
+    ctx = ccfv.GPUContext(N, K=K)
+    ctx.v_d_Cn.copy_(dev(C0))
+    ccfv.FinePropagator(ctx, tn, DT, 5)
+    assert rel_l2(host(ctx.v_d_Cn), oracle.fine(g, C0, tn, DT, 5)) < TOL
+    ctx.v_d_Cn.copy_(dev(C0))
+    ccfv.CoarsePropagator(ctx, tn, DT)
+    assert rel_l2(host(ctx.v_d_Cn), oracle.coarse(g, C0, tn, DT, 1)) < TOL
+    c = dev(C0)
+    ctx.solver.coarse(c, tn, DT, 3)
+    assert rel_l2(host(c), oracle.coarse(g, C0, tn, DT, 3)) < TOL
+
+
+def test_fp32_coarse_close_to_fp64(ccfv):
+    N = 128
+    C0 = periodic_field(N, 2)
+    s = ccfv.Solver(ccfv.make_grid(N, bc=1, velocity=3, vel_params=(1.5,), K=1e-3, scheme=1))
+    a, b = dev(C0), dev(C0)
+    s.coarse(a, 0.0, 0.05, 4, ccfv.FP64)
+    s.coarse(b, 0.0, 0.05, 4, ccfv.FP32)
+    assert rel_l2(host(b), host(a)) < 2e-6
+
+
+def test_host_memory_run_matches_device(ccfv):
+    N = 80
+    C0 = seeded_field(N, 8)
+    s = ccfv.Solver(ccfv.make_grid(N, K=1e-3))
+    out_h = s.run(C0, 0.0, 0.002, 5)
+    c = dev(C0)
+    s.run(c, 0.0, 0.002, 5)
+    assert np.array_equal(out_h, host(c))
