@@ -60,8 +60,14 @@ struct SweepField {
   const void *tab;         // T[3L]: alpha_k | g_k | z_k (solver factors)
 };
 
-// Shared-memory bytes of the sweep kernel for a launch.
+// Kernel variants: the per-cell kernel (any velocity / boundary / scheme) and
+// the fused stencil kernel (uniform displacement, periodic, derivative of the
+// sweep input).
+enum { SWEEP_GENERAL = 0, SWEEP_FAST = 1 };
+
+// Shared-memory bytes of the sweep kernels for a launch.
 size_t sweep_smem_bytes(int lc_max, int halo, bool fp64);
+size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64);
 
 // Launches one fused sweep over all fields of `d_fields` (device array,
 // sorted by group0; tiles group_base .. group_base+groups_total-1).  All fields share the cluster size `cs`, their
@@ -69,7 +75,7 @@ size_t sweep_smem_bytes(int lc_max, int halo, bool fp64);
 // every field's ta_rel/tb_rel (the launch time); `data` (if non-null)
 // replaces fields[0].data (single-field launches).
 template <typename T>
-cudaError_t launch_sweep(const SweepField *d_fields, int nfields, int group_base,
+cudaError_t launch_sweep(int variant, const SweepField *d_fields, int nfields, int group_base,
                          int groups_total, int cs, int lc_max, int halo, double toff, void *data,
                          unsigned *d_status, cudaStream_t stream);
 

@@ -213,9 +213,14 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
     const SolverTable *tab = get_table(ctx, dir, Dt, fp64, &st);
     if (!tab) return st;
     LaunchGeom G = geom_for(g, dir, Dt, dsrc);
+    const bool uniform = g.velocity == CCFV_VEL_REF_ROT4 || g.velocity == CCFV_VEL_CONST ||
+                         g.velocity == CCFV_VEL_ROTATION;
+    G.variant = (uniform && g.bc == CCFV_BC_PERIODIC && dsrc == 0 && !ctx->force_general)
+                    ? SWEEP_FAST : SWEEP_GENERAL;
     if (G.cs > MAX_CLUSTER)
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
-    if (sweep_smem_bytes(G.lc_max, G.halo, fp64) > 227 * 1024)
+    if (std::max(sweep_smem_bytes(G.lc_max, G.halo, fp64),
+                 sweep_fast_smem_bytes(G.lc_max, G.halo, fp64)) > 227 * 1024)
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
     for (int i = 0; i < nf; ++i) {
       SweepField f = make_field(g, dir, Dt, ta + fields[i].second, tb + fields[i].second,
@@ -241,10 +246,10 @@ int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int
     const int gpf = plan.groups_per_field[kind];
     const SweepField *fk = base + (size_t)kind * plan.nf;
     cudaError_t e =
-        fp64 ? launch_sweep<double>(fk, plan.nf, first * gpf, count * gpf, G.cs, G.lc_max,
-                                    G.halo, toff, data_override, status, st)
-             : launch_sweep<float>(fk, plan.nf, first * gpf, count * gpf, G.cs, G.lc_max, G.halo,
-                                   toff, data_override, status, st);
+        fp64 ? launch_sweep<double>(G.variant, fk, plan.nf, first * gpf, count * gpf, G.cs,
+                                    G.lc_max, G.halo, toff, data_override, status, st)
+             : launch_sweep<float>(G.variant, fk, plan.nf, first * gpf, count * gpf, G.cs,
+                                   G.lc_max, G.halo, toff, data_override, status, st);
     CK(e);
   }
   return CCFV_OK;

@@ -35,7 +35,7 @@ struct SolverTable {
 
 // Launch geometry shared by all fields of one sweep launch.
 struct LaunchGeom {
-  int cs = 1, lc_max = 0, halo = 0, groups = 0;
+  int cs = 1, lc_max = 0, halo = 0, groups = 0, variant = 0;
 };
 
 // Three sweep launches (x dt/2, y dt, x dt/2) of one step over a set of fields.
@@ -61,6 +61,7 @@ struct ccfv_ctx {
   double fine_plan_key[4] = {0, 0, 0, 0};
   int fine_plan_slices = 0;
   std::string last_error;
+  bool force_general = false;  // test hook: route every sweep through the per-cell kernel
 };
 
 namespace ccfv {

@@ -273,7 +273,7 @@ __device__ __forceinline__ Smem<T> carve(unsigned char *raw, int lc_max, int H) 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(NTH) sweep_kernel(const SweepField *__restrict__ fields,
+__global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restrict__ fields,
                                                     int nfields, int group_base, double toff,
                                                     void *data_override, int lc_max, int H,
                                                     unsigned *status) {
@@ -622,6 +622,312 @@ __global__ void __launch_bounds__(NTH) sweep_kernel(const SweepField *__restrict
   if (cs > 1) cluster.sync();  // keep shared memory alive for remote readers
 }
 
+
+// ---------------------------------------------------------------------------
+// Fast path: uniform displacement + periodic cells, derivative of the input.
+// Every cell of a line uses the same 6-tap RHS stencil, so phase 1 and the
+// forward recurrence fuse into one walk with a sliding register window (one
+// shared-memory read per cell).  The chunk prefix / suffix products of
+// alpha_k are line-invariant and kept once per chunk, which lets the forward
+// fix-up and the backward recurrence fuse into a single reverse walk, and the
+// backward fix-up, the Sherman-Morrison correction and the store into a final
+// walk.
+
+__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *sdst, const void *gsrc) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Stage rows p0-H .. p1+H-1 of LPG lines into Cs[row][line] with cp.async
+// (wrapped positions for periodic lines, zeros elsewhere).
+template <typename T>
+__device__ __forceinline__ void stage_async(const SweepField &F, T *Cs, int p0, int np, int H,
+                                            long long line0) {
+  const int nrows = np + 2 * H;
+  const int total = nrows * LPG;
+  const int L = F.L;
+  const bool xs = (F.s_line == 1);
+  const T *gdata = reinterpret_cast<const T *>(F.data);
+  for (int e = threadIdx.x; e < total; e += NTH) {
+    int row, ln;
+    if (xs) { row = e / LPG; ln = e - row * LPG; }
+    else { ln = e / nrows; row = e - ln * nrows; }
+    int pos = p0 - H + row;
+    const long long gl = line0 + ln;
+    T *dst = Cs + row * PITCH + ln;
+    if (gl < F.M) {
+      if (pos < 0 || pos >= L) { pos %= L; if (pos < 0) pos += L; }
+      const T *src = gdata + (long long)pos * F.s_pos + gl * F.s_line;
+      if (sizeof(T) == 8) cp_async8(dst, src); else cp_async4(dst, src);
+    } else {
+      *dst = T(0);
+    }
+  }
+  cp_async_wait_all();
+}
+
+template <typename T>
+struct FastSmem {
+  T *C;      // [(lc_max + 2H) * PITCH]
+  T *Q;      // [lc_max * PITCH]   q, then x (row = position - p0)
+  T *tA, *tG, *tZ, *tP, *tS;  // [lc_max] factors, chunk prefix/suffix products
+  T *aggA;   // [NCH]        chunk products (line-invariant)
+  T *aggF;   // [NCH * LPG]  chunk forward values
+  T *aggR;   // [NCH * LPG]  chunk backward values
+  T *xch;    // [8 * LPG]    cluster exchange
+  SweepField *fd;
+};
+
+template <typename T>
+__device__ __forceinline__ FastSmem<T> carve_fast(unsigned char *raw, int lc_max, int H) {
+  FastSmem<T> s;
+  s.fd = reinterpret_cast<SweepField *>(raw);
+  T *p = reinterpret_cast<T *>(raw + ((sizeof(SweepField) + 15) & ~size_t(15)));
+  s.C = p; p += (lc_max + 2 * H) * PITCH;
+  s.Q = p; p += lc_max * PITCH;
+  s.tA = p; p += lc_max;
+  s.tG = p; p += lc_max;
+  s.tZ = p; p += lc_max;
+  s.tP = p; p += lc_max;
+  s.tS = p; p += lc_max;
+  s.aggA = p; p += NCH;
+  s.aggF = p; p += NCH * LPG;
+  s.aggR = p; p += NCH * LPG;
+  s.xch = p;
+  return s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NTH, 2)
+    sweep_fast_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
+                      double toff, void *data_override, int lc_max, int H, unsigned *status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int cs = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  const int tile = blockIdx.x / cs + group_base;
+  FastSmem<T> S = carve_fast<T>(smem_raw, lc_max, H);
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = nfields - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (fields[mid].group0 <= tile) lo = mid; else hi = mid - 1;
+    }
+    *S.fd = fields[lo];
+    if (data_override) S.fd->data = data_override;
+  }
+  __syncthreads();
+  const SweepField &F = *S.fd;
+  const int L = F.L;
+  const long long line0 = (long long)(tile - F.group0) * LPG;
+  const int Lc = (L + cs - 1) / cs;
+  const int p0 = min(L, rank * Lc);
+  const int p1 = min(L, p0 + Lc);
+  const int np = p1 - p0;
+  const int nrows = np + 2 * H;
+
+  stage_async(F, S.C, p0, np, H, line0);
+  {
+    const T *tab = reinterpret_cast<const T *>(F.tab);
+    for (int k = threadIdx.x; k < np; k += NTH) {
+      S.tA[k] = tab[p0 + k];
+      S.tG[k] = tab[L + p0 + k];
+      S.tZ[k] = tab[2 * L + p0 + k];
+    }
+  }
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ln = lane % LPG;
+  const int c = warp * CPW + lane / LPG;
+  const long long gl = line0 + ln;
+  const int m = (np + NCH - 1) / NCH;
+  const int s = min(p1, p0 + c * m);
+  const int e = min(p1, s + m);
+
+  // per-line stencil: b_k = sum_t om_t C_{k+n0+t}, t = -2..3
+  T om[6];
+  int n0;
+  {
+    const double tau0 = F.t_min + F.ht * (double)gl;
+    const double tau1 = F.t_min + F.ht * (double)(gl + 1);
+    const double f0 = edge_foot(F, 0, tau0, tau1, toff + F.ta_rel, toff + F.tb_rel);
+    const double u = (f0 - F.s_min) / F.h;
+    const double fl = floor(u);
+    n0 = (int)fl;
+    const double x = u - fl, x2 = x * x, x3 = x2 * x;
+    const double A = x - 2.0 * x2 + x3, B = x3 - x2, Cc = 3.0 * x2 - 2.0 * x3;
+    const double kq = F.kb * F.inv12h;
+    const double pm2 = 2.0 * x3 - 6.0 * x2 + 3.0 * x + 1.0;
+    const double pm1 = -8.0 * x3 + 18.0 * x2 + 6.0 * x - 15.0;
+    const double pz = 12.0 * x3 - 18.0 * x2 - 24.0 * x + 15.0;
+    const double pp1 = -8.0 * x3 + 6.0 * x2 + 18.0 * x - 1.0;
+    const double pp2 = 2.0 * x3 - 3.0 * x;
+    om[0] = T(A / 12.0 - kq * pm2);
+    om[1] = T((B - 8.0 * A) / 12.0 + kq * (pm2 - pm1));
+    om[2] = T(1.0 - Cc - 2.0 * B / 3.0 + kq * (pm1 - pz));
+    om[3] = T(Cc + 2.0 * A / 3.0 + kq * (pz - pp1));
+    om[4] = T((8.0 * B - A) / 12.0 + kq * (pp1 - pp2));
+    om[5] = T(-B / 12.0 + kq * pp2);
+  }
+
+  // ---- fused RHS + compact mass matrix + local forward recurrence ----
+  {
+    T A = T(1), q = T(0);
+    if (s < e) {
+      const int r0 = (s - 1) + n0 - 2 - p0 + H;   // row of tap -2 of cell s-1
+      const int rlast = e + n0 + 3 - p0 + H;       // row of tap +3 of cell e
+      if (r0 < 0 || rlast >= nrows) {
+        atomicOr(status, STATUS_HALO);
+      } else {
+        const T *cp = S.C + r0 * PITCH + ln;
+        T w0 = cp[0], w1 = cp[PITCH], w2 = cp[2 * PITCH], w3 = cp[3 * PITCH],
+          w4 = cp[4 * PITCH], w5 = cp[5 * PITCH];
+        auto bval = [&]() {
+          return om[0] * w0 + om[1] * w1 + om[2] * w2 + om[3] * w3 + om[4] * w4 + om[5] * w5;
+        };
+        T bm = bval();
+        w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[6 * PITCH];
+        T bc = bval();
+        const T *nxt = cp + 7 * PITCH;
+        T *qp = S.Q + (s - p0) * PITCH + ln;
+        for (int k = s; k < e; ++k) {
+          w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = *nxt;
+          nxt += PITCH;
+          const T bp = bval();
+          const T mb = (bp + T(10.0) * bc + bm) * T(1.0 / 12.0);
+          const T a = S.tA[k - p0];
+          q = S.tG[k - p0] * mb + a * q;
+          A *= a;
+          *qp = q;
+          qp += PITCH;
+          if (ln == 0) S.tP[k - p0] = A;
+          bm = bc;
+          bc = bp;
+        }
+      }
+    }
+    S.aggF[c * LPG + ln] = q;
+    if (ln == 0) S.aggA[c] = A;
+  }
+  __syncthreads();
+
+  // ---- forward carries ----
+  T carry;
+  {
+    T PA = T(1), PB = T(0);
+    for (int j = 0; j < c; ++j) {
+      const T a = S.aggA[j];
+      PB = a * PB + S.aggF[j * LPG + ln];
+      PA = a * PA;
+    }
+    T cin = T(0);
+    if (cs > 1) {
+      T *xA = S.xch, *xB = S.xch + LPG;
+      if (c == NCH - 1) {
+        const T a = S.aggA[c];
+        xA[ln] = a * PA;
+        xB[ln] = a * PB + S.aggF[c * LPG + ln];
+      }
+      cluster.sync();
+      for (int r = 0; r < rank; ++r) {
+        const T *ra = cluster.map_shared_rank(xA, r);
+        const T *rb = cluster.map_shared_rank(xB, r);
+        cin = ra[ln] * cin + rb[ln];
+      }
+    }
+    carry = PA * cin + PB;
+  }
+  // ---- fused forward fix-up + local backward recurrence (reverse walk) ----
+  {
+    T x = T(0), Sp = T(1);
+    T *qp = S.Q + (e - 1 - p0) * PITCH + ln;
+    for (int k = e - 1; k >= s; --k) {
+      const T a = S.tA[k - p0];
+      x = (*qp + S.tP[k - p0] * carry) + a * x;
+      *qp = x;
+      qp -= PITCH;
+      Sp *= a;
+      if (ln == 0) S.tS[k - p0] = Sp;
+    }
+    S.aggR[c * LPG + ln] = x;
+  }
+  __syncthreads();
+  // ---- backward carries ----
+  T carry2;
+  {
+    T SA = T(1), SB = T(0);
+    for (int j = NCH - 1; j > c; --j) {
+      const T a = S.aggA[j];
+      SB = S.aggR[j * LPG + ln] + a * SB;
+      SA = a * SA;
+    }
+    T cin = T(0);
+    if (cs > 1) {
+      T *xA = S.xch + 2 * LPG, *xB = S.xch + 3 * LPG;
+      if (c == 0) {
+        const T a = S.aggA[0];
+        xA[ln] = a * SA;
+        xB[ln] = S.aggR[ln] + a * SB;
+      }
+      cluster.sync();
+      for (int r = cs - 1; r > rank; --r) {
+        const T *ra = cluster.map_shared_rank(xA, r);
+        const T *rb = cluster.map_shared_rank(xB, r);
+        cin = rb[ln] + ra[ln] * cin;
+      }
+    }
+    carry2 = SB + SA * cin;
+  }
+  // ---- cyclic correction (Sherman-Morrison): needs y_0 and y_{L-1} ----
+  T fct;
+  {
+    T *y0 = S.xch + 4 * LPG, *yL = S.xch + 5 * LPG;
+    if (p0 == 0 && s == p0 && s < e) y0[ln] = S.Q[ln] + S.tS[0] * carry2;
+    if (p1 == L && e == p1 && s < e) yL[ln] = S.Q[(np - 1) * PITCH + ln] + S.tS[np - 1] * carry2;
+    T a0, aL;
+    if (cs > 1) {
+      cluster.sync();
+      a0 = cluster.map_shared_rank(y0, 0)[ln];
+      aL = cluster.map_shared_rank(yL, cs - 1)[ln];
+    } else {
+      __syncthreads();
+      a0 = y0[ln];
+      aL = yL[ln];
+    }
+    fct = (a0 + T(F.sm_fac) * aL) * T(F.sm_inv_den);
+  }
+  // ---- backward fix-up + correction + store ----
+  T *gdata = reinterpret_cast<T *>(F.data);
+  if (F.s_line == 1) {
+    // x-sweep: a half-warp writes 16 consecutive doubles of one row
+    if (gl < F.M)
+      for (int k = s; k < e; ++k)
+        gdata[(long long)k * F.s_pos + gl] =
+            S.Q[(k - p0) * PITCH + ln] + S.tS[k - p0] * carry2 - fct * S.tZ[k - p0];
+  } else {
+    for (int k = s; k < e; ++k) {
+      T *qp = S.Q + (k - p0) * PITCH + ln;
+      *qp = *qp + S.tS[k - p0] * carry2 - fct * S.tZ[k - p0];
+    }
+    __syncthreads();
+    const int total = np * LPG;
+    for (int q = threadIdx.x; q < total; q += NTH) {
+      const int l2 = q / np, row = q - l2 * np;
+      const long long gl2 = line0 + l2;
+      if (gl2 < F.M) gdata[gl2 * F.s_line + (long long)(p0 + row)] = S.Q[row * PITCH + l2];
+    }
+  }
+  if (cs > 1) cluster.sync();  // keep shared memory alive for remote readers
+}
+
 }  // namespace
 
 size_t sweep_smem_bytes(int lc_max, int halo, bool fp64) {
@@ -631,18 +937,29 @@ size_t sweep_smem_bytes(int lc_max, int halo, bool fp64) {
   return ((sizeof(SweepField) + 15) & ~size_t(15)) + n * el;
 }
 
+size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64) {
+  size_t el = fp64 ? 8 : 4;
+  size_t n = (size_t)(lc_max + 2 * halo) * PITCH + (size_t)lc_max * PITCH + 5 * (size_t)lc_max +
+             NCH + 2 * (size_t)NCH * LPG + 8 * (size_t)LPG;
+  return ((sizeof(SweepField) + 15) & ~size_t(15)) + n * el;
+}
+
 template <typename T>
-cudaError_t launch_sweep(const SweepField *d_fields, int nfields, int group_base,
+cudaError_t launch_sweep(int variant, const SweepField *d_fields, int nfields, int group_base,
                          int groups_total, int cs, int lc_max, int halo, double toff, void *data,
                          unsigned *d_status, cudaStream_t stream) {
-  const size_t smem = sweep_smem_bytes(lc_max, halo, sizeof(T) == 8);
+  const bool fast = (variant == SWEEP_FAST);
+  const size_t smem = fast ? sweep_fast_smem_bytes(lc_max, halo, sizeof(T) == 8)
+                           : sweep_smem_bytes(lc_max, halo, sizeof(T) == 8);
   static bool configured = false;
   if (!configured) {
-    cudaError_t err = cudaFuncSetAttribute(sweep_kernel<T>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    if (err != cudaSuccess) return err;
-    err = cudaFuncSetAttribute(sweep_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (err != cudaSuccess) return err;
+    for (const void *fn : {(const void *)sweep_kernel<T>, (const void *)sweep_fast_kernel<T>}) {
+      cudaError_t err =
+          cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+      if (err != cudaSuccess) return err;
+      err = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      if (err != cudaSuccess) return err;
+    }
     configured = true;
   }
   cudaLaunchConfig_t cfg = {};
@@ -658,13 +975,16 @@ cudaError_t launch_sweep(const SweepField *d_fields, int nfields, int group_base
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   count_launch();
+  if (fast)
+    return cudaLaunchKernelEx(&cfg, sweep_fast_kernel<T>, d_fields, nfields, group_base, toff,
+                              data, lc_max, halo, d_status);
   return cudaLaunchKernelEx(&cfg, sweep_kernel<T>, d_fields, nfields, group_base, toff, data,
                             lc_max, halo, d_status);
 }
 
-template cudaError_t launch_sweep<double>(const SweepField *, int, int, int, int, int, int,
+template cudaError_t launch_sweep<double>(int, const SweepField *, int, int, int, int, int, int,
                                           double, void *, unsigned *, cudaStream_t);
-template cudaError_t launch_sweep<float>(const SweepField *, int, int, int, int, int, int,
+template cudaError_t launch_sweep<float>(int, const SweepField *, int, int, int, int, int, int,
                                          double, void *, unsigned *, cudaStream_t);
 
 }  // namespace ccfv
