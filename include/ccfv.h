@@ -162,6 +162,20 @@ typedef struct ccfv_stats {
 int ccfv_parareal(ccfv_ctx *ctx, const ccfv_parareal_opts *opts, const double *C0, double *C_T,
                   ccfv_stats *stats, void *stream);
 
+/* ---- allocation-free step ---------------------------------------------- */
+/* One split step like ccfv_step, for callers that cannot allocate device
+ * memory (inside another framework's memory pool, services that forbid
+ * allocation after start-up, hosts that budget device memory up front).  No
+ * counterpart in the reference.  Needs no context and calls no cudaMalloc,
+ * cudaFree or allocating library routine: its scratch (solver factors, sweep
+ * descriptors, status word) is a fixed file-scope device array of about
+ * 200 KB that every GPU loading the library holds until exit.  Limit:
+ * nx, ny <= 4096, else CCFV_ERR_UNSUPPORTED.  The first call on a device
+ * looks up the array's address with that device current: make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race.  Synchronises `stream` before returning. */
+int ccfv_step_noalloc(const ccfv_grid *grid, double *d_C, double tn, double dt, void *stream);
+
 /* ---- library info ---------------------------------------------------- */
 /* Number of kernels this library launched since load (all contexts). */
 uint64_t ccfv_kernel_launches(void);

@@ -97,6 +97,8 @@ _SIGS = {
                                 C.POINTER(Stats), C.c_void_p]),
     "ccfv_kernel_launches": (C.c_uint64, []),
     "ccfv_last_error": (C.c_char_p, [C.c_void_p]),
+    "ccfv_step_noalloc": (C.c_int, [C.POINTER(Grid), C.c_void_p, C.c_double, C.c_double,
+                                    C.c_void_p]),
 }
 
 
