@@ -54,6 +54,15 @@ def parse():
     ap.add_argument("--form", default="delta", choices=["standard", "delta"])
     ap.add_argument("--cpu-sample-s", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve"],
+                    help="plain: one instance (default workload); batch: a mixed batch of "
+                         "instances in shared launches; serve: Poisson arrivals through the "
+                         "continuous-batching server")
+    ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=20261206)
+    ap.add_argument("--plain-sample", type=int, default=24,
+                    help="instances solved one at a time (FP64 coarse) for the plain rate")
     return ap.parse_args()
 
 
@@ -71,26 +80,15 @@ def workload_name(w, a):
             f"form), Parareal to relative update < {w['tol']:g} (cap {w['kmax']})")
 
 
-def initial_field(w, device):
+def initial_field(w, solver, device):
     """Cell averages (3x3 Simpson, as T2S4_Parareal.cu:118-140) of the
-    Gaussian hump with its periodic images; synthetic input data."""
+    Gaussian hump with its periodic images, computed on the device by
+    ccfv_gaussians; synthetic input data."""
     import torch
     N = w["N"]
-    h = 1.0 / N
-    den = 2.0 * w["sigma"] ** 2
-    x = (torch.arange(N, dtype=torch.float64, device=device) + 0.5) * h
-    X, Y = torch.meshgrid(x, x, indexing="ij")
-    acc = torch.zeros_like(X)
-    wts = {-1: 1.0, 0: 4.0, 1: 1.0}
-    for dxs in (-1, 0, 1):
-        for dys in (-1, 0, 1):
-            wgt = wts[dxs] * wts[dys]
-            px, py = X + 0.5 * h * dxs, Y + 0.5 * h * dys
-            for ix in (-1, 0, 1):
-                for iy in (-1, 0, 1):
-                    acc += wgt * torch.exp(-((px - w["hump"][0] + ix) ** 2 +
-                                             (py - w["hump"][1] + iy) ** 2) / den)
-    return (acc / 36.0).contiguous()
+    C = torch.empty(N, N, dtype=torch.float64, device=device)
+    solver.gaussians(C, [[w["hump"][0], w["hump"][1], 2.0 * w["sigma"] ** 2, 1.0]], images=1)
+    return C
 
 
 class ClockSampler:
@@ -315,7 +313,7 @@ def run_ours(a, w, ws, rank, local):
                           vel_params=(w["omega"], *w["center"]), K=w["nu"],
                           scheme=ccfv.SCHEME_CONSISTENT)
     solver = ccfv.Solver(grid, local)
-    C0 = initial_field(w, dev)
+    C0 = initial_field(w, solver, dev)
     out = torch.empty_like(C0)
     prec = ccfv.FP32 if a.coarse == "fp32" else ccfv.FP64
     form = ccfv.FORM_DELTA if a.form == "delta" else ccfv.FORM_STANDARD
@@ -420,6 +418,189 @@ def run_ours(a, w, ws, rank, local):
         print(json.dumps(line))
 
 
+def batch_problems(a, rng, n, nmin=64, nmax=1024, mixed_velocity=False):
+    """Mixed instances: N log-uniform, velocity, diffusivity log-uniform, 1-8
+    Gaussians, T = 1, slices scaled with N, coarse dt = 8 x fine, FP32 coarse
+    (synthetic, seeded)."""
+    import ccfv
+    probs = []
+    for _ in range(n):
+        N = int(round(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))
+        T = 1.0
+        if mixed_velocity:
+            kind = int(rng.integers(0, 3))
+            nu = float(np.exp(rng.uniform(np.log(1e-4), np.log(1e-2))))
+            T = float(rng.uniform(0.25, 2.0))
+            tol = float(rng.choice([1e-8, 1e-10]))
+        else:
+            kind = 0
+            nu = float(np.exp(rng.uniform(np.log(1e-4), np.log(1e-1))))
+            tol = 1e-10
+        if kind == 0:
+            V = rng.uniform(-2, 2, 2)
+            vel, vp, vmax = ccfv.VEL_CONST, (float(V[0]), float(V[1])), float(np.abs(V).max())
+        elif kind == 1:
+            vel, vp, vmax = ccfv.VEL_ROTATION, (2 * np.pi, 0.5, 0.5), np.pi
+        else:
+            vel, vp, vmax = ccfv.VEL_SWIRL, (T,), 1.0
+        S = int(min(64, max(16, 16 * 2 ** round(np.log2(N / 64)))))
+        ratio = 8
+        dt = 0.8 / (N * max(vmax, 1e-3))
+        nt = int(np.ceil(T / dt / (S * ratio))) * S * ratio
+        ng = int(rng.integers(1, 9))
+        par = [[float(rng.uniform(0.2, 0.8)), float(rng.uniform(0.2, 0.8)),
+                2.0 * float(rng.uniform(0.03, 0.1)) ** 2, float(rng.uniform(0.5, 1.0))]
+               for _ in range(ng)]
+        g = ccfv.make_grid(N, bc=ccfv.BC_PERIODIC, velocity=vel, vel_params=vp, K=nu,
+                           scheme=ccfv.SCHEME_CONSISTENT)
+        probs.append(dict(grid=g, gauss=par, t0=0.0, t1=T, nt_fine=nt, n_slices=S,
+                          coarse_ratio=ratio, tol=tol, kmax=S, coarse_precision=ccfv.FP32,
+                          form=ccfv.FORM_DELTA, N=N))
+    return probs
+
+
+def _fields(probs, device, host=False):
+    import torch
+    import ccfv
+    for p in probs:
+        s = ccfv.Solver(p["grid"], device)
+        C0 = torch.empty(p["N"], p["N"], dtype=torch.float64, device=f"cuda:{device}")
+        s.gaussians(C0, p["gauss"], images=1)
+        if host:
+            p["C0"] = C0.cpu().numpy()
+            p["C_T"] = np.empty_like(p["C0"])
+        else:
+            p["C0"] = C0
+            p["C_T"] = torch.empty_like(C0)
+        s.close()
+
+
+def plain_rate(probs, device):
+    """Plain single-instance FP64 form: each problem alone, FP64 coarse."""
+    import torch
+    import ccfv
+    cells, ms = 0.0, 0.0
+    for p in probs:
+        s = ccfv.Solver(p["grid"], device)
+        kw = {k: p[k] for k in ("t0", "t1", "nt_fine", "n_slices", "coarse_ratio", "tol", "kmax")}
+        s.parareal(p["C0"], p["C_T"], coarse_precision=ccfv.FP64, form=ccfv.FORM_DELTA, **kw)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        s.parareal(p["C0"], p["C_T"], coarse_precision=ccfv.FP64, form=ccfv.FORM_DELTA, **kw)
+        b.record()
+        torch.cuda.synchronize()
+        ms += a.elapsed_time(b)
+        cells += p["N"] ** 2 * p["nt_fine"]
+        s.close()
+    return cells / (ms * 1e-3)
+
+
+def run_batch(a, ws, rank, local):
+    import torch
+    import ccfv
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(a.seed + rank)
+    probs = batch_problems(a, rng, a.instances)
+    _fields(probs, local)
+    cells = sum(p["N"] ** 2 * p["nt_fine"] for p in probs)
+    for _ in range(a.warmup):
+        st = ccfv.batch_solve(probs, device=local)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = ccfv.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(a.steps):
+        st = ccfv.batch_solve(probs, device=local)
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = ccfv.kernel_launches() - l0
+    ck = clocks.stop()
+    ms = reduce_max(ev0.elapsed_time(ev1), ws)
+    value = ws * cells * a.steps / (ms * 1e-3)
+    sample = probs[:: max(1, len(probs) // a.plain_sample)][: a.plain_sample]
+    plain = plain_rate(sample, local) if rank == 0 else None
+    if rank == 0:
+        its = [x["iterations"] for x in st]
+        conv = sum(1 for x in st if x["converged"])
+        print(json.dumps(dict(
+            metric="parareal_cell_updates_per_s", value=value, unit="cell-updates/s",
+            mode="batch", n_gpus=ws, steps=a.steps, warmup=a.warmup,
+            ms_per_step=ms / a.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
+            dtype="f64", data="synthetic",
+            config={"workload": f"{a.instances} periodic instances per GPU, N log-uniform "
+                                "64..1024, constant velocity U[-2,2]^2, nu log-uniform "
+                                "1e-4..1e-1, 1-8 Gaussians, T=1, fine dt at CFL 0.8, 16-64 "
+                                "slices, coarse dt = 8 x fine, FP32 coarse / FP64 fine, "
+                                "tol 1e-10 (cap = slices)", "seed": a.seed},
+            iterations_mean=float(np.mean(its)), converged=conv, instances=len(st),
+            plain_fp64_single_instance_cell_updates_per_s=plain,
+            batched_vs_plain=(value / ws / plain) if plain else None,
+            clocks=ck, gpu_launches=launches)))
+
+
+def run_serve(a, ws, rank, local):
+    import torch
+    import ccfv
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(a.seed + 1000 + rank)
+    probs = batch_problems(a, rng, a.requests, nmin=128, nmax=1024, mixed_velocity=True)
+    _fields(probs, local, host=True)
+    cells = [p["N"] ** 2 * p["nt_fine"] for p in probs]
+    budget = int(96e9)
+    # capacity: the same requests all at once (closed loop)
+    srv = ccfv.Server(budget, device=local)
+    t0 = time.perf_counter()
+    tk = [srv.submit(p) for p in probs]
+    for t in tk:
+        srv.wait(t)
+    cap = sum(cells) / (time.perf_counter() - t0)
+    srv.close()
+    # open loop: Poisson arrivals at 80% of capacity
+    rate = 0.8 * cap / float(np.mean(cells))
+    gaps = rng.exponential(1.0 / rate, len(probs))
+    srv = ccfv.Server(budget, device=local)
+    lat, tickets = [], []
+    t_start = time.perf_counter()
+    t_next = t_start
+    for p, gap in zip(probs, gaps):
+        t_next += gap
+        while time.perf_counter() < t_next:
+            time.sleep(0.0002)
+        tickets.append(srv.submit(p))
+    its = []
+    for t in tickets:
+        st, l_ms = srv.wait(t)
+        lat.append(l_ms)
+        its.append(st["iterations"])
+    span = time.perf_counter() - t_start
+    srv.close()
+    sample = probs[:: max(1, len(probs) // a.plain_sample)][: a.plain_sample]
+    for p in sample:
+        p["C0"] = torch.from_numpy(p["C0"]).cuda(local)
+        p["C_T"] = torch.empty_like(p["C0"])
+    plain = plain_rate(sample, local) if rank == 0 else None
+    if rank == 0:
+        value = sum(cells) / span
+        print(json.dumps(dict(
+            metric="parareal_cell_updates_per_s", value=value, unit="cell-updates/s",
+            mode="serve", n_gpus=ws, requests=len(probs), higher_is_better=True,
+            scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
+            config={"workload": f"{a.requests} requests, Poisson arrivals at 80% of measured "
+                                "capacity, N log-uniform 128..1024, velocity from {constant, "
+                                "rotation, swirl}, nu log-uniform 1e-4..1e-2, T U[0.25,2], "
+                                "tol in {1e-8,1e-10}, HBM budget 96 GB, FP32 coarse",
+                    "seed": a.seed},
+            latency_ms_p50=float(np.percentile(lat, 50)),
+            latency_ms_p99=float(np.percentile(lat, 99)),
+            capacity_cell_updates_per_s=cap, arrival_rate_per_s=rate,
+            iterations_mean=float(np.mean(its)),
+            plain_fp64_single_instance_cell_updates_per_s=plain,
+            served_vs_plain=(value / plain) if plain else None)))
+
+
 def main():
     a = parse()
     w = workload(a)
@@ -427,6 +608,10 @@ def main():
     try:
         if a.impl == "reference":
             run_reference(a, w, ws, rank)
+        elif a.mode == "batch":
+            run_batch(a, ws, rank, local)
+        elif a.mode == "serve":
+            run_serve(a, ws, rank, local)
         else:
             run_ours(a, w, ws, rank, local)
     finally:

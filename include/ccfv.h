@@ -137,6 +137,10 @@ typedef struct ccfv_parareal_opts {
   int form;            /* CCFV_FORM_STANDARD or CCFV_FORM_DELTA; FP32 coarse
                           requires DELTA                                    */
   int mem;             /* where C0 / C_T live: CCFV_MEM_DEVICE or _HOST      */
+  const double *d_ref; /* optional device field (e.g. the serial fine solution
+                          at t1): stats.err_* get ||U_k(t1) - ref|| after
+                          every iteration, the reference's diagnostic
+                          (T2S4_Parareal.cu:1333-1346); NULL = off          */
 } ccfv_parareal_opts;
 
 #define CCFV_MAX_ITERS 128
@@ -152,6 +156,8 @@ typedef struct ccfv_stats {
   double coarse_ms;                      /* device time of the G phases    */
   long long fine_sweep_launches;         /* sweep launches in the F phases */
   long long fine_sweep_cells;            /* cells swept in the F phases    */
+  double err_max[CCFV_MAX_ITERS];        /* max |U_k(t1) - d_ref| (d_ref)  */
+  double err_l2[CCFV_MAX_ITERS];         /* relative L2 of the same        */
 } ccfv_stats;
 
 /* Parareal solve of C0 over [t0,t1]; the final state goes to C_T.
@@ -162,6 +168,103 @@ typedef struct ccfv_stats {
 int ccfv_parareal(ccfv_ctx *ctx, const ccfv_parareal_opts *opts, const double *C0, double *C_T,
                   ccfv_stats *stats, void *stream);
 
+/* ---- Parareal building blocks (slice-distributed drivers) -------------- */
+/* FinePropagator (T2S4_Parareal.cu:977-984) on n contiguous fields at once:
+ * field i starts at t0 + i*slice_dt and takes J steps of DT/J; all fields
+ * advance in the same sweep launches.  Synchronises `stream`. */
+int ccfv_fine_slices(ccfv_ctx *ctx, double *d_fields, int n, double t0, double slice_dt,
+                     double DT, int J, void *stream);
+
+/* Parareal correction of one slice (parareal_correction_kernel,
+ * T2S4_Parareal.cu:771-782) fused with its update norms.
+ *   STANDARD: U <- W + (F - Gold), Gold <- W          (W = G(U+ of the previous slice))
+ *   DELTA:    U <- F + W,          W <- U_new - U_old  (W = G(increment))
+ * *sq_update = sum (U_new - U_old)^2, *sq_state = sum U_new^2.
+ * Synchronises `stream`. */
+int ccfv_correct(ccfv_ctx *ctx, int form, double *d_U, const double *d_F, double *d_Gold,
+                 double *d_W, double *sq_update, double *sq_state, void *stream);
+
+/* ---- batched solves ---------------------------------------------------- */
+/* One Parareal problem of a batch: its own grid, physics, options and
+ * initial / final fields (device or host memory per opts.mem). */
+typedef struct ccfv_problem {
+  ccfv_grid grid;
+  ccfv_parareal_opts opts;
+  const double *C0;
+  double *C_T;
+} ccfv_problem;
+
+/* Solves n independent Parareal problems of different sizes, velocities and
+ * diffusivities together on `device`: the fine propagators of every active
+ * slice of every problem advance in the same sweep launches, and the
+ * sequential coarse sweeps of all problems advance slice by slice in shared
+ * launches.  stats[i] (optional, n entries) receives problem i's iterations,
+ * updates and executed cell-updates; stats[i].ms is the batch's device time.
+ * No counterpart in the reference (one instance, one slice at a time). */
+int ccfv_batch_solve(int n, const ccfv_problem *problems, ccfv_stats *stats, int device,
+                     void *stream);
+
+/* ---- serving ----------------------------------------------------------- */
+/* A request loop with continuous batching: requests of different sizes are
+ * admitted in arrival order while their resident slice states fit
+ * hbm_budget_bytes (and max_active, if > 0); every epoch all resident
+ * requests advance by one Parareal iteration in shared launches, new
+ * requests join at the next epoch boundary, finished ones return their result
+ * to the caller's C_T and release their memory.  The caller keeps C0 / C_T
+ * alive until the request completes.  No counterpart in the reference. */
+typedef struct ccfv_server ccfv_server;
+
+typedef struct ccfv_server_opts {
+  int device;
+  size_t hbm_budget_bytes;  /* device memory for resident request states     */
+  int max_active;           /* max resident requests (0 = budget only)        */
+} ccfv_server_opts;
+
+enum ccfv_request_state {
+  CCFV_REQ_QUEUED = 0,
+  CCFV_REQ_RUNNING = 1,
+  CCFV_REQ_DONE = 2,
+  CCFV_REQ_FAILED = 3,
+  CCFV_REQ_CANCELLED = 4
+};
+
+int ccfv_server_create(ccfv_server **out, const ccfv_server_opts *opts);
+/* Queues a problem; CCFV_ERR_BUDGET if its states exceed the whole budget. */
+int ccfv_server_submit(ccfv_server *s, const ccfv_problem *problem, uint64_t *ticket);
+/* Non-blocking state query; stats / latency (submit to completion, ms) are
+ * filled once the request has completed. */
+int ccfv_server_poll(ccfv_server *s, uint64_t ticket, int *state, ccfv_stats *stats,
+                     double *latency_ms);
+/* Blocks until the request completes (timeout_s <= 0: no limit;
+ * CCFV_ERR_TIMEOUT when the wait gives up). */
+int ccfv_server_wait(ccfv_server *s, uint64_t ticket, double timeout_s, ccfv_stats *stats,
+                     double *latency_ms);
+/* Cancels a queued request, or a running one at the next epoch boundary. */
+int ccfv_server_cancel(ccfv_server *s, uint64_t ticket);
+/* Resident bytes, running and queued request counts. */
+int ccfv_server_info(ccfv_server *s, size_t *used_bytes, int *active, int *queued);
+/* Finishes running requests, cancels queued ones, stops the loop. */
+int ccfv_server_destroy(ccfv_server *s);
+
+/* ---- fields and diagnostics -------------------------------------------- */
+/* 3x3 Simpson cell averages of the reference's exact solution (the rotated,
+ * diffused Gaussian C_Exact, x0 = -0.35, sigma = 0.005, rotation rate 4) at
+ * time t on the context's grid; t = 0 is the reference's initial condition.
+ * Replaces get_exact_solution_on_gpu (T2S4_Parareal.cu:118-140). */
+int ccfv_exact_ref(ccfv_ctx *ctx, double *d_C, double t, void *stream);
+
+/* 3x3 Simpson cell averages of sum_q amp_q exp(-((x-cx_q)^2+(y-cy_q)^2)/den_q),
+ * params = n x (cx, cy, den, amp), with the periodic images of the domain
+ * box over [-images, images]^2 (0..4).  Synthetic initial fields. */
+int ccfv_gaussians(ccfv_ctx *ctx, double *d_C, int n, const double *params, int images,
+                   void *stream);
+
+/* Relative L2 norm ||a-b||/||b|| and max |a-b| of two device fields on the
+ * device (the reference computes the max norm on the host,
+ * T2S4_Parareal.cu:1333-1346).  Synchronises `stream`. */
+int ccfv_error_norms(ccfv_ctx *ctx, const double *d_a, const double *d_b, double *rel_l2,
+                     double *max_abs, void *stream);
+
 /* ---- allocation-free step ---------------------------------------------- */
 /* One split step like ccfv_step, for callers that cannot allocate device
  * memory (inside another framework's memory pool, services that forbid
@@ -169,12 +272,20 @@ int ccfv_parareal(ccfv_ctx *ctx, const ccfv_parareal_opts *opts, const double *C
  * counterpart in the reference.  Needs no context and calls no cudaMalloc,
  * cudaFree or allocating library routine: its scratch (solver factors, sweep
  * descriptors, status word) is a fixed file-scope device array of about
- * 200 KB that every GPU loading the library holds until exit.  Limit:
+ * 340 KB that every GPU loading the library holds until exit.  Limit:
  * nx, ny <= 4096, else CCFV_ERR_UNSUPPORTED.  The first call on a device
  * looks up the array's address with that device current: make it before any
  * stream capture.  All calls share the array: calls that overlap on the GPU
  * race.  Synchronises `stream` before returning. */
 int ccfv_step_noalloc(const ccfv_grid *grid, double *d_C, double tn, double dt, void *stream);
+
+/* ---- tuning ------------------------------------------------------------ */
+/* Autotunes the line-tile shape of the sweeps for this context's grid: times
+ * the candidate segment lengths (cells per CTA along a line: the tile height,
+ * which also sets the recurrence chunk length) of one step of dt in the given
+ * precision and keeps the fastest for every later plan with these line
+ * lengths (process-wide).  *segment (optional) receives the choice. */
+int ccfv_autotune(ccfv_ctx *ctx, double dt, int precision, int *segment, void *stream);
 
 /* ---- library info ---------------------------------------------------- */
 /* Number of kernels this library launched since load (all contexts). */

@@ -55,7 +55,7 @@ class PararealOpts(C.Structure):
         ("t0", C.c_double), ("t1", C.c_double),
         ("nt_fine", C.c_int), ("n_slices", C.c_int), ("coarse_ratio", C.c_int),
         ("tol", C.c_double), ("kmax", C.c_int), ("coarse_precision", C.c_int),
-        ("form", C.c_int), ("mem", C.c_int),
+        ("form", C.c_int), ("mem", C.c_int), ("d_ref", C.c_void_p),
     ]
 
 
@@ -66,6 +66,7 @@ class Stats(C.Structure):
         ("fine_cell_updates", C.c_double), ("coarse_cell_updates", C.c_double),
         ("ms", C.c_double), ("fine_ms", C.c_double), ("coarse_ms", C.c_double),
         ("fine_sweep_launches", C.c_longlong), ("fine_sweep_cells", C.c_longlong),
+        ("err_max", C.c_double * MAX_ITERS), ("err_l2", C.c_double * MAX_ITERS),
     ]
 
     def as_dict(self) -> dict:
@@ -76,8 +77,20 @@ class Stats(C.Structure):
                     coarse_cell_updates=self.coarse_cell_updates, ms=self.ms,
                     fine_ms=self.fine_ms, coarse_ms=self.coarse_ms,
                     fine_sweep_launches=self.fine_sweep_launches,
-                    fine_sweep_cells=self.fine_sweep_cells)
+                    fine_sweep_cells=self.fine_sweep_cells,
+                    err_max=[self.err_max[i] for i in range(min(n, MAX_ITERS))],
+                    err_l2=[self.err_l2[i] for i in range(min(n, MAX_ITERS))])
 
+
+class Problem(C.Structure):
+    _fields_ = [("grid", Grid), ("opts", PararealOpts), ("C0", C.c_void_p), ("C_T", C.c_void_p)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_size_t), ("max_active", C.c_int)]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = 0, 1, 2, 3, 4
 
 _lib = None
 
@@ -97,6 +110,29 @@ _SIGS = {
                                 C.POINTER(Stats), C.c_void_p]),
     "ccfv_kernel_launches": (C.c_uint64, []),
     "ccfv_last_error": (C.c_char_p, [C.c_void_p]),
+    "ccfv_exact_ref": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
+    "ccfv_gaussians": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                 C.c_void_p]),
+    "ccfv_error_norms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double), C.c_void_p]),
+    "ccfv_batch_solve": (C.c_int, [C.c_int, C.POINTER(Problem), C.POINTER(Stats), C.c_int,
+                                   C.c_void_p]),
+    "ccfv_server_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(ServerOpts)]),
+    "ccfv_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.POINTER(C.c_uint64)]),
+    "ccfv_server_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_int), C.POINTER(Stats),
+                                   C.POINTER(C.c_double)]),
+    "ccfv_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(Stats),
+                                   C.POINTER(C.c_double)]),
+    "ccfv_server_cancel": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "ccfv_server_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_int)]),
+    "ccfv_server_destroy": (C.c_int, [C.c_void_p]),
+    "ccfv_fine_slices": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double,
+                                   C.c_double, C.c_int, C.c_void_p]),
+    "ccfv_correct": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                               C.c_void_p]),
+    "ccfv_autotune": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_int), C.c_void_p]),
     "ccfv_step_noalloc": (C.c_int, [C.POINTER(Grid), C.c_void_p, C.c_double, C.c_double,
                                     C.c_void_p]),
 }
@@ -215,15 +251,51 @@ class Solver:
     def check(self, stream=None):
         self._chk(lib().ccfv_check(self._h, _stream_ptr(stream)))
 
+    def fine_slices(self, fields, t0, slice_dt, DT, J, stream=None):
+        """F on every field of a (n, nx, ny) CUDA tensor, in place."""
+        self._chk(lib().ccfv_fine_slices(self._h, _dptr(fields), int(fields.shape[0]), t0,
+                                         slice_dt, DT, int(J), _stream_ptr(stream)))
+
+    def correct(self, form, U, F, W, Gold=None, stream=None):
+        """Parareal correction of one slice; returns (sum dU^2, sum U^2)."""
+        a, b = C.c_double(), C.c_double()
+        self._chk(lib().ccfv_correct(self._h, int(form), _dptr(U), _dptr(F),
+                                     None if Gold is None else _dptr(Gold), _dptr(W),
+                                     C.byref(a), C.byref(b), _stream_ptr(stream)))
+        return a.value, b.value
+
+    def autotune(self, dt, precision=FP64, stream=None) -> int:
+        seg = C.c_int(0)
+        self._chk(lib().ccfv_autotune(self._h, dt, int(precision), C.byref(seg),
+                                      _stream_ptr(stream)))
+        return seg.value
+
+    # -- fields and diagnostics --------------------------------------------
+    def exact_ref(self, C_dev, t, stream=None):
+        self._chk(lib().ccfv_exact_ref(self._h, _dptr(C_dev), t, _stream_ptr(stream)))
+
+    def gaussians(self, C_dev, params, images=0, stream=None):
+        p = np.ascontiguousarray(params, dtype=np.float64).reshape(-1, 4)
+        self._chk(lib().ccfv_gaussians(self._h, _dptr(C_dev), p.shape[0], C_void(p),
+                                       int(images), _stream_ptr(stream)))
+
+    def error_norms(self, a, b, stream=None):
+        r, m = C.c_double(), C.c_double()
+        self._chk(lib().ccfv_error_norms(self._h, _dptr(a), _dptr(b), C.byref(r), C.byref(m),
+                                         _stream_ptr(stream)))
+        return r.value, m.value
+
     # -- Parareal --------------------------------------------------------
     def parareal(self, C0, C_T=None, *, t0, t1, nt_fine, n_slices, coarse_ratio=0, tol=0.0,
-                 kmax=8, coarse_precision=FP64, form=FORM_STANDARD, stream=None):
+                 kmax=8, coarse_precision=FP64, form=FORM_STANDARD, ref=None, stream=None):
         """Parareal solve.  C0 / C_T are CUDA tensors (device) or numpy
-        arrays (host).  Returns (C_T, stats dict)."""
+        arrays (host); `ref` an optional CUDA tensor the iterates at t1 are
+        compared with.  Returns (C_T, stats dict)."""
         host = isinstance(C0, np.ndarray)
         o = PararealOpts(t0, t1, int(nt_fine), int(n_slices), int(coarse_ratio), float(tol),
                          int(kmax), int(coarse_precision), int(form),
-                         MEM_HOST if host else MEM_DEVICE)
+                         MEM_HOST if host else MEM_DEVICE,
+                         None if ref is None else _dptr(ref).value)
         st = Stats()
         if host:
             c0 = np.ascontiguousarray(C0, dtype=np.float64)
@@ -237,6 +309,112 @@ class Solver:
                                      _stream_ptr(stream))
         self._chk(rc)
         return out, st.as_dict()
+
+
+def _problem(p):
+    """ctypes Problem from a dict (grid, C0, C_T, Parareal options)."""
+    host = isinstance(p["C0"], np.ndarray)
+    o = PararealOpts(p["t0"], p["t1"], int(p["nt_fine"]), int(p["n_slices"]),
+                     int(p.get("coarse_ratio", 0)), float(p.get("tol", 0.0)),
+                     int(p.get("kmax", 8)), int(p.get("coarse_precision", FP64)),
+                     int(p.get("form", FORM_STANDARD)), MEM_HOST if host else MEM_DEVICE, None)
+    pr = Problem()
+    pr.grid = p["grid"]
+    pr.opts = o
+    if host:
+        pr.C0 = p["C0"].ctypes.data
+        pr.C_T = p["C_T"].ctypes.data
+    else:
+        pr.C0 = _dptr(p["C0"]).value
+        pr.C_T = _dptr(p["C_T"]).value
+    return pr
+
+
+class Server:
+    """Continuous-batching request loop (ccfv_server_*).  Problems are dicts
+    as for batch_solve; C0 / C_T (host numpy or device tensors) must stay
+    alive until the request completes."""
+
+    def __init__(self, hbm_budget_bytes, device=0, max_active=0):
+        self._h = C.c_void_p()
+        o = ServerOpts(int(device), int(hbm_budget_bytes), int(max_active))
+        rc = lib().ccfv_server_create(C.byref(self._h), C.byref(o))
+        if rc:
+            raise CcfvError(rc, lib().ccfv_strerror(rc).decode())
+        self._keep = {}
+
+    def submit(self, problem) -> int:
+        t = C.c_uint64()
+        rc = lib().ccfv_server_submit(self._h, C.byref(_problem(problem)), C.byref(t))
+        if rc:
+            raise CcfvError(rc, lib().ccfv_strerror(rc).decode())
+        self._keep[t.value] = problem
+        return t.value
+
+    def poll(self, ticket):
+        st, s, lat = C.c_int(), Stats(), C.c_double()
+        rc = lib().ccfv_server_poll(self._h, ticket, C.byref(st), C.byref(s), C.byref(lat))
+        return rc, st.value, (s.as_dict() if st.value == REQ_DONE else None), lat.value
+
+    def wait(self, ticket, timeout_s=0.0):
+        s, lat = Stats(), C.c_double()
+        rc = lib().ccfv_server_wait(self._h, ticket, float(timeout_s), C.byref(s), C.byref(lat))
+        if rc:
+            raise CcfvError(rc, lib().ccfv_strerror(rc).decode())
+        self._keep.pop(ticket, None)
+        return s.as_dict(), lat.value
+
+    def cancel(self, ticket):
+        return lib().ccfv_server_cancel(self._h, ticket)
+
+    def info(self):
+        u, a, q = C.c_size_t(), C.c_int(), C.c_int()
+        lib().ccfv_server_info(self._h, C.byref(u), C.byref(a), C.byref(q))
+        return dict(used_bytes=u.value, active=a.value, queued=q.value)
+
+    def close(self):
+        if self._h:
+            lib().ccfv_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_solve(problems, device=0, stream=None):
+    """Solve several Parareal problems together (ccfv_batch_solve).
+
+    `problems` is a list of dicts with keys grid (Grid), C0, C_T (CUDA
+    tensors or numpy arrays, all problems alike) and the Parareal options of
+    Solver.parareal.  Returns the list of stats dicts."""
+    n = len(problems)
+    arr = (Problem * n)()
+    keep = []
+    for i, p in enumerate(problems):
+        host = isinstance(p["C0"], np.ndarray)
+        o = PararealOpts(p["t0"], p["t1"], int(p["nt_fine"]), int(p["n_slices"]),
+                         int(p.get("coarse_ratio", 0)), float(p.get("tol", 0.0)),
+                         int(p.get("kmax", 8)), int(p.get("coarse_precision", FP64)),
+                         int(p.get("form", FORM_STANDARD)), MEM_HOST if host else MEM_DEVICE,
+                         None)
+        arr[i].grid = p["grid"]
+        arr[i].opts = o
+        if host:
+            c0 = np.ascontiguousarray(p["C0"], dtype=np.float64)
+            keep.append(c0)
+            arr[i].C0 = c0.ctypes.data
+            arr[i].C_T = p["C_T"].ctypes.data
+        else:
+            arr[i].C0 = _dptr(p["C0"]).value
+            arr[i].C_T = _dptr(p["C_T"]).value
+    st = (Stats * n)()
+    rc = lib().ccfv_batch_solve(n, arr, st, int(device), _stream_ptr(stream))
+    if rc:
+        raise CcfvError(rc, lib().ccfv_strerror(rc).decode())
+    return [st[i].as_dict() for i in range(n)]
 
 
 def C_void(a: np.ndarray):

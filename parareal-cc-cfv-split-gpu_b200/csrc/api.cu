@@ -63,8 +63,9 @@ int ccfv_create(ccfv_ctx **out, const ccfv_grid *grid, int device) {
   int rc = use_device(ctx);
   if (rc) { delete ctx; return rc; }
   if (ctx->status.alloc(sizeof(unsigned) * 4) != cudaSuccess ||
-      ctx->partial.alloc(sizeof(double) * 2 * RED_BLOCKS_MAX) != cudaSuccess ||
-      ctx->counter.alloc(sizeof(unsigned) * 4) != cudaSuccess) {
+      ctx->partial.alloc(sizeof(double) * 3 * RED_BLOCKS_MAX) != cudaSuccess ||
+      ctx->counter.alloc(sizeof(unsigned) * 4) != cudaSuccess ||
+      ctx->aux.alloc(sizeof(double) * 64) != cudaSuccess) {
     delete ctx;
     return CCFV_ERR_NOMEM;
   }
@@ -161,6 +162,60 @@ int ccfv_parareal(ccfv_ctx *ctx, const ccfv_parareal_opts *opts, const double *C
   int rc = use_device(ctx);
   if (rc) return rc;
   return parareal(ctx, opts, C0, C_T, stats, (cudaStream_t)stream);
+}
+
+int ccfv_exact_ref(ccfv_ctx *ctx, double *d_C, double t, void *stream) {
+  if (!ctx || !d_C) return CCFV_ERR_INVALID;
+  int rc = use_device(ctx);
+  return rc ? rc : exact_ref(ctx, d_C, t, (cudaStream_t)stream);
+}
+
+int ccfv_gaussians(ccfv_ctx *ctx, double *d_C, int n, const double *params, int images,
+                   void *stream) {
+  if (!ctx || !d_C || n < 1 || !params || images < 0 || images > 4) return CCFV_ERR_INVALID;
+  for (int q = 0; q < n; ++q)
+    if (!(params[4 * q + 2] > 0.0)) return CCFV_ERR_INVALID;
+  int rc = use_device(ctx);
+  return rc ? rc : gaussians(ctx, d_C, n, params, images, (cudaStream_t)stream);
+}
+
+int ccfv_error_norms(ccfv_ctx *ctx, const double *d_a, const double *d_b, double *rel_l2,
+                     double *max_abs, void *stream) {
+  if (!ctx || !d_a || !d_b) return CCFV_ERR_INVALID;
+  int rc = use_device(ctx);
+  return rc ? rc : norms(ctx, d_a, d_b, rel_l2, max_abs, (cudaStream_t)stream);
+}
+
+int ccfv_batch_solve(int n, const ccfv_problem *problems, ccfv_stats *stats, int device,
+                     void *stream) {
+  if (n < 1 || !problems) return CCFV_ERR_INVALID;
+  for (int i = 0; i < n; ++i)
+    if (!grid_ok(&problems[i].grid) || !problems[i].C0 || !problems[i].C_T) return CCFV_ERR_INVALID;
+  std::string err;
+  return batch_solve(n, problems, stats, device, (cudaStream_t)stream, &err);
+}
+
+int ccfv_fine_slices(ccfv_ctx *ctx, double *d_fields, int n, double t0, double slice_dt,
+                     double DT, int J, void *stream) {
+  if (!ctx || !d_fields || n < 1 || J < 1) return CCFV_ERR_INVALID;
+  int rc = use_device(ctx);
+  return rc ? rc : fine_slices(ctx, d_fields, n, t0, slice_dt, DT, J, (cudaStream_t)stream);
+}
+
+int ccfv_correct(ccfv_ctx *ctx, int form, double *d_U, const double *d_F, double *d_Gold,
+                 double *d_W, double *sq_update, double *sq_state, void *stream) {
+  if (!ctx || !d_U || !d_F || !d_W) return CCFV_ERR_INVALID;
+  if (form != CCFV_FORM_STANDARD && form != CCFV_FORM_DELTA) return CCFV_ERR_INVALID;
+  if (form == CCFV_FORM_STANDARD && !d_Gold) return CCFV_ERR_INVALID;
+  int rc = use_device(ctx);
+  return rc ? rc : correct(ctx, form, d_U, d_F, d_Gold, d_W, sq_update, sq_state, (cudaStream_t)stream);
+}
+
+int ccfv_autotune(ccfv_ctx *ctx, double dt, int precision, int *segment, void *stream) {
+  if (!ctx || !(dt > 0.0) || (precision != CCFV_FP64 && precision != CCFV_FP32))
+    return CCFV_ERR_INVALID;
+  int rc = use_device(ctx);
+  return rc ? rc : autotune(ctx, dt, precision == CCFV_FP64, (cudaStream_t)stream, segment);
 }
 
 uint64_t ccfv_kernel_launches(void) { return launches(); }

@@ -46,7 +46,15 @@ struct SweepField {
   int uniform;           // 1: the velocity along the sweep depends only on the
                          // transverse coordinate (every foot of a line has the
                          // same displacement): stencil fast path
-  int pad1;
+  int jf;                // filter kernel: recurrence warm-up length J
+  // Batched launches (all zero for single-instance launches):
+  int inst;              // instance index into the launch's `nlo` array
+  int slice;             // >= 0: fixed slice of this field; -1: the launch's slice
+  int jmax;              // the field takes part while jstep < jmax (0: always)
+  int smax;              // slice-indexed fields: while slice < smax
+  int gskip;             // slice-indexed fields: skip slice == nlo (zero increment)
+  double t_step;         // added per launch step: time = ... + jstep * t_step
+  double t_slice;        // added per launch slice: time = ... + slice * t_slice
   double vp[4];          // velocity parameters
   double s_min, s_max, h;  // along-line edge coordinates: s_min + h*e
   double t_min, ht;        // transverse edges: t_min + ht*line
@@ -55,19 +63,22 @@ struct SweepField {
   double eps_remap;        // compat remap clamp (x: 1e-15, y: 1e-16)
   double kb;               // 0.5*K*(Dt/h): RHS diffusion coefficient
   double inv12h;           // 1/(12 h)
-  double sm_fac;           // periodic: a / gamma
-  double sm_inv_den;       // periodic: 1 / (1 + z0 + (a/gamma) z_{L-1})
+  double sm_fac;           // periodic, scan kernels: a / gamma; filter kernel: mu
+  double sm_inv_den;       // periodic, scan kernels: 1 / (1 + z0 + (a/gamma) z_{L-1});
+                           // filter kernel: 1 / c
   const void *tab;         // T[3L]: alpha_k | g_k | z_k (solver factors)
 };
 
 // Kernel variants: the per-cell kernel (any velocity / boundary / scheme) and
 // the fused stencil kernel (uniform displacement, periodic, derivative of the
 // sweep input).
-enum { SWEEP_GENERAL = 0, SWEEP_FAST = 1 };
+enum { SWEEP_GENERAL = 0, SWEEP_FAST = 1, SWEEP_FILTER = 2 };
+constexpr int FILTER_JMAX = 64;  // longest recurrence warm-up of the filter kernel
 
 // Shared-memory bytes of the sweep kernels for a launch.
 size_t sweep_smem_bytes(int lc_max, int halo, bool fp64);
 size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64);
+size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64);
 
 // Launches one fused sweep over all fields of `d_fields` (device array,
 // sorted by group0; tiles group_base .. group_base+groups_total-1).  All fields share the cluster size `cs`, their
@@ -78,6 +89,33 @@ template <typename T>
 cudaError_t launch_sweep(int variant, const SweepField *d_fields, int nfields, int group_base,
                          int groups_total, int cs, int lc_max, int halo, double toff, void *data,
                          unsigned *d_status, cudaStream_t stream);
+
+// Batched form: `jstep` / `nslice` select the step and slice of this launch,
+// `nlo[inst]` the first active slice of every instance (see SweepField).
+struct BatchStep {
+  int jstep = 0, nslice = 0;
+  const int *nlo = nullptr;
+};
+template <typename T>
+cudaError_t launch_sweep_batch(int variant, const SweepField *d_fields, int nfields,
+                               int group_base, int groups_total, int cs, int lc_max, int halo,
+                               const BatchStep &bs, unsigned *d_status, cudaStream_t stream);
+
+// Solver-table layout (T values): alpha[L] g[L] z[L] tP[L] tS[L]
+// aggA[cs*NCH] PA[cs*(NCH+1)], where, for the chunk partition the sweep
+// kernels use (cs = ceil(L/LC_MAX) CTAs per line, NCH chunks per CTA),
+// tP[k] / tS[k] are the products of alpha from the chunk start to k / from k
+// to the chunk end, aggA the chunk products and PA the CTA-local exclusive
+// prefix products of the chunks (PA[NCH] = product over the CTA).
+inline int table_cs(int L) { return (L + LC_MAX - 1) / LC_MAX; }
+inline size_t table_len(int L) {
+  const int cs = table_cs(L);
+  return 5 * (size_t)L + (size_t)cs * NCH + (size_t)cs * (NCH + 1);
+}
+// Fills tP, tS, aggA, PA of a table whose alpha is already in place
+// (heap-free; T = double or float, computed in double).
+template <typename T>
+void fill_chunk_products(int L, T *tab);
 
 // Counts kernel launches made by the library.
 void count_launch(uint64_t n = 1);

@@ -6,6 +6,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 namespace ccfv {
 
@@ -64,7 +65,7 @@ static void build_table(int L, double coA, double coB, int bc, std::vector<T> &o
     g[k] = 1.0 / (diag[k] - p[k - 1] * coA);
     p[k] = coC * g[k];
   }
-  out.assign(3 * (size_t)L, T(0));
+  out.assign(table_len(L), T(0));
   for (int k = 0; k < L; ++k) {
     out[k] = T(-coA * g[k]);
     out[L + k] = T(g[k]);
@@ -83,7 +84,40 @@ static void build_table(int L, double coA, double coB, int bc, std::vector<T> &o
     sm_fac = coA / gam;
     sm_inv_den = 1.0 / (1.0 + z[0] + sm_fac * z[L - 1]);
   }
+  fill_chunk_products(L, out.data());
 }
+
+template <typename T>
+void fill_chunk_products(int L, T *tab) {
+  const int cs = table_cs(L), Lc = (L + cs - 1) / cs;
+  const T *alpha = tab;
+  T *tP = tab + 3 * (size_t)L, *tS = tab + 4 * (size_t)L;
+  T *aggA = tab + 5 * (size_t)L, *PA = aggA + (size_t)cs * NCH;
+  for (int r = 0; r < cs; ++r) {
+    const int p0 = std::min(L, r * Lc), p1 = std::min(L, p0 + Lc), np = p1 - p0;
+    const int m = np > 0 ? (np + NCH - 1) / NCH : 1;
+    double pre = 1.0;
+    for (int c = 0; c < NCH; ++c) {
+      const int s0 = std::min(p1, p0 + c * m), e0 = std::min(p1, s0 + m);
+      double a = 1.0;
+      for (int k = s0; k < e0; ++k) {
+        a *= (double)alpha[k];
+        tP[k] = T(a);
+      }
+      double b = 1.0;
+      for (int k = e0 - 1; k >= s0; --k) {
+        b *= (double)alpha[k];
+        tS[k] = T(b);
+      }
+      aggA[(size_t)r * NCH + c] = T(a);
+      PA[(size_t)r * (NCH + 1) + c] = T(pre);
+      pre *= a;
+    }
+    PA[(size_t)r * (NCH + 1) + NCH] = T(pre);
+  }
+}
+template void fill_chunk_products<double>(int, double *);
+template void fill_chunk_products<float>(int, float *);
 
 static double spacing(const ccfv_grid &g, int dir) {
   return dir == 0 ? (g.x_max - g.x_min) / g.nx : (g.y_max - g.y_min) / g.ny;
@@ -100,7 +134,7 @@ const SolverTable *get_table(ccfv_ctx *ctx, int dir, double Dt, bool fp64, int *
   const double coA = 1.0 / 12 - 0.5 * g.K * r2;
   const double coB = 10.0 / 12 + g.K * r2;
   auto tab = std::make_unique<SolverTable>();
-  size_t bytes = 3 * (size_t)L * (fp64 ? 8 : 4);
+  size_t bytes = table_len(L) * (fp64 ? 8 : 4);
   if (tab->buf.alloc(bytes) != cudaSuccess) {
     *status = set_error(ctx, CCFV_ERR_NOMEM, "solver table allocation failed");
     return nullptr;
@@ -181,14 +215,132 @@ SweepField make_field(const ccfv_grid &g, int dir, double Dt, double ta_rel, dou
   return f;
 }
 
-static LaunchGeom geom_for(const ccfv_grid &g, int dir, double Dt, int dsrc) {
+// Factorisation of the cyclic constant system used by the filter kernel:
+// a z^-1 + b + a z = c (1 + mu z^-1)(1 + mu z), |mu| < 1; J = warm-up length
+// with |mu|^J below the rounding of the precision.  Returns false when the
+// warm-up would exceed FILTER_JMAX (strong diffusion: exact-scan kernels).
+bool filter_params(const ccfv_grid &g, int dir, double Dt, bool fp64, double *mu, double *ic,
+                   int *J) {
+  const double h = spacing(g, dir);
+  const double r2 = Dt / (h * h);
+  const double a = 1.0 / 12 - 0.5 * g.K * r2, b = 10.0 / 12 + g.K * r2;
+  const double r = a / b;  // |r| < 1/2 (diagonal dominance)
+  const double m = 2.0 * r / (1.0 + std::sqrt(std::max(0.0, 1.0 - 4.0 * r * r)));
+  const double c = b / (1.0 + m * m);
+  const double eps = fp64 ? std::ldexp(1.0, -56) : std::ldexp(1.0, -27);
+  int j = 1;
+  if (std::fabs(m) > 1e-300) j = std::max(1, (int)std::ceil(std::log(eps) / std::log(std::fabs(m))));
+  if (mu) *mu = m;
+  if (ic) *ic = 1.0 / c;
+  if (J) *J = j;
+  return j <= FILTER_JMAX;
+}
+
+// Autotuned segment length (cells per CTA) of the filter kernel, per line
+// length and precision; the default until ccfv_autotune measures it.
+static std::mutex g_tune_mu;
+static std::map<std::pair<int, int>, int> g_filter_lc;
+static thread_local int g_lc_override = 0;
+
+int filter_lc(int L, bool fp64) {
+  if (g_lc_override > 0) return g_lc_override;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_filter_lc.find({L, fp64 ? 1 : 0});
+  return it == g_filter_lc.end() ? LC_MAX : it->second;
+}
+
+LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64) {
   LaunchGeom G;
   const int L = dir == 0 ? g.nx : g.ny;
   G.cs = (L + LC_MAX - 1) / LC_MAX;
   G.lc_max = (L + G.cs - 1) / G.cs;
   const int sh = shift_cells(g, dir, Dt);
   G.halo = dsrc ? (sh + 4) + sh + 5 : sh + 5;
+  const bool uniform = g.velocity == CCFV_VEL_REF_ROT4 || g.velocity == CCFV_VEL_CONST ||
+                       g.velocity == CCFV_VEL_ROTATION;
+  G.variant = SWEEP_GENERAL;
+  if (uniform && g.bc == CCFV_BC_PERIODIC && dsrc == 0) {
+    int J = 0;
+    if (filter_params(g, dir, Dt, fp64, nullptr, nullptr, &J) && L > 2 * J) {
+      G.variant = SWEEP_FILTER;
+      G.halo = J + sh + 6;
+      // independent CTAs: any number per line, segment length from the tuner
+      const int lc = std::max(32, std::min(L, filter_lc(L, fp64)));
+      G.cs = (L + lc - 1) / lc;
+      G.lc_max = (L + G.cs - 1) / G.cs;
+    } else {
+      G.variant = SWEEP_FAST;
+    }
+  }
   return G;
+}
+
+// Times the filter kernel's candidate segment lengths on this grid (x and y
+// sweeps of one step of dt on a scratch field) and keeps the fastest.
+int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen) {
+  const ccfv_grid &g = ctx->grid;
+  const size_t el = fp64 ? 8 : 4;
+  const size_t NN = (size_t)g.nx * g.ny;
+  CK(ctx->io.alloc(el * NN));
+  CK(cudaMemsetAsync(ctx->io.p, 0, el * NN, st));
+  static const int cand[] = {64, 96, 128, 192, 256, 384, 512};
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  float best = 1e30f;
+  int best_lc = LC_MAX;
+  for (int lc : cand) {
+    if (lc > std::max(g.nx, g.ny) && lc != cand[0]) break;
+    g_lc_override = lc;
+    StepPlan plan;
+    std::vector<std::pair<void *, double>> f{{nullptr, 0.0}};
+    int rc = build_step_plan(ctx, &plan, dt, fp64, f);
+    if (rc == CCFV_OK && plan.geom[0].variant != SWEEP_FILTER && plan.geom[1].variant != SWEEP_FILTER) {
+      g_lc_override = 0;
+      break;  // nothing to tune: this grid does not use the filter kernel
+    }
+    if (rc == CCFV_OK) rc = run_step_plan(ctx, plan, fp64, 0, 1, 0.0, ctx->io.p, st);  // warm-up
+    if (rc == CCFV_OK) {
+      cudaEventRecord(a, st);
+      for (int r = 0; r < 5 && rc == CCFV_OK; ++r)
+        rc = run_step_plan(ctx, plan, fp64, 0, 1, 0.0, ctx->io.p, st);
+      cudaEventRecord(b, st);
+      cudaEventSynchronize(b);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, a, b);
+      if (rc == CCFV_OK && ms < best) {
+        best = ms;
+        best_lc = lc;
+      }
+    }
+    g_lc_override = 0;
+    if (rc != CCFV_OK && rc != CCFV_ERR_UNSUPPORTED) {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      return rc;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_filter_lc[{g.nx, fp64 ? 1 : 0}] = best_lc;
+    g_filter_lc[{g.ny, fp64 ? 1 : 0}] = best_lc;
+  }
+  ctx->step_plans.clear();  // plans built with the old geometry
+  ctx->fine_plan.reset();
+  if (chosen) *chosen = best_lc;
+  return CCFV_OK;
+}
+
+// Fills the filter-kernel constants of a field (its variant must be FILTER).
+void filter_field(const ccfv_grid &g, SweepField &f, bool fp64) {
+  double mu = 0, ic = 0;
+  int J = 0;
+  filter_params(g, f.dir, f.Dt, fp64, &mu, &ic, &J);
+  f.sm_fac = mu;
+  f.sm_inv_den = ic;
+  f.jf = J;
 }
 
 // Sub-steps of one split step: x(dt/2) over [t, t+dt/2], y(dt) over
@@ -212,19 +364,17 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
     int st = CCFV_OK;
     const SolverTable *tab = get_table(ctx, dir, Dt, fp64, &st);
     if (!tab) return st;
-    LaunchGeom G = geom_for(g, dir, Dt, dsrc);
-    const bool uniform = g.velocity == CCFV_VEL_REF_ROT4 || g.velocity == CCFV_VEL_CONST ||
-                         g.velocity == CCFV_VEL_ROTATION;
-    G.variant = (uniform && g.bc == CCFV_BC_PERIODIC && dsrc == 0 && !ctx->force_general)
-                    ? SWEEP_FAST : SWEEP_GENERAL;
+    LaunchGeom G = step_geom(g, dir, Dt, dsrc, fp64);
+    if (ctx->force_general) G.variant = SWEEP_GENERAL;
     if (G.cs > MAX_CLUSTER)
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
-    if (std::max(sweep_smem_bytes(G.lc_max, G.halo, fp64),
-                 sweep_fast_smem_bytes(G.lc_max, G.halo, fp64)) > 227 * 1024)
+    if (std::max({sweep_smem_bytes(G.lc_max, G.halo, fp64), sweep_fast_smem_bytes(G.lc_max, G.halo, fp64),
+                  sweep_filter_smem_bytes(G.lc_max, G.halo, fp64)}) > 227 * 1024)
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
     for (int i = 0; i < nf; ++i) {
       SweepField f = make_field(g, dir, Dt, ta + fields[i].second, tb + fields[i].second,
                                 fields[i].first, tab, dsrc);
+      if (G.variant == SWEEP_FILTER) filter_field(g, f, fp64);
       f.group0 = i * f.groups;
       h[(size_t)kind * nf + i] = f;
       plan->groups_per_field[kind] = f.groups;
@@ -504,6 +654,11 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
         return rc;
     }
     CK(cudaEventRecord(gb, st));
+    if (o->d_ref && stats && k - 1 < CCFV_MAX_ITERS) {
+      int rc = ccfv::norms(ctx, U + (size_t)S * NN, o->d_ref, &stats->err_l2[k - 1],
+                           &stats->err_max[k - 1], st);
+      if (rc) return rc;
+    }
     CK(cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 2 * (S + 1), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     {
@@ -575,6 +730,39 @@ int parareal(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const double *C0, doubl
     CK(cudaMemset(ctx->status.p, 0, sizeof(unsigned)));
     return set_error(ctx, CCFV_ERR_HALO, "a characteristic foot left the staged halo");
   }
+  return CCFV_OK;
+}
+
+// F over n contiguous fields (field i starts at t0 + i * slice_dt): J steps of
+// DT/J each, every field advancing in the same launches (the F phase).
+int fine_slices(ccfv_ctx *ctx, double *d_fields, int n, double t0, double slice_dt, double DT,
+                int J, cudaStream_t st) {
+  const long long NN = (long long)ctx->grid.nx * ctx->grid.ny;
+  const double dt = DT / (double)J;
+  StepPlan plan;
+  std::vector<std::pair<void *, double>> fl;
+  for (int i = 0; i < n; ++i) fl.push_back({d_fields + (size_t)i * NN, t0 + i * slice_dt});
+  int rc = build_step_plan(ctx, &plan, dt, true, fl);
+  if (rc) return rc;
+  for (int j = 0; j < J; ++j)
+    if ((rc = run_step_plan(ctx, plan, true, 0, n, j * dt, nullptr, st))) return rc;
+  CK(cudaStreamSynchronize(st));  // the plan's descriptors are released on return
+  return CCFV_OK;
+}
+
+// Stand-alone Parareal correction of one slice with its update norms (the
+// building block of the slice-distributed driver).
+int correct(ccfv_ctx *ctx, int form, double *U, const double *Fv, double *Gold, double *W,
+            double *sq_update, double *sq_state, cudaStream_t st) {
+  const long long NN = (long long)ctx->grid.nx * ctx->grid.ny;
+  double *out = ctx->aux.as<double>() + 8;
+  int rc = correction<double>(ctx, form, NN, U, Fv, Gold, W, out, st);
+  if (rc) return rc;
+  double h[2];
+  CK(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (sq_update) *sq_update = h[0];
+  if (sq_state) *sq_state = h[1];
   return CCFV_OK;
 }
 

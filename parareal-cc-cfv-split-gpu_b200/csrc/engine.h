@@ -55,7 +55,7 @@ struct ccfv_ctx {
   std::map<std::tuple<int, double, int>, std::unique_ptr<ccfv::SolverTable>> tables;
   std::map<std::tuple<double, int>, std::unique_ptr<ccfv::StepPlan>> step_plans;
   // Parareal slice states and scratch
-  ccfv::DevBuf U, F, Gold, W, C64, C32, norms, partial, counter, io;
+  ccfv::DevBuf U, F, Gold, W, C64, C32, norms, partial, counter, io, aux;
   size_t slices_cap = 0;
   std::unique_ptr<ccfv::StepPlan> fine_plan;
   double fine_plan_key[4] = {0, 0, 0, 0};
@@ -70,14 +70,27 @@ int set_error(ccfv_ctx *ctx, int code, const std::string &msg);
 const SolverTable *get_table(ccfv_ctx *ctx, int dir, double Dt, bool fp64, int *status);
 SweepField make_field(const ccfv_grid &g, int dir, double Dt, double ta_rel, double tb_rel,
                       void *data, const SolverTable *tab, int dsrc);
+LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64);
+void filter_field(const ccfv_grid &g, SweepField &f, bool fp64);
+int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen);
+int batch_solve(int n, const ccfv_problem *probs, ccfv_stats *stats, int device,
+                cudaStream_t st, std::string *errmsg);
 int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
                     const std::vector<std::pair<void *, double>> &fields);
 int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int count,
                   double toff, void *data_override, cudaStream_t st);
 int steps(ccfv_ctx *ctx, void *d_C, bool fp64, double t0, double dt, int nsteps, cudaStream_t st);
 int coarse_fp32(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, cudaStream_t st);
+int fine_slices(ccfv_ctx *ctx, double *d_fields, int n, double t0, double slice_dt, double DT,
+                int J, cudaStream_t st);
+int correct(ccfv_ctx *ctx, int form, double *U, const double *Fv, double *Gold, double *W,
+            double *sq_update, double *sq_state, cudaStream_t st);
 int parareal(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const double *C0, double *C_T,
              ccfv_stats *stats, cudaStream_t st);
+int exact_ref(ccfv_ctx *ctx, double *d_C, double t, cudaStream_t st);
+int gaussians(ccfv_ctx *ctx, double *d_C, int ng, const double *params, int img, cudaStream_t st);
+int norms(ccfv_ctx *ctx, const double *a, const double *b, double *rel_l2, double *max_abs,
+          cudaStream_t st);
 constexpr int RED_BLOCKS_MAX = 592;
 
 }  // namespace ccfv

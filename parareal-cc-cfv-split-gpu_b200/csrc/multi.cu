@@ -1,0 +1,553 @@
+// multi.cu -- many Parareal solves of different sizes, velocities and
+// diffusivities advanced together (batched solves and the serving loop).
+//
+// Every instance keeps its slice states resident on the device.  All fine
+// propagators of all instances (every active slice) advance in the same sweep
+// launches, and the sequential coarse sweeps of all instances advance slice by
+// slice in shared launches, so a launch covers hundreds of fields and fills
+// the GPU even when each instance alone cannot.  Fields are grouped into
+// launch classes (kernel variant, precision, cluster size, segment length);
+// instances that have converged, slices that are already exact and instances
+// with fewer steps or slices drop out on the device (per-instance `nlo`
+// array, SweepField::jmax/smax) without any host work per launch.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include "multi.h"
+
+namespace ccfv {
+namespace {
+
+// Per-instance element-wise work of one batched launch.
+struct BElem {
+  double *U, *F, *Gold;
+  void *W;
+  long long NN;
+  int S, form, g64, pad;
+  double *norms;  // [2*(S+1)]
+};
+
+enum { OP_LOAD_W = 0, OP_STORE_W = 1, OP_COPY_F = 2, OP_CORRECT = 3, OP_LOAD_W_STD = 4 };
+
+constexpr int BT = 256;
+
+__device__ __forceinline__ double wload(const BElem &b, long long i) {
+  return b.g64 ? reinterpret_cast<const double *>(b.W)[i]
+               : (double)reinterpret_cast<const float *>(b.W)[i];
+}
+__device__ __forceinline__ void wstore(const BElem &b, long long i, double v) {
+  if (b.g64) reinterpret_cast<double *>(b.W)[i] = v;
+  else reinterpret_cast<float *>(b.W)[i] = (float)v;
+}
+
+// blockIdx.y = instance.  OP_CORRECT reduces the update norms of slice n+1
+// per instance with fixed-order block partials (deterministic).
+__global__ void __launch_bounds__(BT)
+    batch_elem_kernel(int op, const BElem *__restrict__ d, int n, const int *__restrict__ nlo,
+                      double *__restrict__ partial, unsigned *__restrict__ counters) {
+  const int inst = blockIdx.y;
+  const BElem b = d[inst];
+  const int lo = nlo[inst];
+  long long n0 = 0, cnt = b.NN;
+  if (op == OP_LOAD_W_STD) {  // G-phase: only the standard form restarts G from U
+    if (b.form != CCFV_FORM_STANDARD) return;
+    op = OP_LOAD_W;
+  }
+  switch (op) {
+    case OP_LOAD_W:
+    case OP_STORE_W:
+    case OP_CORRECT:
+      if (n >= b.S || n < lo) return;
+      break;
+    case OP_COPY_F:  // F[m+1] <- U[m] for every active slice m >= lo
+      if (lo >= b.S) return;
+      n0 = (long long)lo * b.NN;
+      cnt = (long long)(b.S - lo) * b.NN;
+      break;
+  }
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long first = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double se = 0.0, su = 0.0;
+  if (op == OP_LOAD_W) {
+    const double *src = b.U + (long long)n * b.NN;
+    for (long long i = first; i < cnt; i += stride) wstore(b, i, src[i]);
+  } else if (op == OP_STORE_W) {
+    double *dst = b.U + (long long)(n + 1) * b.NN;
+    double *gd = b.Gold ? b.Gold + (long long)(n + 1) * b.NN : nullptr;
+    for (long long i = first; i < cnt; i += stride) {
+      const double v = wload(b, i);
+      dst[i] = v;
+      if (gd) gd[i] = v;
+    }
+  } else if (op == OP_COPY_F) {
+    const double *src = b.U + n0;
+    double *dst = b.F + n0 + b.NN;
+    for (long long i = first; i < cnt; i += stride) dst[i] = src[i];
+  } else {
+    double *U = b.U + (long long)(n + 1) * b.NN;
+    const double *Fv = b.F + (long long)(n + 1) * b.NN;
+    double *Go = b.Gold ? b.Gold + (long long)(n + 1) * b.NN : nullptr;
+    const bool zero_g = (b.form == CCFV_FORM_DELTA && n == lo);  // G(0) = 0
+    for (long long i = first; i < cnt; i += stride) {
+      const double uo = U[i];
+      const double gw = zero_g ? 0.0 : wload(b, i);
+      double un;
+      if (b.form == CCFV_FORM_STANDARD) {
+        un = gw + (Fv[i] - Go[i]);  // parareal_correction_kernel, T2S4:771-782
+        Go[i] = gw;
+      } else {
+        un = Fv[i] + gw;
+        wstore(b, i, un - uo);
+      }
+      const double dd = un - uo;
+      U[i] = un;
+      se += dd * dd;
+      su += un * un;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      se += __shfl_down_sync(0xffffffffu, se, o);
+      su += __shfl_down_sync(0xffffffffu, su, o);
+    }
+    __shared__ double red[2][BT / 32];
+    __shared__ bool last;
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { red[0][w] = se; red[1][w] = su; }
+    __syncthreads();
+    double *part = partial + (size_t)inst * 2 * gridDim.x;
+    if (threadIdx.x == 0) {
+      double a = 0, c = 0;
+      for (int k = 0; k < BT / 32; ++k) { a += red[0][k]; c += red[1][k]; }
+      part[2 * blockIdx.x] = a;
+      part[2 * blockIdx.x + 1] = c;
+      __threadfence();
+      last = (atomicAdd(&counters[inst], 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+      __threadfence();
+      double a = 0, c = 0;
+      for (unsigned k = 0; k < gridDim.x; ++k) {
+        a += ((volatile double *)part)[2 * k];
+        c += ((volatile double *)part)[2 * k + 1];
+      }
+      b.norms[2 * (n + 1)] = a;
+      b.norms[2 * (n + 1) + 1] = c;
+      counters[inst] = 0;
+    }
+  }
+}
+
+}  // namespace
+
+using KKey = std::tuple<int, int, int, int, int>;  // kind, variant, cs, lc bucket, fp64
+
+static void add_field(std::map<KKey, SweepClass> &classes, int kind, const ccfv_grid &g,
+                      const SweepField &f0, bool fp64) {
+  const LaunchGeom G = step_geom(g, f0.dir, f0.Dt, f0.dsrc, fp64);
+  const int bucket = (G.lc_max + 63) / 64;  // segment-length bucket bounds the staged tile
+  SweepClass &K = classes[KKey{kind, G.variant, G.cs, bucket, fp64 ? 1 : 0}];
+  K.kind = kind;
+  K.variant = G.variant;
+  K.cs = G.cs;
+  K.fp64 = fp64 ? 1 : 0;
+  K.lc_max = std::max(K.lc_max, G.lc_max);
+  K.halo = std::max(K.halo, G.halo);
+  SweepField f = f0;
+  if (G.variant == SWEEP_FILTER) filter_field(g, f, fp64);
+  f.group0 = K.groups;
+  K.groups += f.groups;
+  K.h.push_back(f);
+}
+
+size_t problem_bytes(const ccfv_grid &g, const ccfv_parareal_opts &o) {
+  const size_t fb = sizeof(double) * (size_t)g.nx * g.ny;
+  const size_t S = (size_t)std::max(o.n_slices, 1);
+  const bool g64 = o.coarse_precision != CCFV_FP32;
+  return fb * (S + 1) * 2 + (o.form == CCFV_FORM_STANDARD ? fb * (S + 1) : 0) +
+         (g64 ? fb : fb / 2) + 4 * 256;
+}
+
+int problem_setup(Problem &P, const ccfv_problem &p, std::string *err) {
+  P.g = p.grid;
+  P.o = p.opts;
+  P.C0 = p.C0;
+  P.C_T = p.C_T;
+  const ccfv_parareal_opts &o = P.o;
+  if (o.n_slices < 1 || o.nt_fine < o.n_slices || o.nt_fine % o.n_slices || o.kmax < 1 ||
+      o.kmax > CCFV_MAX_ITERS || (o.coarse_precision == CCFV_FP32 && o.form != CCFV_FORM_DELTA) ||
+      (o.form != CCFV_FORM_STANDARD && o.form != CCFV_FORM_DELTA)) {
+    if (err) *err = "invalid Parareal options";
+    return CCFV_ERR_INVALID;
+  }
+  P.S = o.n_slices;
+  P.J = o.nt_fine / P.S;
+  if (o.coarse_ratio < 0 || (o.coarse_ratio > 0 && P.J % o.coarse_ratio)) {
+    if (err) *err = "coarse_ratio must divide nt_fine / n_slices";
+    return CCFV_ERR_INVALID;
+  }
+  P.m = o.coarse_ratio > 0 ? P.J / o.coarse_ratio : 1;
+  P.DT = (o.t1 - o.t0) / P.S;
+  P.dt = P.DT / (double)P.J;
+  P.dtc = P.DT / (double)P.m;
+  P.NN = (long long)P.g.nx * P.g.ny;
+  P.g64 = o.coarse_precision != CCFV_FP32;
+  P.bytes = problem_bytes(P.g, o);
+  return CCFV_OK;
+}
+
+#define MCK(call)                                                                      \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(e_ == cudaErrorMemoryAllocation ? CCFV_ERR_NOMEM : CCFV_ERR_CUDA,    \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+  } while (0)
+
+MultiEngine::~MultiEngine() {
+  cudaSetDevice(device_);
+  cudaStreamSynchronize(st_);
+  for (auto &p : slots_)
+    if (p && p->mem) cudaFreeAsync(p->mem, st_);
+  cudaStreamSynchronize(st_);
+}
+
+int MultiEngine::live() const {
+  int n = 0;
+  for (const auto &p : slots_) n += p ? 1 : 0;
+  return n;
+}
+
+int MultiEngine::add(const ccfv_problem &pr, int *slot) {
+  auto P = std::make_unique<Problem>();
+  std::string e;
+  int rc = problem_setup(*P, pr, &e);
+  if (rc) return fail(rc, e);
+  P->ctx = std::make_unique<ccfv_ctx>();
+  P->ctx->grid = P->g;
+  P->ctx->device = device_;
+  for (int t = 0; t < 4; ++t) {
+    const int dir = t & 1;
+    const double Dt = (t < 2 ? P->dt : P->dtc) * (dir == 0 ? 0.5 : 1.0);
+    P->tab[t] = get_table(P->ctx.get(), dir, Dt, t < 2 ? true : P->g64, &rc);
+    if (!P->tab[t]) return fail(rc, P->ctx->last_error);
+  }
+  for (int kind = 0; kind < 3; ++kind)
+    for (int level = 0; level < 2; ++level) {
+      const int dir = kind == 1 ? 1 : 0;
+      const double Dt = (level == 0 ? P->dt : P->dtc) * (dir == 0 ? 0.5 : 1.0);
+      const int dsrc = (kind == 2 && P->g.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
+      const LaunchGeom G = step_geom(P->g, dir, Dt, dsrc, level == 0 || P->g64);
+      if (G.cs > MAX_CLUSTER) return fail(CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
+      if (std::max({sweep_smem_bytes(G.lc_max, G.halo, true), sweep_fast_smem_bytes(G.lc_max, G.halo, true),
+                    sweep_filter_smem_bytes(G.lc_max, G.halo, true)}) > 227 * 1024)
+        return fail(CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
+    }
+  MCK(cudaMallocAsync(&P->mem, P->bytes, st_));
+  unsigned char *q = static_cast<unsigned char *>(P->mem);
+  auto take = [&](size_t b) {
+    unsigned char *r = q;
+    q += (b + 255) & ~size_t(255);
+    return r;
+  };
+  const size_t fb = sizeof(double) * P->NN;
+  P->U = reinterpret_cast<double *>(take(fb * (P->S + 1)));
+  P->F = reinterpret_cast<double *>(take(fb * (P->S + 1)));
+  P->Gold = P->o.form == CCFV_FORM_STANDARD ? reinterpret_cast<double *>(take(fb * (P->S + 1))) : nullptr;
+  P->W = take(P->g64 ? fb : fb / 2);
+  MCK(cudaMemcpyAsync(P->U, P->C0, fb,
+                      P->o.mem == CCFV_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st_));
+  int s = -1;
+  for (int i = 0; i < (int)slots_.size(); ++i)
+    if (!slots_[i]) { s = i; break; }
+  if (s < 0) {
+    s = (int)slots_.size();
+    slots_.emplace_back();
+  }
+  slots_[s] = std::move(P);
+  dirty_ = true;
+  if (slot) *slot = s;
+  return CCFV_OK;
+}
+
+int MultiEngine::finish(int slot) {
+  Problem *P = get(slot);
+  if (!P) return fail(CCFV_ERR_NOT_FOUND, "no such problem");
+  MCK(cudaMemcpyAsync(P->C_T, P->U + (size_t)P->S * P->NN, sizeof(double) * P->NN,
+                      P->o.mem == CCFV_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st_));
+  return CCFV_OK;
+}
+
+void MultiEngine::remove(int slot) {
+  Problem *P = get(slot);
+  if (!P) return;
+  if (P->mem) cudaFreeAsync(P->mem, st_);
+  slots_[slot].reset();
+  dirty_ = true;
+}
+
+// Rebuilds the launch classes, element-wise descriptors and norm offsets
+// after problems joined or left.
+int MultiEngine::rebuild() {
+  fine_.clear();
+  coarse_.clear();
+  const int n = (int)slots_.size();
+  std::vector<BElem> he(n);
+  norm_off_.assign(n, 0);
+  size_t noff = 0;
+  for (int i = 0; i < n; ++i) {
+    Problem *P = slots_[i].get();
+    if (!P) {
+      std::memset(&he[i], 0, sizeof(BElem));
+      continue;
+    }
+    norm_off_[i] = noff;
+    noff += 2 * (size_t)(P->S + 1);
+  }
+  MCK(norms_d_.alloc(sizeof(double) * std::max<size_t>(noff, 2)));
+  hnorms_.assign(std::max<size_t>(noff, 2), 0.0);
+  for (int i = 0; i < n; ++i) {
+    Problem *P = slots_[i].get();
+    if (!P) continue;
+    const ccfv_grid &g = P->g;
+    he[i] = BElem{P->U, P->F, P->Gold, P->W, P->NN, P->S, P->o.form, P->g64 ? 1 : 0, 0,
+                  norms_d_.as<double>() + norm_off_[i]};
+    for (int kind = 0; kind < 3; ++kind) {
+      const int dir = kind == 1 ? 1 : 0;
+      const int dsrc = (kind == 2 && g.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
+      {  // fine: field s = F[s+1], time t0 + s DT (+ j dt per launch step)
+        const double Dt = kind == 1 ? P->dt : 0.5 * P->dt;
+        const double ta = kind == 2 ? 0.5 * P->dt : 0.0, tb = kind == 0 ? 0.5 * P->dt : P->dt;
+        for (int s = 0; s < P->S; ++s) {
+          SweepField f = make_field(g, dir, Dt, ta + P->o.t0 + s * P->DT, tb + P->o.t0 + s * P->DT,
+                                    P->F + (size_t)(s + 1) * P->NN, P->tab[dir], dsrc);
+          f.inst = i;
+          f.slice = s;
+          f.jmax = P->J;
+          f.t_step = P->dt;
+          add_field(fine_, kind, g, f, true);
+        }
+      }
+      {  // coarse: the work field W, slice from the launch (t0 + n DT + i dtc)
+        const double Dt = kind == 1 ? P->dtc : 0.5 * P->dtc;
+        const double ta = kind == 2 ? 0.5 * P->dtc : 0.0, tb = kind == 0 ? 0.5 * P->dtc : P->dtc;
+        SweepField f = make_field(g, dir, Dt, ta + P->o.t0, tb + P->o.t0, P->W, P->tab[2 + dir], dsrc);
+        f.inst = i;
+        f.slice = -1;
+        f.jmax = P->m;
+        f.smax = P->S;
+        f.gskip = P->o.form == CCFV_FORM_DELTA ? 1 : 0;
+        f.t_step = P->dtc;
+        f.t_slice = P->DT;
+        add_field(coarse_, kind, g, f, P->g64);
+      }
+    }
+  }
+  for (auto *cls : {&fine_, &coarse_})
+    for (auto &kv : *cls) {
+      SweepClass &K = kv.second;
+      MCK(K.d.alloc(sizeof(SweepField) * K.h.size()));
+      MCK(cudaMemcpyAsync(K.d.p, K.h.data(), sizeof(SweepField) * K.h.size(), cudaMemcpyHostToDevice, st_));
+    }
+  const int eb = 148;
+  MCK(elems_.alloc(sizeof(BElem) * std::max(n, 1)));
+  if (n) MCK(cudaMemcpyAsync(elems_.p, he.data(), sizeof(BElem) * n, cudaMemcpyHostToDevice, st_));
+  MCK(nlo_d_.alloc(sizeof(int) * std::max(n, 1)));
+  MCK(partial_.alloc(sizeof(double) * 2 * eb * (size_t)std::max(n, 1)));
+  if (counters_.bytes < sizeof(unsigned) * std::max(n, 1)) {
+    MCK(counters_.alloc(sizeof(unsigned) * std::max(n, 1) * 2));
+    MCK(cudaMemsetAsync(counters_.p, 0, counters_.bytes, st_));
+  }
+  if (!status_.p) {
+    MCK(status_.alloc(sizeof(unsigned) * 4));
+    MCK(cudaMemsetAsync(status_.p, 0, sizeof(unsigned) * 4, st_));
+  }
+  MCK(cudaStreamSynchronize(st_));  // host staging vectors are reused
+  nlo_.assign(n, 0);
+  dirty_ = false;
+  return CCFV_OK;
+}
+
+int MultiEngine::push_nlo() {
+  if (!nlo_.empty())
+    MCK(cudaMemcpyAsync(nlo_d_.p, nlo_.data(), sizeof(int) * nlo_.size(), cudaMemcpyHostToDevice, st_));
+  return CCFV_OK;
+}
+
+int MultiEngine::elem(int op, int slice) {
+  const int n = (int)slots_.size();
+  if (!n) return CCFV_OK;
+  count_launch();
+  batch_elem_kernel<<<dim3(148, n), BT, 0, st_>>>(op, elems_.as<BElem>(), slice, nlo_d_.as<int>(),
+                                                   partial_.as<double>(), counters_.as<unsigned>());
+  MCK(cudaGetLastError());
+  return CCFV_OK;
+}
+
+int MultiEngine::sweeps(std::map<KKey, SweepClass> &classes, int kind, int jstep, int nslice) {
+  BatchStep bs;
+  bs.jstep = jstep;
+  bs.nslice = nslice;
+  bs.nlo = nlo_d_.as<int>();
+  unsigned *status = status_.as<unsigned>();
+  for (auto &kv : classes) {
+    SweepClass &K = kv.second;
+    if (K.kind != kind) continue;
+    cudaError_t e =
+        K.fp64 ? launch_sweep_batch<double>(K.variant, K.d.as<SweepField>(), (int)K.h.size(), 0, K.groups,
+                                            K.cs, K.lc_max, K.halo, bs, status, st_)
+               : launch_sweep_batch<float>(K.variant, K.d.as<SweepField>(), (int)K.h.size(), 0, K.groups,
+                                           K.cs, K.lc_max, K.halo, bs, status, st_);
+    MCK(e);
+  }
+  return CCFV_OK;
+}
+
+int MultiEngine::coarse_slice(int s, int mmax) {
+  for (int i = 0; i < mmax; ++i)
+    for (int kind = 0; kind < 3; ++kind)
+      if (int rc = sweeps(coarse_, kind, i, s)) return rc;
+  return CCFV_OK;
+}
+
+int MultiEngine::iterate(std::vector<int> *finished) {
+  if (finished) finished->clear();
+  if (dirty_)
+    if (int rc = rebuild()) return rc;
+  const int n = (int)slots_.size();
+  cudaEvent_t e0, e1;
+  MCK(cudaEventCreate(&e0));
+  MCK(cudaEventCreate(&e1));
+  MCK(cudaEventRecord(e0, st_));
+  // first coarse sweep U[s+1] = G(U[s]) of newly admitted problems
+  // (T2S4:1271-1280); nlo = -1: every slice active, G starts from U
+  int Snew = 0, mnew = 0;
+  for (int i = 0; i < n; ++i) {
+    Problem *P = slots_[i].get();
+    const bool fresh = P && P->state == Problem::NEW;
+    nlo_[i] = fresh ? -1 : (P ? P->S : 0);
+    if (fresh) {
+      Snew = std::max(Snew, P->S);
+      mnew = std::max(mnew, P->m);
+    }
+  }
+  if (Snew) {
+    if (int rc = push_nlo()) return rc;
+    for (int s = 0; s < Snew; ++s) {
+      int rc = elem(OP_LOAD_W, s);
+      if (!rc) rc = coarse_slice(s, mnew);
+      if (!rc) rc = elem(OP_STORE_W, s);
+      if (rc) return rc;
+    }
+    for (auto &p : slots_)
+      if (p && p->state == Problem::NEW) {
+        p->state = Problem::RUNNING;
+        p->coarse_cu += (double)p->S * p->m * p->NN;
+      }
+  }
+  // one Parareal iteration of every running problem; iteration k+1 leaves
+  // slices < k untouched (already exact)
+  int Smax = 0, Jmax = 0, mmax = 0, running = 0;
+  bool any_std = false;
+  for (int i = 0; i < n; ++i) {
+    Problem *P = slots_[i].get();
+    if (P && P->state == Problem::RUNNING) {
+      nlo_[i] = P->k;
+      Smax = std::max(Smax, P->S);
+      Jmax = std::max(Jmax, P->J);
+      mmax = std::max(mmax, P->m);
+      any_std |= P->o.form == CCFV_FORM_STANDARD;
+      ++running;
+      P->fine_cu += (double)(P->S - P->k) * P->J * P->NN;
+      P->coarse_cu += (double)(P->S - P->k - (P->o.form == CCFV_FORM_DELTA ? 1 : 0)) * P->m * P->NN;
+    } else {
+      nlo_[i] = P ? P->S : 0;
+    }
+  }
+  if (running) {
+    if (int rc = push_nlo()) return rc;
+    if (int rc = elem(OP_COPY_F, 0)) return rc;
+    for (int j = 0; j < Jmax; ++j)
+      for (int kind = 0; kind < 3; ++kind)
+        if (int rc = sweeps(fine_, kind, j, 0)) return rc;
+    for (int s = 0; s < Smax; ++s) {
+      int rc = any_std ? elem(OP_LOAD_W_STD, s) : CCFV_OK;
+      if (!rc) rc = coarse_slice(s, mmax);
+      if (!rc) rc = elem(OP_CORRECT, s);
+      if (rc) return rc;
+    }
+    MCK(cudaMemcpyAsync(hnorms_.data(), norms_d_.p, sizeof(double) * hnorms_.size(),
+                        cudaMemcpyDeviceToHost, st_));
+  }
+  MCK(cudaEventRecord(e1, st_));
+  MCK(cudaStreamSynchronize(st_));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  ms_ += ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  unsigned flag = 0;
+  MCK(cudaMemcpy(&flag, status_.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (flag) return fail(CCFV_ERR_HALO, "a characteristic foot left the staged halo");
+  for (int i = 0; i < n; ++i) {
+    Problem *P = slots_[i].get();
+    if (!P || P->state != Problem::RUNNING) continue;
+    const double *hn = hnorms_.data() + norm_off_[i];
+    double worst = 0.0;
+    for (int s = P->k + 1; s <= P->S; ++s) {
+      const double e = std::sqrt(hn[2 * s]), u = std::sqrt(hn[2 * s + 1]);
+      worst = std::max(worst, u > 0 ? e / u : e);
+    }
+    P->upd[P->k] = worst;
+    P->k += 1;
+    if (P->o.tol > 0 && worst < P->o.tol) P->converged = 1;
+    if (P->converged || P->k >= P->o.kmax || P->k >= P->S) {
+      // after S iterations Parareal equals the serial fine solve exactly
+      P->state = Problem::DONE;
+      if (finished) finished->push_back(i);
+    }
+  }
+  return CCFV_OK;
+}
+
+void fill_stats(const Problem &P, ccfv_stats *s, double ms) {
+  std::memset(s, 0, sizeof(*s));
+  s->iterations = P.k;
+  s->converged = P.converged;
+  for (int k = 0; k < P.k && k < CCFV_MAX_ITERS; ++k) s->update[k] = P.upd[k];
+  s->fine_cell_updates = P.fine_cu;
+  s->coarse_cell_updates = P.coarse_cu;
+  s->ms = ms;
+}
+
+int batch_solve(int n, const ccfv_problem *probs, ccfv_stats *stats, int device, cudaStream_t st,
+                std::string *errmsg) {
+  if (cudaSetDevice(device) != cudaSuccess) return CCFV_ERR_CUDA;
+  MultiEngine E(device, st);
+  std::vector<int> slot(n, -1);
+  auto bail = [&](int rc) {
+    if (errmsg) *errmsg = E.error();
+    return rc;
+  };
+  for (int i = 0; i < n; ++i)
+    if (int rc = E.add(probs[i], &slot[i])) return bail(rc);
+  std::vector<int> fin;
+  int remaining = n;
+  while (remaining > 0) {
+    if (int rc = E.iterate(&fin)) return bail(rc);
+    for (int sl : fin) {
+      if (int rc = E.finish(sl)) return bail(rc);
+      --remaining;
+    }
+    if (E.live() == 0) break;
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess) return bail(CCFV_ERR_CUDA);
+  if (stats)
+    for (int i = 0; i < n; ++i) fill_stats(*E.get(slot[i]), &stats[i], E.device_ms());
+  return CCFV_OK;
+}
+
+}  // namespace ccfv

@@ -1,0 +1,103 @@
+// multi.h -- incremental multi-problem Parareal engine (batched solves and the
+// serving loop).
+#pragma once
+
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "engine.h"
+
+namespace ccfv {
+
+// One live problem.  Its slice states stay resident on the device from
+// admission until it finishes.
+struct Problem {
+  ccfv_grid g;
+  ccfv_parareal_opts o;
+  const double *C0 = nullptr;
+  double *C_T = nullptr;
+  int S = 0, J = 0, m = 0;
+  double DT = 0, dt = 0, dtc = 0;
+  long long NN = 0;
+  bool g64 = true;
+  void *mem = nullptr;       // cudaMallocAsync arena: U, F, Gold, W
+  size_t bytes = 0;
+  double *U = nullptr, *F = nullptr, *Gold = nullptr;
+  void *W = nullptr;
+  std::unique_ptr<ccfv_ctx> ctx;  // owns the solver tables of this grid
+  const SolverTable *tab[4] = {};  // fine x, fine y, coarse x, coarse y
+  enum { NEW, RUNNING, DONE } state = NEW;
+  int k = 0;                 // iterations done
+  int converged = 0;
+  double upd[CCFV_MAX_ITERS] = {};
+  double fine_cu = 0, coarse_cu = 0;
+};
+
+// Fills the public stats of a finished problem (ms: caller-defined time).
+void fill_stats(const Problem &P, ccfv_stats *s, double ms);
+// Device bytes a problem keeps resident (slice states and work field).
+size_t problem_bytes(const ccfv_grid &g, const ccfv_parareal_opts &o);
+// Validates options and fills the derived sizes; no device work.
+int problem_setup(Problem &P, const ccfv_problem &p, std::string *err);
+
+struct SweepClass {
+  int kind = 0, variant = 0, cs = 1, lc_max = 0, halo = 0, fp64 = 1;
+  std::vector<SweepField> h;
+  DevBuf d;
+  int groups = 0;
+};
+
+class MultiEngine {
+ public:
+  MultiEngine(int device, cudaStream_t st) : device_(device), st_(st) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;  // keep released problem states cached in the pool
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+  }
+  ~MultiEngine();
+  // Admits a problem (allocates its states stream-ordered, uploads C0).
+  int add(const ccfv_problem &p, int *slot);
+  // Copies the final state of a finished problem into its C_T (stream-ordered).
+  int finish(int slot);
+  // Releases a problem's device memory.
+  void remove(int slot);
+  // One engine step: the first coarse sweep of newly admitted problems, then
+  // one Parareal iteration of every running problem.  `finished` receives the
+  // slots whose problems converged or reached kmax in this step.
+  int iterate(std::vector<int> *finished);
+  Problem *get(int slot) { return slot >= 0 && slot < (int)slots_.size() ? slots_[slot].get() : nullptr; }
+  int live() const;
+  const std::string &error() const { return err_; }
+  double device_ms() const { return ms_; }
+
+ private:
+  int rebuild();
+  int push_nlo();
+  int elem(int op, int slice);
+  int sweeps(std::map<std::tuple<int, int, int, int, int>, SweepClass> &cls, int kind, int jstep,
+             int nslice);
+  int coarse_slice(int s, int mmax);
+  int fail(int code, const std::string &msg) {
+    err_ = msg;
+    return code;
+  }
+
+  int device_;
+  cudaStream_t st_;
+  std::vector<std::unique_ptr<Problem>> slots_;
+  bool dirty_ = true;
+  std::map<std::tuple<int, int, int, int, int>, SweepClass> fine_, coarse_;
+  DevBuf elems_, nlo_d_, partial_, counters_, status_, norms_d_;
+  std::vector<int> nlo_;
+  std::vector<size_t> norm_off_;
+  std::vector<double> hnorms_;
+  std::string err_;
+  double ms_ = 0;
+};
+
+}  // namespace ccfv

@@ -13,7 +13,7 @@
 // Limits and rules (also stated in include/ccfv.h):
 //  - nx, ny <= NOALLOC_MAX_LINE (4096); larger grids are rejected with
 //    CCFV_ERR_UNSUPPORTED before any device work.
-//  - Every GPU that loads this library holds the array (about 200 KB) until
+//  - Every GPU that loads this library holds the array (about 340 KB) until
 //    the process exits.
 //  - The first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current; make that first call
@@ -33,7 +33,10 @@ namespace {
 
 constexpr int NOALLOC_MAX_LINE = 4096;
 constexpr size_t NOALLOC_HDR = 1024;  // status word + 3 sweep descriptors
-constexpr size_t NOALLOC_TAB = 3 * (size_t)NOALLOC_MAX_LINE * sizeof(double);
+// solver table of one direction (layout of table_len(): factors, chunk products)
+constexpr size_t NOALLOC_TAB_LEN =
+    5 * (size_t)NOALLOC_MAX_LINE + (size_t)MAX_CLUSTER * NCH + (size_t)MAX_CLUSTER * (NCH + 1);
+constexpr size_t NOALLOC_TAB = NOALLOC_TAB_LEN * sizeof(double);
 constexpr size_t NOALLOC_BYTES = NOALLOC_HDR + 2 * NOALLOC_TAB;
 static_assert(sizeof(SweepField) * 3 + 256 <= NOALLOC_HDR, "descriptor area too small");
 
@@ -41,7 +44,7 @@ static_assert(sizeof(SweepField) * 3 + 256 <= NOALLOC_HDR, "descriptor area too 
 __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
 // Host staging (static, never heap-allocated).
-double h_tab[2][3 * NOALLOC_MAX_LINE];
+double h_tab[2][NOALLOC_TAB_LEN];
 SweepField h_fields[3];
 
 constexpr int MAX_DEVICES = 64;
@@ -83,6 +86,7 @@ void table_static(int L, double coA, double coB, int bc, double *out, double *sm
     *sm_fac = coA / gam;
     *sm_inv_den = 1.0 / (1.0 + z[0] + *sm_fac * z[L - 1]);
   }
+  fill_chunk_products(L, out);
 }
 
 int shift_of(const ccfv_grid &g, int dir, double Dt) {
@@ -179,9 +183,11 @@ extern "C" int ccfv_step_noalloc(const ccfv_grid *grid, double *d_C, double tn, 
   }
   cudaError_t e = cudaMemsetAsync(d_status, 0, sizeof(unsigned), st);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(d_tab[0], h_tab[0], sizeof(double) * 3 * g.nx, cudaMemcpyHostToDevice, st);
+    e = cudaMemcpyAsync(d_tab[0], h_tab[0], sizeof(double) * table_len(g.nx),
+                        cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(d_tab[1], h_tab[1], sizeof(double) * 3 * g.ny, cudaMemcpyHostToDevice, st);
+    e = cudaMemcpyAsync(d_tab[1], h_tab[1], sizeof(double) * table_len(g.ny),
+                        cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(d_fields, h_fields, sizeof(h_fields), cudaMemcpyHostToDevice, st);
   for (int kind = 0; kind < 3 && e == cudaSuccess; ++kind) {

@@ -78,6 +78,20 @@ __device__ __forceinline__ double edge_foot(const SweepField &f, int e, double t
   return 0.5 * (corner_foot(f, s, tau0, ta, tb) + corner_foot(f, s, tau1, ta, tb));
 }
 
+// Whether a field takes part in a batched launch, and its launch time offset.
+__device__ __forceinline__ bool field_active(const SweepField &f, int jstep, int nslice,
+                                             const int *nlo) {
+  if (f.jmax > 0 && jstep >= f.jmax) return false;
+  if (!nlo) return true;
+  const int lo = nlo[f.inst];
+  if (f.slice >= 0) return f.slice >= lo;
+  return nslice < f.smax && nslice >= lo + f.gskip;
+}
+__device__ __forceinline__ double field_time(const SweepField &f, double toff, int jstep,
+                                             int nslice) {
+  return toff + jstep * f.t_step + (f.slice < 0 ? nslice * f.t_slice : 0.0);
+}
+
 // Bounds-checked view of one line in the shared tile, indexed by position.
 template <typename T>
 struct LineView {
@@ -276,7 +290,8 @@ template <typename T>
 __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restrict__ fields,
                                                     int nfields, int group_base, double toff,
                                                     void *data_override, int lc_max, int H,
-                                                    unsigned *status) {
+                                                    unsigned *status, int jstep, int nslice,
+                                                    const int *nlo) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cg::cluster_group cluster = cg::this_cluster();
   const int cs = (int)cluster.num_blocks();
@@ -296,6 +311,8 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
   }
   __syncthreads();
   const SweepField &F = *S.fd;
+  if (!field_active(F, jstep, nslice, nlo)) return;  // uniform over the cluster
+  toff = field_time(F, toff, jstep, nslice);
   const int L = F.L;
   const int g = tile - F.group0;
   const long long line0 = (long long)g * LPG;
@@ -641,47 +658,28 @@ __device__ __forceinline__ void cp_async4(void *sdst, const void *gsrc) {
   unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gsrc) : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all_committed() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Stage rows p0-H .. p1+H-1 of LPG lines into Cs[row][line] with cp.async
-// (wrapped positions for periodic lines, zeros elsewhere).
-template <typename T>
-__device__ __forceinline__ void stage_async(const SweepField &F, T *Cs, int p0, int np, int H,
-                                            long long line0) {
-  const int nrows = np + 2 * H;
-  const int total = nrows * LPG;
-  const int L = F.L;
-  const bool xs = (F.s_line == 1);
-  const T *gdata = reinterpret_cast<const T *>(F.data);
-  for (int e = threadIdx.x; e < total; e += NTH) {
-    int row, ln;
-    if (xs) { row = e / LPG; ln = e - row * LPG; }
-    else { ln = e / nrows; row = e - ln * nrows; }
-    int pos = p0 - H + row;
-    const long long gl = line0 + ln;
-    T *dst = Cs + row * PITCH + ln;
-    if (gl < F.M) {
-      if (pos < 0 || pos >= L) { pos %= L; if (pos < 0) pos += L; }
-      const T *src = gdata + (long long)pos * F.s_pos + gl * F.s_line;
-      if (sizeof(T) == 8) cp_async8(dst, src); else cp_async4(dst, src);
-    } else {
-      *dst = T(0);
-    }
-  }
-  cp_async_wait_all();
-}
+static_assert(sizeof(SweepField) <= 256 && sizeof(SweepField) % 8 == 0, "descriptor slot");
 
 template <typename T>
 struct FastSmem {
   T *C;      // [(lc_max + 2H) * PITCH]
   T *Q;      // [lc_max * PITCH]   q, then x (row = position - p0)
-  T *tA, *tG, *tZ, *tP, *tS;  // [lc_max] factors, chunk prefix/suffix products
+  T *tA, *tG, *tZ, *tP, *tS;  // [lc_max] factors and chunk prefix/suffix products
   T *aggA;   // [NCH]        chunk products (line-invariant)
+  T *PA;     // [NCH + 1]    CTA-local exclusive prefix products of the chunks
   T *aggF;   // [NCH * LPG]  chunk forward values
   T *aggR;   // [NCH * LPG]  chunk backward values
+  T *om;     // [6 * LPG]    per-line stencil weights
+  T *cin;    // [2 * LPG]    per-line carries from the other CTAs of the cluster
   T *xch;    // [8 * LPG]    cluster exchange
+  int *n0;   // [LPG]        per-line foot offset
   SweepField *fd;
 };
 
@@ -689,7 +687,8 @@ template <typename T>
 __device__ __forceinline__ FastSmem<T> carve_fast(unsigned char *raw, int lc_max, int H) {
   FastSmem<T> s;
   s.fd = reinterpret_cast<SweepField *>(raw);
-  T *p = reinterpret_cast<T *>(raw + ((sizeof(SweepField) + 15) & ~size_t(15)));
+  s.n0 = reinterpret_cast<int *>(raw + 256);
+  T *p = reinterpret_cast<T *>(raw + 256 + 64 * sizeof(int));
   s.C = p; p += (lc_max + 2 * H) * PITCH;
   s.Q = p; p += lc_max * PITCH;
   s.tA = p; p += lc_max;
@@ -698,8 +697,11 @@ __device__ __forceinline__ FastSmem<T> carve_fast(unsigned char *raw, int lc_max
   s.tP = p; p += lc_max;
   s.tS = p; p += lc_max;
   s.aggA = p; p += NCH;
+  s.PA = p; p += NCH + 1;
   s.aggF = p; p += NCH * LPG;
   s.aggR = p; p += NCH * LPG;
+  s.om = p; p += 6 * LPG;
+  s.cin = p; p += 2 * LPG;
   s.xch = p;
   return s;
 }
@@ -707,24 +709,32 @@ __device__ __forceinline__ FastSmem<T> carve_fast(unsigned char *raw, int lc_max
 template <typename T>
 __global__ void __launch_bounds__(NTH, 2)
     sweep_fast_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
-                      double toff, void *data_override, int lc_max, int H, unsigned *status) {
+                      double toff, void *data_override, int lc_max, int H, unsigned *status,
+                      int jstep, int nslice, const int *nlo) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cg::cluster_group cluster = cg::this_cluster();
   const int cs = (int)cluster.num_blocks();
   const int rank = (int)cluster.block_rank();
   const int tile = blockIdx.x / cs + group_base;
   FastSmem<T> S = carve_fast<T>(smem_raw, lc_max, H);
-  if (threadIdx.x == 0) {
+  {
+    // every thread finds the field; the descriptor is copied cooperatively
     int lo = 0, hi = nfields - 1;
     while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if (fields[mid].group0 <= tile) lo = mid; else hi = mid - 1;
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(&fields[mid].group0) <= tile) lo = mid; else hi = mid - 1;
     }
-    *S.fd = fields[lo];
-    if (data_override) S.fd->data = data_override;
+    constexpr int NW8 = (int)(sizeof(SweepField) / 8);
+    if (threadIdx.x < NW8)
+      reinterpret_cast<long long *>(S.fd)[threadIdx.x] =
+          __ldg(reinterpret_cast<const long long *>(&fields[lo]) + threadIdx.x);
   }
   __syncthreads();
+  if (threadIdx.x == 0 && data_override) S.fd->data = data_override;
+  __syncthreads();
   const SweepField &F = *S.fd;
+  if (!field_active(F, jstep, nslice, nlo)) return;  // uniform over the cluster
+  toff = field_time(F, toff, jstep, nslice);
   const int L = F.L;
   const long long line0 = (long long)(tile - F.group0) * LPG;
   const int Lc = (L + cs - 1) / cs;
@@ -732,19 +742,88 @@ __global__ void __launch_bounds__(NTH, 2)
   const int p1 = min(L, p0 + Lc);
   const int np = p1 - p0;
   const int nrows = np + 2 * H;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  stage_async(F, S.C, p0, np, H, line0);
+  // ---- stage the tile (cp.async, no integer division) ----
   {
+    const T *gdata = reinterpret_cast<const T *>(F.data);
+    if (F.s_line == 1) {
+      // x-sweep: a warp copies two rows of 16 consecutive doubles per step
+      const int ln = lane & (LPG - 1);
+      const long long gl = line0 + ln;
+      const bool okl = gl < F.M;
+      for (int row = warp * 2 + (lane >> 4); row < nrows; row += 2 * NW) {
+        int pos = p0 - H + row;
+        if (pos < 0 || pos >= L) { pos %= L; if (pos < 0) pos += L; }
+        T *dst = S.C + row * PITCH + ln;
+        if (okl) {
+          const T *src = gdata + (long long)pos * F.s_pos + gl;
+          if (sizeof(T) == 8) cp_async8(dst, src); else cp_async4(dst, src);
+        } else {
+          *dst = T(0);
+        }
+      }
+    } else {
+      // y-sweep: a warp copies 32 consecutive cells of one line per step
+      for (int ln = warp; ln < LPG; ln += NW) {
+        const long long gl = line0 + ln;
+        const bool okl = gl < F.M;
+        const T *lbase = gdata + gl * F.s_line;
+        for (int row = lane; row < nrows; row += 32) {
+          int pos = p0 - H + row;
+          if (pos < 0 || pos >= L) { pos %= L; if (pos < 0) pos += L; }
+          T *dst = S.C + row * PITCH + ln;
+          if (okl) {
+            if (sizeof(T) == 8) cp_async8(dst, lbase + pos); else cp_async4(dst, lbase + pos);
+          } else {
+            *dst = T(0);
+          }
+        }
+      }
+    }
+    cp_async_commit();
+    // solver factors and chunk products of this CTA's positions
     const T *tab = reinterpret_cast<const T *>(F.tab);
     for (int k = threadIdx.x; k < np; k += NTH) {
       S.tA[k] = tab[p0 + k];
       S.tG[k] = tab[L + p0 + k];
       S.tZ[k] = tab[2 * L + p0 + k];
+      S.tP[k] = tab[3 * L + p0 + k];
+      S.tS[k] = tab[4 * L + p0 + k];
     }
+    if (threadIdx.x < NCH) S.aggA[threadIdx.x] = tab[5 * L + rank * NCH + threadIdx.x];
+    if (threadIdx.x <= NCH)
+      S.PA[threadIdx.x] = tab[5 * L + cs * NCH + rank * (NCH + 1) + threadIdx.x];
+    // per-line stencil: b_k = sum_t om_t C_{k+n0+t}, t = -2..3 (see sweep_kernel)
+    if (threadIdx.x < LPG) {
+      const int l = threadIdx.x;
+      const long long gl = line0 + l;
+      const double tau0 = F.t_min + F.ht * (double)gl;
+      const double tau1 = F.t_min + F.ht * (double)(gl + 1);
+      const double f0 = edge_foot(F, 0, tau0, tau1, toff + F.ta_rel, toff + F.tb_rel);
+      const double u = (f0 - F.s_min) / F.h;
+      const double fl = floor(u);
+      S.n0[l] = (int)fl;
+      const double x = u - fl, x2 = x * x, x3 = x2 * x;
+      const double A = x - 2.0 * x2 + x3, B = x3 - x2, Cc = 3.0 * x2 - 2.0 * x3;
+      const double kq = F.kb * F.inv12h;
+      const double pm2 = 2.0 * x3 - 6.0 * x2 + 3.0 * x + 1.0;
+      const double pm1 = -8.0 * x3 + 18.0 * x2 + 6.0 * x - 15.0;
+      const double pz = 12.0 * x3 - 18.0 * x2 - 24.0 * x + 15.0;
+      const double pp1 = -8.0 * x3 + 6.0 * x2 + 18.0 * x - 1.0;
+      const double pp2 = 2.0 * x3 - 3.0 * x;
+      T *om = S.om + 6 * l;
+      om[0] = T(A / 12.0 - kq * pm2);
+      om[1] = T((B - 8.0 * A) / 12.0 + kq * (pm2 - pm1));
+      om[2] = T(1.0 - Cc - 2.0 * B / 3.0 + kq * (pm1 - pz));
+      om[3] = T(Cc + 2.0 * A / 3.0 + kq * (pz - pp1));
+      om[4] = T((8.0 * B - A) / 12.0 + kq * (pp1 - pp2));
+      om[5] = T(-B / 12.0 + kq * pp2);
+    }
+    cp_async_wait_all_committed();
   }
   __syncthreads();
 
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int ln = lane % LPG;
   const int c = warp * CPW + lane / LPG;
   const long long gl = line0 + ln;
@@ -752,16 +831,276 @@ __global__ void __launch_bounds__(NTH, 2)
   const int s = min(p1, p0 + c * m);
   const int e = min(p1, s + m);
 
-  // per-line stencil: b_k = sum_t om_t C_{k+n0+t}, t = -2..3
-  T om[6];
-  int n0;
+  // ---- fused RHS + compact mass matrix + local forward recurrence ----
   {
+    T q = T(0);
+    if (s < e) {
+      const int n0 = S.n0[ln];
+      const int r0 = (s - 1) + n0 - 2 - p0 + H;   // row of tap -2 of cell s-1
+      const int rlast = e + n0 + 3 - p0 + H;       // row of tap +3 of cell e
+      if (r0 < 0 || rlast >= nrows) {
+        atomicOr(status, STATUS_HALO);
+      } else {
+        const T *omp = S.om + 6 * ln;
+        const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5];
+        const T *cp = S.C + r0 * PITCH + ln;
+        T w0 = cp[0], w1 = cp[PITCH], w2 = cp[2 * PITCH], w3 = cp[3 * PITCH],
+          w4 = cp[4 * PITCH], w5 = cp[5 * PITCH];
+        T bm = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
+        w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[6 * PITCH];
+        T bc = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
+        const T *nxt = cp + 7 * PITCH;
+        T *qp = S.Q + (s - p0) * PITCH + ln;
+        const T *ta = S.tA + (s - p0), *tg = S.tG + (s - p0);
+        const int n = e - s;
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) {
+          w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = nxt[i * PITCH];
+          const T bp = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
+          const T mb = (bp + T(10.0) * bc + bm) * T(1.0 / 12.0);
+          q = tg[i] * mb + ta[i] * q;
+          qp[i * PITCH] = q;
+          bm = bc;
+          bc = bp;
+        }
+      }
+    }
+    S.aggF[c * LPG + ln] = q;
+  }
+  __syncthreads();
+
+  // ---- forward carries: CTA prefix (this line) + cluster prefix ----
+  T carry;
+  {
+    T PB = T(0);
+    for (int j = 0; j < c; ++j) PB = S.aggA[j] * PB + S.aggF[j * LPG + ln];
+    if (cs > 1) {
+      T *xB = S.xch + LPG;
+      if (c == NCH - 1) xB[ln] = S.aggA[c] * PB + S.aggF[c * LPG + ln];
+      cluster.sync();
+      if (threadIdx.x < LPG) {  // compose the preceding CTAs once per line
+        const T *tab = reinterpret_cast<const T *>(F.tab);
+        const T *PAg = tab + 5 * L + cs * NCH;
+        T cin = T(0);
+        for (int r = 0; r < rank; ++r) {
+          const T *rb = cluster.map_shared_rank(xB, r);
+          cin = PAg[r * (NCH + 1) + NCH] * cin + rb[threadIdx.x];
+        }
+        S.cin[threadIdx.x] = cin;
+      }
+      __syncthreads();
+      carry = S.PA[c] * S.cin[ln] + PB;
+    } else {
+      carry = PB;
+    }
+  }
+  // ---- fused forward fix-up + local backward recurrence (reverse walk) ----
+  {
+    T x = T(0);
+    const int n = e - s;
+    T *qp = S.Q + (s - p0) * PITCH + ln;
+    const T *ta = S.tA + (s - p0), *tp = S.tP + (s - p0);
+#pragma unroll 4
+    for (int i = n - 1; i >= 0; --i) {
+      x = (qp[i * PITCH] + tp[i] * carry) + ta[i] * x;
+      qp[i * PITCH] = x;
+    }
+    S.aggR[c * LPG + ln] = x;
+  }
+  __syncthreads();
+  // ---- backward carries: CTA suffix + cluster suffix ----
+  T carry2;
+  {
+    T SB = T(0), SA = T(1);
+    for (int j = NCH - 1; j > c; --j) {
+      const T a = S.aggA[j];
+      SB = S.aggR[j * LPG + ln] + a * SB;
+      SA = a * SA;
+    }
+    if (cs > 1) {
+      T *xB = S.xch + 3 * LPG;
+      if (c == 0) xB[ln] = S.aggR[ln] + S.aggA[0] * SB;
+      cluster.sync();
+      if (threadIdx.x < LPG) {
+        const T *tab = reinterpret_cast<const T *>(F.tab);
+        const T *PAg = tab + 5 * L + cs * NCH;
+        T cin = T(0);
+        for (int r = cs - 1; r > rank; --r) {
+          const T *rb = cluster.map_shared_rank(xB, r);
+          cin = rb[threadIdx.x] + PAg[r * (NCH + 1) + NCH] * cin;
+        }
+        S.cin[LPG + threadIdx.x] = cin;
+      }
+      __syncthreads();
+      carry2 = SB + SA * S.cin[LPG + ln];
+    } else {
+      carry2 = SB;
+    }
+  }
+  // ---- cyclic correction (Sherman-Morrison): needs y_0 and y_{L-1} ----
+  T fct;
+  {
+    T *y0 = S.xch + 4 * LPG, *yL = S.xch + 5 * LPG;
+    if (p0 == 0 && s == p0 && s < e) y0[ln] = S.Q[ln] + S.tS[0] * carry2;
+    if (p1 == L && e == p1 && s < e) yL[ln] = S.Q[(np - 1) * PITCH + ln] + S.tS[np - 1] * carry2;
+    if (cs > 1) {
+      cluster.sync();
+      if (threadIdx.x < LPG) {
+        S.cin[threadIdx.x] = cluster.map_shared_rank(y0, 0)[threadIdx.x];
+        S.cin[LPG + threadIdx.x] = cluster.map_shared_rank(yL, cs - 1)[threadIdx.x];
+      }
+      __syncthreads();
+      fct = (S.cin[ln] + T(F.sm_fac) * S.cin[LPG + ln]) * T(F.sm_inv_den);
+    } else {
+      __syncthreads();
+      fct = (y0[ln] + T(F.sm_fac) * yL[ln]) * T(F.sm_inv_den);
+    }
+  }
+  // ---- backward fix-up + correction + store ----
+  T *gdata = reinterpret_cast<T *>(F.data);
+  {
+    const int n = e - s;
+    T *qp = S.Q + (s - p0) * PITCH + ln;
+    const T *ts = S.tS + (s - p0), *tz = S.tZ + (s - p0);
+    if (F.s_line == 1) {
+      // x-sweep: a half-warp writes 16 consecutive doubles of one row
+      if (gl < F.M) {
+        T *gp = gdata + (long long)s * F.s_pos + gl;
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) gp[i * F.s_pos] = qp[i * PITCH] + ts[i] * carry2 - fct * tz[i];
+      }
+    } else {
+#pragma unroll 4
+      for (int i = 0; i < n; ++i) qp[i * PITCH] = qp[i * PITCH] + ts[i] * carry2 - fct * tz[i];
+      __syncthreads();
+      for (int l2 = warp; l2 < LPG; l2 += NW) {
+        const long long gl2 = line0 + l2;
+        if (gl2 >= F.M) continue;
+        T *lbase = gdata + gl2 * F.s_line + p0;
+        for (int row = lane; row < np; row += 32) lbase[row] = S.Q[row * PITCH + l2];
+      }
+    }
+  }
+  if (cs > 1) cluster.sync();  // keep shared memory alive for remote readers
+}
+
+// ---------------------------------------------------------------------------
+// Filter path: uniform displacement + periodic cells + derivative of the
+// sweep input, for diffusion numbers where |mu| (below) is small enough.
+//
+// The cyclic constant system a x_{k-1} + b x_k + a x_{k+1} = r_k factors as
+// c (1 + mu S^-1)(1 + mu S) x = r with |mu| < 1, mu / (1 + mu^2) = a / b,
+// c = a / mu, so it is solved exactly by two first-order recurrences,
+//   w_k = r_k / c - mu w_{k-1},   x_k = w_k - mu x_{k+1},
+// whose periodic wrap-around needs no correction term.  A recurrence started
+// from zero J positions early agrees with the exact one to |mu|^J, and J is
+// chosen on the host so that |mu|^J is below the rounding of T.  Every chunk
+// therefore warms its recurrences up over the J positions before (forward) or
+// after (backward) it: no carries cross threads or CTAs, the CTAs of a line
+// are independent (no cluster), and no factor tables are needed.
+
+template <typename T>
+struct FiltSmem {
+  T *C;      // [(lc_max + 2H) * PITCH]  input cells, later w
+  T *R;      // [(lc_max + 2H) * PITCH]  compact RHS M b, later x
+  T *om;     // [6 * LPG]
+  int *n0;   // [LPG]
+  SweepField *fd;
+};
+
+template <typename T>
+__device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max, int H) {
+  FiltSmem<T> s;
+  s.fd = reinterpret_cast<SweepField *>(raw);
+  s.n0 = reinterpret_cast<int *>(raw + 256);
+  T *p = reinterpret_cast<T *>(raw + 256 + 64 * sizeof(int));
+  s.om = p; p += 6 * LPG;
+  s.C = p; p += (lc_max + 2 * H) * PITCH;
+  s.R = p;
+  return s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NTH, 3)
+    sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
+                        double toff, void *data_override, int lc_max, int H, unsigned *status,
+                        int jstep, int nslice, const int *nlo, int cs) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int rank = (int)(blockIdx.x % cs);
+  const int tile = (int)(blockIdx.x / cs) + group_base;
+  FiltSmem<T> S = carve_filt<T>(smem_raw, lc_max, H);
+  {
+    int lo = 0, hi = nfields - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(&fields[mid].group0) <= tile) lo = mid; else hi = mid - 1;
+    }
+    constexpr int NW8 = (int)(sizeof(SweepField) / 8);
+    if (threadIdx.x < NW8)
+      reinterpret_cast<long long *>(S.fd)[threadIdx.x] =
+          __ldg(reinterpret_cast<const long long *>(&fields[lo]) + threadIdx.x);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && data_override) S.fd->data = data_override;
+  __syncthreads();
+  const SweepField &F = *S.fd;
+  if (!field_active(F, jstep, nslice, nlo)) return;
+  toff = field_time(F, toff, jstep, nslice);
+  const int L = F.L;
+  const long long line0 = (long long)(tile - F.group0) * LPG;
+  const int Lc = (L + cs - 1) / cs;
+  const int p0 = min(L, rank * Lc);
+  const int p1 = min(L, p0 + Lc);
+  const int np = p1 - p0;
+  const int nrows = np + 2 * H;
+  const int J = F.jf;
+  const T mu = T(F.sm_fac), ic = T(F.sm_inv_den);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T *gdata = reinterpret_cast<T *>(F.data);
+
+  // ---- stage rows p0-H .. p1+H-1 (periodic wrap) ----
+  if (F.s_line == 1) {
+    const int ln = lane & (LPG - 1);
+    const long long gl = line0 + ln;
+    const bool okl = gl < F.M;
+    for (int row = warp * 2 + (lane >> 4); row < nrows; row += 2 * NW) {
+      int pos = p0 - H + row;
+      if (pos < 0 || pos >= L) { pos %= L; if (pos < 0) pos += L; }
+      T *dst = S.C + row * PITCH + ln;
+      if (okl) {
+        const T *src = gdata + (long long)pos * F.s_pos + gl;
+        if (sizeof(T) == 8) cp_async8(dst, src); else cp_async4(dst, src);
+      } else {
+        *dst = T(0);
+      }
+    }
+  } else {
+    for (int ln = warp; ln < LPG; ln += NW) {
+      const long long gl = line0 + ln;
+      const bool okl = gl < F.M;
+      const T *lbase = gdata + gl * F.s_line;
+      for (int row = lane; row < nrows; row += 32) {
+        int pos = p0 - H + row;
+        if (pos < 0 || pos >= L) { pos %= L; if (pos < 0) pos += L; }
+        T *dst = S.C + row * PITCH + ln;
+        if (okl) {
+          if (sizeof(T) == 8) cp_async8(dst, lbase + pos); else cp_async4(dst, lbase + pos);
+        } else {
+          *dst = T(0);
+        }
+      }
+    }
+  }
+  cp_async_commit();
+  if (threadIdx.x < LPG) {  // per-line stencil b_k = sum_t om_t C_{k+n0+t}
+    const int l = threadIdx.x;
+    const long long gl = line0 + l;
     const double tau0 = F.t_min + F.ht * (double)gl;
     const double tau1 = F.t_min + F.ht * (double)(gl + 1);
     const double f0 = edge_foot(F, 0, tau0, tau1, toff + F.ta_rel, toff + F.tb_rel);
     const double u = (f0 - F.s_min) / F.h;
     const double fl = floor(u);
-    n0 = (int)fl;
+    S.n0[l] = (int)fl;
     const double x = u - fl, x2 = x * x, x3 = x2 * x;
     const double A = x - 2.0 * x2 + x3, B = x3 - x2, Cc = 3.0 * x2 - 2.0 * x3;
     const double kq = F.kb * F.inv12h;
@@ -770,6 +1109,7 @@ __global__ void __launch_bounds__(NTH, 2)
     const double pz = 12.0 * x3 - 18.0 * x2 - 24.0 * x + 15.0;
     const double pp1 = -8.0 * x3 + 6.0 * x2 + 18.0 * x - 1.0;
     const double pp2 = 2.0 * x3 - 3.0 * x;
+    T *om = S.om + 6 * l;
     om[0] = T(A / 12.0 - kq * pm2);
     om[1] = T((B - 8.0 * A) / 12.0 + kq * (pm2 - pm1));
     om[2] = T(1.0 - Cc - 2.0 * B / 3.0 + kq * (pm1 - pz));
@@ -777,155 +1117,106 @@ __global__ void __launch_bounds__(NTH, 2)
     om[4] = T((8.0 * B - A) / 12.0 + kq * (pp1 - pp2));
     om[5] = T(-B / 12.0 + kq * pp2);
   }
+  cp_async_wait_all_committed();
+  __syncthreads();
 
-  // ---- fused RHS + compact mass matrix + local forward recurrence ----
+  const int ln = lane % LPG;
+  const int c = warp * CPW + lane / LPG;
+  const long long gl = line0 + ln;
+
+  // ---- phase 1: M b at positions p0-J .. p1+J-1 into R (row = pos - p0 + H) ----
   {
-    T A = T(1), q = T(0);
-    if (s < e) {
-      const int r0 = (s - 1) + n0 - 2 - p0 + H;   // row of tap -2 of cell s-1
-      const int rlast = e + n0 + 3 - p0 + H;       // row of tap +3 of cell e
+    const int q0 = p0 - J, nq = np + 2 * J;
+    const int m1 = (nq + NCH - 1) / NCH;
+    const int s1 = q0 + min(nq, c * m1), e1 = q0 + min(nq, (c + 1) * m1);
+    if (s1 < e1) {
+      const int n0 = S.n0[ln];
+      const int r0 = (s1 - 1) + n0 - 2 - p0 + H;  // row of tap -2 of cell s1-1
+      const int rlast = e1 + n0 + 3 - p0 + H;     // row of tap +3 of cell e1
       if (r0 < 0 || rlast >= nrows) {
         atomicOr(status, STATUS_HALO);
       } else {
+        const T *omp = S.om + 6 * ln;
+        const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5];
         const T *cp = S.C + r0 * PITCH + ln;
         T w0 = cp[0], w1 = cp[PITCH], w2 = cp[2 * PITCH], w3 = cp[3 * PITCH],
           w4 = cp[4 * PITCH], w5 = cp[5 * PITCH];
-        auto bval = [&]() {
-          return om[0] * w0 + om[1] * w1 + om[2] * w2 + om[3] * w3 + om[4] * w4 + om[5] * w5;
-        };
-        T bm = bval();
+        T bm = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
         w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[6 * PITCH];
-        T bc = bval();
+        T bc = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
         const T *nxt = cp + 7 * PITCH;
-        T *qp = S.Q + (s - p0) * PITCH + ln;
-        for (int k = s; k < e; ++k) {
-          w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = *nxt;
-          nxt += PITCH;
-          const T bp = bval();
-          const T mb = (bp + T(10.0) * bc + bm) * T(1.0 / 12.0);
-          const T a = S.tA[k - p0];
-          q = S.tG[k - p0] * mb + a * q;
-          A *= a;
-          *qp = q;
-          qp += PITCH;
-          if (ln == 0) S.tP[k - p0] = A;
+        T *rp = S.R + (s1 - p0 + H) * PITCH + ln;
+        const int n = e1 - s1;
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) {
+          w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = nxt[i * PITCH];
+          const T bp = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
+          rp[i * PITCH] = (bp + T(10.0) * bc + bm) * T(1.0 / 12.0);
           bm = bc;
           bc = bp;
         }
       }
     }
-    S.aggF[c * LPG + ln] = q;
-    if (ln == 0) S.aggA[c] = A;
   }
   __syncthreads();
-
-  // ---- forward carries ----
-  T carry;
+  // ---- phase 2: forward filter w at p0 .. p1+J-1 into C (warm-up J cells) ----
   {
-    T PA = T(1), PB = T(0);
-    for (int j = 0; j < c; ++j) {
-      const T a = S.aggA[j];
-      PB = a * PB + S.aggF[j * LPG + ln];
-      PA = a * PA;
-    }
-    T cin = T(0);
-    if (cs > 1) {
-      T *xA = S.xch, *xB = S.xch + LPG;
-      if (c == NCH - 1) {
-        const T a = S.aggA[c];
-        xA[ln] = a * PA;
-        xB[ln] = a * PB + S.aggF[c * LPG + ln];
-      }
-      cluster.sync();
-      for (int r = 0; r < rank; ++r) {
-        const T *ra = cluster.map_shared_rank(xA, r);
-        const T *rb = cluster.map_shared_rank(xB, r);
-        cin = ra[ln] * cin + rb[ln];
+    const int nq = np + J;
+    const int m2 = (nq + NCH - 1) / NCH;
+    const int s2 = p0 + min(nq, c * m2), e2 = p0 + min(nq, (c + 1) * m2);
+    if (s2 < e2) {
+      const T *rp = S.R + (s2 - J - p0 + H) * PITCH + ln;
+      T w = T(0);
+      for (int i = 0; i < J; ++i) w = ic * rp[i * PITCH] - mu * w;
+      rp += J * PITCH;
+      T *wp = S.C + (s2 - p0 + H) * PITCH + ln;
+      const int n = e2 - s2;
+#pragma unroll 4
+      for (int i = 0; i < n; ++i) {
+        w = ic * rp[i * PITCH] - mu * w;
+        wp[i * PITCH] = w;
       }
     }
-    carry = PA * cin + PB;
-  }
-  // ---- fused forward fix-up + local backward recurrence (reverse walk) ----
-  {
-    T x = T(0), Sp = T(1);
-    T *qp = S.Q + (e - 1 - p0) * PITCH + ln;
-    for (int k = e - 1; k >= s; --k) {
-      const T a = S.tA[k - p0];
-      x = (*qp + S.tP[k - p0] * carry) + a * x;
-      *qp = x;
-      qp -= PITCH;
-      Sp *= a;
-      if (ln == 0) S.tS[k - p0] = Sp;
-    }
-    S.aggR[c * LPG + ln] = x;
   }
   __syncthreads();
-  // ---- backward carries ----
-  T carry2;
+  // ---- phase 3: backward filter x at p0 .. p1-1 (warm-up J cells) + store ----
   {
-    T SA = T(1), SB = T(0);
-    for (int j = NCH - 1; j > c; --j) {
-      const T a = S.aggA[j];
-      SB = S.aggR[j * LPG + ln] + a * SB;
-      SA = a * SA;
-    }
-    T cin = T(0);
-    if (cs > 1) {
-      T *xA = S.xch + 2 * LPG, *xB = S.xch + 3 * LPG;
-      if (c == 0) {
-        const T a = S.aggA[0];
-        xA[ln] = a * SA;
-        xB[ln] = S.aggR[ln] + a * SB;
+    const int m3 = (np + NCH - 1) / NCH;
+    const int s3 = p0 + min(np, c * m3), e3 = p0 + min(np, (c + 1) * m3);
+    if (s3 < e3) {
+      const T *wp = S.C + (e3 - p0 + H) * PITCH + ln;
+      T x = T(0);
+      for (int i = J - 1; i >= 0; --i) x = wp[i * PITCH] - mu * x;
+      const int n = e3 - s3;
+      wp -= n * PITCH;
+      if (F.s_line == 1) {
+        if (gl < F.M) {
+          T *gp = gdata + (long long)s3 * F.s_pos + gl;
+#pragma unroll 4
+          for (int i = n - 1; i >= 0; --i) {
+            x = wp[i * PITCH] - mu * x;
+            gp[i * F.s_pos] = x;
+          }
+        }
+      } else {
+        T *xp = S.R + (s3 - p0) * PITCH + ln;
+#pragma unroll 4
+        for (int i = n - 1; i >= 0; --i) {
+          x = wp[i * PITCH] - mu * x;
+          xp[i * PITCH] = x;
+        }
       }
-      cluster.sync();
-      for (int r = cs - 1; r > rank; --r) {
-        const T *ra = cluster.map_shared_rank(xA, r);
-        const T *rb = cluster.map_shared_rank(xB, r);
-        cin = rb[ln] + ra[ln] * cin;
-      }
     }
-    carry2 = SB + SA * cin;
   }
-  // ---- cyclic correction (Sherman-Morrison): needs y_0 and y_{L-1} ----
-  T fct;
-  {
-    T *y0 = S.xch + 4 * LPG, *yL = S.xch + 5 * LPG;
-    if (p0 == 0 && s == p0 && s < e) y0[ln] = S.Q[ln] + S.tS[0] * carry2;
-    if (p1 == L && e == p1 && s < e) yL[ln] = S.Q[(np - 1) * PITCH + ln] + S.tS[np - 1] * carry2;
-    T a0, aL;
-    if (cs > 1) {
-      cluster.sync();
-      a0 = cluster.map_shared_rank(y0, 0)[ln];
-      aL = cluster.map_shared_rank(yL, cs - 1)[ln];
-    } else {
-      __syncthreads();
-      a0 = y0[ln];
-      aL = yL[ln];
-    }
-    fct = (a0 + T(F.sm_fac) * aL) * T(F.sm_inv_den);
-  }
-  // ---- backward fix-up + correction + store ----
-  T *gdata = reinterpret_cast<T *>(F.data);
-  if (F.s_line == 1) {
-    // x-sweep: a half-warp writes 16 consecutive doubles of one row
-    if (gl < F.M)
-      for (int k = s; k < e; ++k)
-        gdata[(long long)k * F.s_pos + gl] =
-            S.Q[(k - p0) * PITCH + ln] + S.tS[k - p0] * carry2 - fct * S.tZ[k - p0];
-  } else {
-    for (int k = s; k < e; ++k) {
-      T *qp = S.Q + (k - p0) * PITCH + ln;
-      *qp = *qp + S.tS[k - p0] * carry2 - fct * S.tZ[k - p0];
-    }
+  if (F.s_line != 1) {
     __syncthreads();
-    const int total = np * LPG;
-    for (int q = threadIdx.x; q < total; q += NTH) {
-      const int l2 = q / np, row = q - l2 * np;
+    for (int l2 = warp; l2 < LPG; l2 += NW) {
       const long long gl2 = line0 + l2;
-      if (gl2 < F.M) gdata[gl2 * F.s_line + (long long)(p0 + row)] = S.Q[row * PITCH + l2];
+      if (gl2 >= F.M) continue;
+      T *lbase = gdata + gl2 * F.s_line + p0;
+      for (int row = lane; row < np; row += 32) lbase[row] = S.R[row * PITCH + l2];
     }
   }
-  if (cs > 1) cluster.sync();  // keep shared memory alive for remote readers
 }
 
 }  // namespace
@@ -937,23 +1228,32 @@ size_t sweep_smem_bytes(int lc_max, int halo, bool fp64) {
   return ((sizeof(SweepField) + 15) & ~size_t(15)) + n * el;
 }
 
+size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64) {
+  size_t el = fp64 ? 8 : 4;
+  return 256 + 64 * sizeof(int) + (6 * (size_t)LPG + 2 * (size_t)(lc_max + 2 * halo) * PITCH) * el;
+}
+
 size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64) {
   size_t el = fp64 ? 8 : 4;
   size_t n = (size_t)(lc_max + 2 * halo) * PITCH + (size_t)lc_max * PITCH + 5 * (size_t)lc_max +
-             NCH + 2 * (size_t)NCH * LPG + 8 * (size_t)LPG;
-  return ((sizeof(SweepField) + 15) & ~size_t(15)) + n * el;
+             2 * (size_t)NCH + 1 + 2 * (size_t)NCH * LPG + 16 * (size_t)LPG;
+  return 256 + 64 * sizeof(int) + n * el;
 }
 
 template <typename T>
-cudaError_t launch_sweep(int variant, const SweepField *d_fields, int nfields, int group_base,
-                         int groups_total, int cs, int lc_max, int halo, double toff, void *data,
-                         unsigned *d_status, cudaStream_t stream) {
+static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfields,
+                               int group_base, int groups_total, int cs, int lc_max, int halo,
+                               double toff, void *data, unsigned *d_status, int jstep,
+                               int nslice, const int *nlo, cudaStream_t stream) {
   const bool fast = (variant == SWEEP_FAST);
-  const size_t smem = fast ? sweep_fast_smem_bytes(lc_max, halo, sizeof(T) == 8)
-                           : sweep_smem_bytes(lc_max, halo, sizeof(T) == 8);
+  const bool filt = (variant == SWEEP_FILTER);
+  const size_t smem = filt ? sweep_filter_smem_bytes(lc_max, halo, sizeof(T) == 8)
+                      : fast ? sweep_fast_smem_bytes(lc_max, halo, sizeof(T) == 8)
+                             : sweep_smem_bytes(lc_max, halo, sizeof(T) == 8);
   static bool configured = false;
   if (!configured) {
-    for (const void *fn : {(const void *)sweep_kernel<T>, (const void *)sweep_fast_kernel<T>}) {
+    for (const void *fn : {(const void *)sweep_kernel<T>, (const void *)sweep_fast_kernel<T>,
+                           (const void *)sweep_filter_kernel<T>}) {
       cudaError_t err =
           cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
       if (err != cudaSuccess) return err;
@@ -961,6 +1261,13 @@ cudaError_t launch_sweep(int variant, const SweepField *d_fields, int nfields, i
       if (err != cudaSuccess) return err;
     }
     configured = true;
+  }
+  if (groups_total <= 0) return cudaSuccess;
+  if (filt) {  // independent CTAs: no cluster
+    count_launch();
+    sweep_filter_kernel<T><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
+        d_fields, nfields, group_base, toff, data, lc_max, halo, d_status, jstep, nslice, nlo, cs);
+    return cudaGetLastError();
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(groups_total * cs), 1, 1);
@@ -977,14 +1284,34 @@ cudaError_t launch_sweep(int variant, const SweepField *d_fields, int nfields, i
   count_launch();
   if (fast)
     return cudaLaunchKernelEx(&cfg, sweep_fast_kernel<T>, d_fields, nfields, group_base, toff,
-                              data, lc_max, halo, d_status);
+                              data, lc_max, halo, d_status, jstep, nslice, nlo);
   return cudaLaunchKernelEx(&cfg, sweep_kernel<T>, d_fields, nfields, group_base, toff, data,
-                            lc_max, halo, d_status);
+                            lc_max, halo, d_status, jstep, nslice, nlo);
+}
+
+template <typename T>
+cudaError_t launch_sweep(int variant, const SweepField *d_fields, int nfields, int group_base,
+                         int groups_total, int cs, int lc_max, int halo, double toff, void *data,
+                         unsigned *d_status, cudaStream_t stream) {
+  return launch_impl<T>(variant, d_fields, nfields, group_base, groups_total, cs, lc_max, halo,
+                        toff, data, d_status, 0, 0, nullptr, stream);
+}
+
+template <typename T>
+cudaError_t launch_sweep_batch(int variant, const SweepField *d_fields, int nfields,
+                               int group_base, int groups_total, int cs, int lc_max, int halo,
+                               const BatchStep &bs, unsigned *d_status, cudaStream_t stream) {
+  return launch_impl<T>(variant, d_fields, nfields, group_base, groups_total, cs, lc_max, halo,
+                        0.0, nullptr, d_status, bs.jstep, bs.nslice, bs.nlo, stream);
 }
 
 template cudaError_t launch_sweep<double>(int, const SweepField *, int, int, int, int, int, int,
                                           double, void *, unsigned *, cudaStream_t);
 template cudaError_t launch_sweep<float>(int, const SweepField *, int, int, int, int, int, int,
                                          double, void *, unsigned *, cudaStream_t);
+template cudaError_t launch_sweep_batch<double>(int, const SweepField *, int, int, int, int, int,
+                                                int, const BatchStep &, unsigned *, cudaStream_t);
+template cudaError_t launch_sweep_batch<float>(int, const SweepField *, int, int, int, int, int,
+                                               int, const BatchStep &, unsigned *, cudaStream_t);
 
 }  // namespace ccfv

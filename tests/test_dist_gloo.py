@@ -1,0 +1,100 @@
+"""Slice-distributed Parareal (ccfv.dist) on CPU: two gloo ranks, the oracle
+as the compute backend.  The pipelined exchange (boundary states, increments,
+the max all-reduce of updates, the final broadcast) must reproduce the
+single-process Parareal of the oracle."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+N, T, NT, S, RATIO, KMAX = 24, 0.25, 48, 6, 2, 4
+VP = (2 * np.pi, 0.5, 0.5)
+
+
+class OracleSlices:
+    """Compute backend on the oracle (test only)."""
+
+    def __init__(self, O, g):
+        self.O, self.g = O, g
+
+    def zeros(self, n):
+        return torch.zeros(n, self.g.nx, self.g.ny, dtype=torch.float64)
+
+    def fine(self, fields, t0, slice_dt, DT, J):
+        for i in range(fields.shape[0]):
+            fields[i].copy_(torch.from_numpy(self.O.fine(self.g, fields[i].numpy(),
+                                                         t0 + i * slice_dt, DT, J)))
+
+    def coarse(self, field, t, DT, m):
+        field.copy_(torch.from_numpy(self.O.coarse(self.g, field.numpy(), t, DT, m)))
+
+    def correct(self, form, U, F, W, Gold=None):
+        u, f, w = U.numpy(), F.numpy(), W.numpy()
+        if form == 0:  # standard
+            g = Gold.numpy()
+            nv = w + (f - g)
+            g[...] = w
+        else:
+            nv = f + w
+        d = nv - u
+        u[...] = nv
+        if form != 0:
+            w[...] = d
+        return float((d * d).sum()), float((nv * nv).sum())
+
+
+def _worker(rank, world, port, form, q):
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    sys.path.insert(0, str(root / "oracle"))
+    sys.path.insert(0, str(root / "parareal-cc-cfv-split-gpu_b200"))
+    sys.path.insert(0, str(root / "tests"))
+    import oracle as O
+    from ccfv.dist import parareal_dist
+    from conftest import periodic_field
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    try:
+        g = O.grid(N, bc=1, vel=2, vp=VP, K=1e-3, scheme=1)
+        C0 = torch.from_numpy(periodic_field(N, 4))
+        out, st = parareal_dist(OracleSlices(O, g), C0, t0=0.0, t1=T, nt_fine=NT, n_slices=S,
+                                coarse_ratio=RATIO, tol=0.0, kmax=KMAX, form=form)
+        q.put((rank, out.numpy().copy(), st))
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+@pytest.mark.parametrize("form", [1, 0], ids=["delta", "standard"])
+def test_distributed_parareal_matches_single_process(oracle, form):
+    from conftest import periodic_field
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, form, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=240) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    g = oracle.grid(N, bc=1, vel=2, vp=VP, K=1e-3, scheme=1)
+    ref, it, upd = oracle.parareal(g, periodic_field(N, 4), t0=0.0, t1=T, nt_fine=NT,
+                                   n_slices=S, coarse_steps=(NT // S) // RATIO, tol=0.0,
+                                   kmax=KMAX, form=form)
+    res.sort(key=lambda x: x[0])
+    for rank, out, st in res:
+        assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 1e-13
+        assert st["iterations"] == KMAX
+        np.testing.assert_allclose(st["update"], upd, rtol=1e-9)
+    assert res[0][2]["slices"] == (0, 3) and res[1][2]["slices"] == (3, 6)

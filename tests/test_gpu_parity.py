@@ -150,3 +150,32 @@ def test_host_memory_run_matches_device(ccfv):
     c = dev(C0)
     s.run(c, 0.0, 0.002, 5)
     assert np.array_equal(out_h, host(c))
+
+
+@pytest.mark.parametrize("K", [1e-4, 1e-2, 0.5, 5.0])
+@pytest.mark.parametrize("nx", [64, 300, 1024])
+def test_periodic_solver_variants_match_oracle(oracle, ccfv, K, nx):
+    """Weak diffusion takes the filter kernel (recurrences warmed up over
+    J cells, |mu|^J below rounding), strong diffusion the exact chunked-scan
+    kernel; both agree with the oracle's Sherman-Morrison cyclic solve."""
+    vp = (0.9, -1.7)
+    dt = 0.8 / nx / 1.7
+    C0 = periodic_field(nx, 21)
+    g = oracle.grid(nx, bc=1, vel=1, vp=vp, K=K, threads=THREADS, scheme=1)
+    ref = oracle.run(g, C0, 0.0, dt, 2)
+    s = ccfv.Solver(ccfv.make_grid(nx, bc=1, velocity=1, vel_params=vp, K=K, scheme=1))
+    c = dev(C0)
+    s.run(c, 0.0, dt, 2)
+    s.check()
+    assert rel_l2(host(c), ref) < TOL
+
+
+def test_fp32_filter_coarse_close_to_fp64(ccfv):
+    N = 256
+    C0 = periodic_field(N, 12)
+    s = ccfv.Solver(ccfv.make_grid(N, bc=1, velocity=2, vel_params=(2 * np.pi, 0.5, 0.5),
+                                   K=1e-3, scheme=1))
+    a, b = dev(C0), dev(C0)
+    s.coarse(a, 0.0, 0.02, 2, ccfv.FP64)
+    s.coarse(b, 0.0, 0.02, 2, ccfv.FP32)
+    assert rel_l2(host(b), host(a)) < 2e-6
