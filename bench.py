@@ -54,10 +54,13 @@ def parse():
     ap.add_argument("--form", default="delta", choices=["standard", "delta"])
     ap.add_argument("--cpu-sample-s", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve"],
+    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "step"],
                     help="plain: one instance (default workload); batch: a mixed batch of "
                          "instances in shared launches; serve: Poisson arrivals through the "
-                         "continuous-batching server")
+                         "continuous-batching server; step: serial fine time-stepping of the "
+                         "workload's field (the sweep kernels alone)")
+    ap.add_argument("--inner", type=int, default=16,
+                    help="step mode: fine steps per timed step")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--seed", type=int, default=20261206)
@@ -196,16 +199,20 @@ def measured_peak():
 
 
 def ncu_traffic(N):
-    """Per-launch DRAM traffic of the fine sweep from a committed ncu summary
-    (profiles/sweep_traffic.json), scaled to this workload's cells."""
-    p = ROOT / "profiles" / "sweep_traffic.json"
+    """DRAM bytes per cell per sweep of the fine sweep kernel, read from the
+    committed ncu summary (the `| bytes_per_cell_sweep | X |` row of
+    profiles/sweep_filter_4096_fp64.md); scaled by the caller to a launch."""
+    p = ROOT / "profiles" / "sweep_filter_4096_fp64.md"
     if not p.exists():
         return None
-    try:
-        d = json.loads(p.read_text())
-        return float(d["bytes_per_cell_sweep"])
-    except Exception:
-        return None
+    for line in p.read_text().splitlines():
+        f = [x.strip() for x in line.strip().strip("|").split("|")]
+        if len(f) == 2 and f[0] == "bytes_per_cell_sweep":
+            try:
+                return float(f[1])
+            except ValueError:
+                return None
+    return None
 
 
 def cpu_baseline(w, sample_s):
@@ -371,7 +378,7 @@ def run_ours(a, w, ws, rank, local):
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None,
             "traffic": (tpc * f_cells / f_launch) if (tpc and f_launch) else None,
-            "kernel": "sweep_kernel<double> (fused x/y sweep, F phase)",
+            "kernel": "F phase: " + solver.variant_names(w["T"] / nt),
             "bytes_per_launch": f_cells * BYTES_PER_FINE_CELL_SWEEP / max(f_launch, 1),
             "avg_launch_us": f_ms * 1e3 / max(f_launch, 1), "peak_source": peak_kind}
 
@@ -601,6 +608,79 @@ def run_serve(a, ws, rank, local):
             served_vs_plain=(value / plain) if plain else None)))
 
 
+def run_step(a, w, ws, rank, local):
+    """Serial fine time-stepping of the workload's field: the fused sweep
+    kernels alone (three launches per fine step), no Parareal around them."""
+    import torch
+    import ccfv
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    N, nt = w["N"], w["nt"]
+    dt = w["T"] / nt
+    grid = ccfv.make_grid(N, bc=ccfv.BC_PERIODIC, velocity=ccfv.VEL_ROTATION,
+                          vel_params=(w["omega"], *w["center"]), K=w["nu"],
+                          scheme=ccfv.SCHEME_CONSISTENT)
+    solver = ccfv.Solver(grid, local)
+    C = initial_field(w, solver, dev)
+    n = a.inner
+    stream = torch.cuda.current_stream()
+    for i in range(a.warmup):
+        solver.run(C, i * n * dt, dt, n)
+    solver.check()
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = ccfv.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for i in range(a.steps):
+        solver.run(C, i * n * dt, dt, n)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = ccfv.kernel_launches() - l0
+    ck = clocks.stop()
+    solver.check()
+    ms = reduce_max(ev0.elapsed_time(ev1), ws)
+    cells = N * N * n * a.steps
+    value = ws * cells / (ms * 1e-3)
+    # e2e: host field in, host field out, through the C ABI, every step
+    h = torch.empty(N, N, dtype=torch.float64, pin_memory=True)
+    h.copy_(C.cpu())
+    hn = h.numpy()
+    solver.run(hn, 0.0, dt, n)
+    barrier(ws)
+    e0 = time.perf_counter()
+    for i in range(a.steps):
+        hn = solver.run(hn, i * n * dt, dt, n)
+    e_s = reduce_max(time.perf_counter() - e0, ws)
+    peak, peak_kind = measured_peak()
+    sweeps = 3 * n * a.steps
+    achieved = N * N * sweeps * BYTES_PER_FINE_CELL_SWEEP / (ms * 1e-3) / 1e9
+    tpc = ncu_traffic(N)
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(w, a.cpu_sample_s)
+    if rank == 0:
+        print(json.dumps(dict(
+            metric="fine_cell_updates_per_s", value=value, unit="cell-updates/s", mode="step",
+            n_gpus=ws, steps=a.steps, warmup=a.warmup, ms_per_step=ms / a.steps,
+            higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
+            data="synthetic",
+            config={"workload": f"serial fine split steps of the periodic {N}^2 rotation "
+                                f"field, nu={w['nu']}, dt=T/{nt}, {n} steps per timed step",
+                    "l2_flush": f"field {N * N * 8 / 1e6:.0f} MB per sweep (read + write "
+                                "stream; L2 not flushed)"},
+            e2e={"value": ws * cells / e_s, "unit": "cell-updates/s",
+                 "h2d_bytes_per_step": 8 * N * N, "d2h_bytes_per_step": 8 * N * N},
+            roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                      "frac": achieved / peak, "traffic": tpc * N * N if tpc else None,
+                      "kernel": solver.variant_names(dt),
+                      "bytes_per_launch": 16 * N * N, "avg_launch_us": ms * 1e3 / sweeps,
+                      "peak_source": peak_kind},
+            cpu_baseline=cpu, clocks=ck, gpu_launches=launches)))
+
+
 def main():
     a = parse()
     w = workload(a)
@@ -612,6 +692,8 @@ def main():
             run_batch(a, ws, rank, local)
         elif a.mode == "serve":
             run_serve(a, ws, rank, local)
+        elif a.mode == "step":
+            run_step(a, w, ws, rank, local)
         else:
             run_ours(a, w, ws, rank, local)
     finally:

@@ -287,6 +287,17 @@ int ccfv_step_noalloc(const ccfv_grid *grid, double *d_C, double tn, double dt, 
  * lengths (process-wide).  *segment (optional) receives the choice. */
 int ccfv_autotune(ccfv_ctx *ctx, double dt, int precision, int *segment, void *stream);
 
+/* Which sweep kernel each sub-step of a step of dt runs (introspection; no
+ * counterpart in the reference): variant[s] for s = x(dt/2), y(dt), x(dt/2)
+ * is CCFV_SWEEP_GENERAL (per-cell feet), CCFV_SWEEP_UNIFORM (shared-foot
+ * stencil with exact chunked scans), CCFV_SWEEP_FILTER (shared-foot stencil
+ * with the factored cyclic solve) or CCFV_SWEEP_SOURCE (per-cell, with the
+ * source term); segment[s] = cells per CTA along a line (either may be NULL).
+ * No device work. */
+enum { CCFV_SWEEP_GENERAL = 0, CCFV_SWEEP_UNIFORM = 1, CCFV_SWEEP_FILTER = 2,
+       CCFV_SWEEP_SOURCE = 3 };
+int ccfv_sweep_plan(ccfv_ctx *ctx, double dt, int precision, int variant[3], int segment[3]);
+
 /* ---- library info ---------------------------------------------------- */
 /* Number of kernels this library launched since load (all contexts). */
 uint64_t ccfv_kernel_launches(void);

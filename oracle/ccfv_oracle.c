@@ -60,6 +60,35 @@ static double vel_v(const or_grid *g, double x, double y, double t) {
 static int nthreads(const or_grid *g) { return g->threads > 0 ? g->threads : 1; }
 
 /* ---------------------------------------------------------------------- */
+/* Source term.  The reference's f is identically zero (T2S4_Parareal.cu:
+ * 58-61) but its step keeps the full source path; GAUSSIAN exercises it. */
+
+static double src_f(const or_grid *g, double x, double y, double t) {
+  if (g->src != OR_SRC_GAUSSIAN) return 0.0;
+  const double dx = x - g->sp[1], dy = y - g->sp[2];
+  return g->sp[0] * exp(-(dx * dx + dy * dy) / g->sp[3]) * cos(g->sp[4] * t);
+}
+
+/* 3x3 Simpson cell averages of f at time t (get_source_term_on_gpu,
+ * T2S4_Parareal.cu:142-165). */
+static void source_cells(const or_grid *g, double t, double *out) {
+  const int nx = g->nx, ny = g->ny;
+  const double dx = (g->x_max - g->x_min) / nx, dy = (g->y_max - g->y_min) / ny;
+  for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++) {
+      const double x_i = g->x_min + (i + 0.5) * dx, y_j = g->y_min + (j + 0.5) * dy;
+      const double xm = x_i - 0.5 * dx, xp = x_i + 0.5 * dx;
+      const double ym = y_j - 0.5 * dy, yp = y_j + 0.5 * dy;
+      out[(size_t)i * ny + j] =
+          1.0 / 36.0 *
+          (src_f(g, xm, ym, t) + src_f(g, xp, ym, t) + src_f(g, xm, yp, t) + src_f(g, xp, yp, t) +
+           4.0 * (src_f(g, xm, y_j, t) + src_f(g, xp, y_j, t) + src_f(g, x_i, ym, t) +
+                  src_f(g, x_i, yp, t)) +
+           16.0 * src_f(g, x_i, y_j, t));
+    }
+}
+
+/* ---------------------------------------------------------------------- */
 /* Characteristic feet.
  * Corner feet by one Heun step backwards over Dt (get_Lagrange_points_on_gpu,
  * T2S4_Parareal.cu:203-229): x* = x - Dt u(x,tb); xbar = x - Dt/2 (u(x,tb) +
@@ -118,6 +147,7 @@ typedef struct line_par {
   int bc;
   double eps_remap; /* x: 1e-15 (T2S4:323-324), y: 1e-16 (T2S4:414-415) */
   int deriv_of_remap; /* derivative taken of the remapped field (3rd sweep) */
+  double src_w;       /* RHS weight of (remapped f(t_a) + f(t_b))           */
 } line_par;
 
 /* PPM antiderivative in cell units (d_intC_ppm4th, T2S4_Parareal.cu:63-65). */
@@ -309,7 +339,8 @@ static void thomas(int L, double coA, const double *coB, double coC, const doubl
 
 /* Full line: remap + foot derivative + RHS + compact mass matrix + solve. */
 static void sweep_line(const line_par *p, const double *c, const double *foot,
-                       const double *nextc0, double *out, double *wk) {
+                       const double *nextc0, const double *s0, const double *s1,
+                       const double *nexts0, double *out, double *wk) {
   const int L = p->L;
   double *CL = wk, *DltC = wk + L, *C6 = wk + 2 * L, *IntC = wk + 3 * L;
   double *D = wk + 4 * L;          /* L+1 */
@@ -321,12 +352,21 @@ static void sweep_line(const line_par *p, const double *c, const double *foot,
    * remapped field: dcdx_bar_on_gpu(v_d_Cnphf_bar_x, ...) (T2S4:929-932),
    * the first two on the sweep input (T2S4:834-837, 882-885). */
   foot_derivative(p, p->deriv_of_remap ? IntC : c, foot, D);
-  /* RHS (x_b_RHS_on_gpu T2S4:564-580 / y_b_RHS_on_gpu T2S4:596-613); the
-   * source f is identically zero (T2S4:59-61), so its terms add 0.0. */
-  const double f0 = 0.0, f1 = 0.0;
+  /* RHS (x_b_RHS_on_gpu T2S4:564-580 / y_b_RHS_on_gpu T2S4:596-613):
+   * b = remap(C) + w (remap(f(t_a)) + f(t_b)) + 0.5 K Dt/h (D_{k+1} - D_k);
+   * f(t_a) is remapped by the same PPM integral as C (T2S4:846-853,
+   * 893-900, 944-951).  The reference's w is 0.25 dt for the x half-steps
+   * and 0.5 dt for the y step, i.e. 0.5 Dt of the sub-step. */
   const double rinv = p->Dt / p->h;
-  for (int k = 0; k < L; k++)
-    b[k] = IntC[k] + 0.5 * p->Dt * (f0 + f1) + 0.5 * p->K * rinv * (D[k + 1] - D[k]);
+  double *F0b = u; /* remapped f(t_a); u is free until the cyclic solve */
+  if (s0) {
+    ppm_coefs(p, s0, CL, DltC, C6);
+    remap(p, s0, foot, CL, DltC, C6, nexts0, F0b);
+  }
+  for (int k = 0; k < L; k++) {
+    const double fs = s0 ? p->src_w * (F0b[k] + s1[k]) : 0.0;
+    b[k] = IntC[k] + fs + 0.5 * p->K * rinv * (D[k + 1] - D[k]);
+  }
   /* compact mass matrix (x_b_rhs_compact_on_gpu T2S4:616-634) */
   if (p->bc == OR_BC_COMPAT) {
     for (int k = 0; k < L; k++) {
@@ -362,14 +402,19 @@ static void sweep_line(const line_par *p, const double *c, const double *foot,
 }
 
 /* Sweep along x (lines j, cells i, stride ny) or y (lines i, contiguous). */
+/* S0, S1: cell averages of f at the sub-step's start (remapped) and end;
+ * NULL when there is no source. */
 static void sweep(const or_grid *g, int dir, const double *in, double *outp, const double *feet,
-                  double Dt, int deriv_of_remap) {
+                  double Dt, int deriv_of_remap, const double *S0, const double *S1) {
   const int nx = g->nx, ny = g->ny;
   line_par p;
   p.K = g->K;
   p.Dt = Dt;
   p.bc = g->bc;
   p.deriv_of_remap = deriv_of_remap;
+  /* the reference's 0.5 Dt adds the source twice over a full split step
+   * (x/2 + y + x/2); the consistent scheme weighs it 0.25 Dt */
+  p.src_w = g->scheme == OR_SCHEME_REFERENCE ? 0.5 * Dt : 0.25 * Dt;
   if (dir == 0) {
     p.L = nx; p.s_min = g->x_min; p.s_max = g->x_max; p.h = (g->x_max - g->x_min) / nx;
     p.eps_remap = 1e-15;
@@ -386,31 +431,46 @@ static void sweep(const or_grid *g, int dir, const double *in, double *outp, con
     double *c = (double *)malloc(sizeof(double) * (size_t)L);
     double *o = (double *)malloc(sizeof(double) * (size_t)L);
     double *f = (double *)malloc(sizeof(double) * (size_t)(L + 1));
+    double *l0 = (double *)malloc(sizeof(double) * (size_t)L);
+    double *l1 = (double *)malloc(sizeof(double) * (size_t)L);
 #ifdef _OPENMP
 #pragma omp for schedule(static)
 #endif
     for (int line = 0; line < M; line++) {
-      double nc[3];
-      const double *nextc0 = NULL;
+      double nc[3], ns[3];
+      const double *nextc0 = NULL, *nexts0 = NULL;
       if (dir == 0) {
         for (int i = 0; i < L; i++) c[i] = in[(size_t)i * ny + line];
         for (int e = 0; e <= L; e++) f[e] = feet[(size_t)e * ny + line];
+        if (S0)
+          for (int i = 0; i < L; i++) {
+            l0[i] = S0[(size_t)i * ny + line];
+            l1[i] = S1[(size_t)i * ny + line];
+          }
       } else {
         memcpy(c, in + (size_t)line * ny, sizeof(double) * L);
         memcpy(f, feet + (size_t)line * (ny + 1), sizeof(double) * (L + 1));
+        if (S0) {
+          memcpy(l0, S0 + (size_t)line * ny, sizeof(double) * L);
+          memcpy(l1, S1 + (size_t)line * ny, sizeof(double) * L);
+        }
         if (g->bc == OR_BC_COMPAT && g->quirks && line + 1 < nx) {
           cell0_coefs_compat(in + (size_t)(line + 1) * ny, L, &nc[0], &nc[1], &nc[2]);
           nextc0 = nc;
+          if (S0) {
+            cell0_coefs_compat(S0 + (size_t)(line + 1) * ny, L, &ns[0], &ns[1], &ns[2]);
+            nexts0 = ns;
+          }
         }
       }
-      sweep_line(&p, c, f, nextc0, o, wk);
+      sweep_line(&p, c, f, nextc0, S0 ? l0 : NULL, S0 ? l1 : NULL, nexts0, o, wk);
       if (dir == 0) {
         for (int i = 0; i < L; i++) outp[(size_t)i * ny + line] = o[i];
       } else {
         memcpy(outp + (size_t)line * ny, o, sizeof(double) * L);
       }
     }
-    free(wk); free(c); free(o); free(f);
+    free(wk); free(c); free(o); free(f); free(l0); free(l1);
   }
 }
 
@@ -430,10 +490,23 @@ int or_step(const or_grid *g, double *C, double tn, double dt) {
   feet_x(g, 0.5 * dt, tn, tnphf, fx1);
   feet_y(g, dt, tn, tnp1, fy2);
   feet_x(g, 0.5 * dt, tnphf, tnp1, fx3);
-  sweep(g, 0, C, t1, fx1, 0.5 * dt, 0);
-  sweep(g, 1, t1, t2, fy2, dt, 0);
-  sweep(g, 0, t2, C, fx3, 0.5 * dt, g->scheme == OR_SCHEME_REFERENCE);
+  double *fa = NULL, *fh = NULL, *fe = NULL;
+  if (g->src != OR_SRC_NONE) {
+    /* f(t_n) remapped + f(t_n+1/2) in the first sweep (T2S4:839-853),
+     * f(t_n) remapped + f(t_n+1) in the second (T2S4:887-900), f(t_n+1)
+     * remapped + f(t_n+1) in the third (T2S4:934-951) */
+    fa = (double *)malloc(sizeof(double) * NN);
+    fh = (double *)malloc(sizeof(double) * NN);
+    fe = (double *)malloc(sizeof(double) * NN);
+    source_cells(g, tn, fa);
+    source_cells(g, tnphf, fh);
+    source_cells(g, tnp1, fe);
+  }
+  sweep(g, 0, C, t1, fx1, 0.5 * dt, 0, fa, fh);
+  sweep(g, 1, t1, t2, fy2, dt, 0, fa, fe);
+  sweep(g, 0, t2, C, fx3, 0.5 * dt, g->scheme == OR_SCHEME_REFERENCE, fe, fe);
   free(fx1); free(fy2); free(fx3); free(t1); free(t2);
+  free(fa); free(fh); free(fe);
   return 0;
 }
 
@@ -565,8 +638,12 @@ int or_parareal(const or_grid *g, const or_parareal_opts *o, const double *C0, d
         }
         memcpy(Go, w, sizeof(double) * NN);
       } else {
-        memcpy(w, e, sizeof(double) * NN); /* e = U+[n] - U[n] */
-        or_coarse(g, w, tn, DT, m);
+        /* e = U+[n] - U[n] goes through the linear part of G (without the
+         * source term), so G(0) = 0 */
+        or_grid gh = *g;
+        gh.src = OR_SRC_NONE;
+        memcpy(w, e, sizeof(double) * NN);
+        or_coarse(&gh, w, tn, DT, m);
         double *Fn = F + (n + 1) * NN;
         for (size_t i = 0; i < NN; ++i) {
           double nv = Fn[i] + w[i];

@@ -23,6 +23,9 @@ enum { OR_FORM_STANDARD = 0, OR_FORM_DELTA = 1 };
  * field, as T2S4_Parareal.cu:929-932 does; CONSISTENT: every sweep takes it
  * of its input (the first two sweeps of the reference do this). */
 enum { OR_SCHEME_REFERENCE = 0, OR_SCHEME_CONSISTENT = 1 };
+/* Source term f(x,y,t): NONE is the reference's f = 0 (T2S4_Parareal.cu:58-61);
+ * GAUSSIAN is sp0 exp(-((x-sp1)^2 + (y-sp2)^2) / sp3) cos(sp4 t). */
+enum { OR_SRC_NONE = 0, OR_SRC_GAUSSIAN = 1 };
 
 typedef struct or_grid {
   int nx, ny;
@@ -34,6 +37,8 @@ typedef struct or_grid {
   int quirks;        /* compat: reproduce the y-remap neighbour-row read    */
   int threads;       /* OpenMP threads for the line loops (<=0: 1)          */
   int scheme;        /* OR_SCHEME_REFERENCE or OR_SCHEME_CONSISTENT         */
+  int src;           /* OR_SRC_NONE or OR_SRC_GAUSSIAN                      */
+  double sp[5];      /* GAUSSIAN: (amplitude, xc, yc, width, omega)         */
 } or_grid;
 
 typedef struct or_parareal_opts {

@@ -22,6 +22,7 @@ BC_COMPAT, BC_PERIODIC = 0, 1
 VEL_REF_ROT4, VEL_CONST, VEL_ROTATION, VEL_SWIRL = 0, 1, 2, 3
 FORM_STANDARD, FORM_DELTA = 0, 1
 SCHEME_REFERENCE, SCHEME_CONSISTENT = 0, 1
+SRC_NONE, SRC_GAUSSIAN = 0, 1
 
 
 class OrGrid(C.Structure):
@@ -34,6 +35,8 @@ class OrGrid(C.Structure):
         ("K", C.c_double),
         ("quirks", C.c_int), ("threads", C.c_int),
         ("scheme", C.c_int),
+        ("src", C.c_int),
+        ("sp", C.c_double * 5),
     ]
 
 
@@ -82,7 +85,8 @@ def lib():
 
 
 def grid(nx, ny=None, *, bc=BC_COMPAT, vel=VEL_REF_ROT4, vp=(0, 0, 0, 0), K=0.0,
-         domain=None, quirks=1, threads=1, scheme=SCHEME_REFERENCE) -> OrGrid:
+         domain=None, quirks=1, threads=1, scheme=SCHEME_REFERENCE, src=SRC_NONE,
+         sp=(0, 0, 0, 1, 0)) -> OrGrid:
     ny = nx if ny is None else ny
     if domain is None:
         domain = (-1.0, 1.0, -1.0, 1.0) if bc == BC_COMPAT else (0.0, 1.0, 0.0, 1.0)
@@ -95,6 +99,9 @@ def grid(nx, ny=None, *, bc=BC_COMPAT, vel=VEL_REF_ROT4, vp=(0, 0, 0, 0), K=0.0,
     g.K = K
     g.quirks, g.threads = quirks, threads
     g.scheme = scheme
+    g.src = src
+    for i in range(5):
+        g.sp[i] = float(sp[i]) if i < len(sp) else 0.0
     return g
 
 

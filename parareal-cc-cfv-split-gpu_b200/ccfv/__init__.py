@@ -133,6 +133,8 @@ _SIGS = {
                                C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                C.c_void_p]),
     "ccfv_autotune": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_int), C.c_void_p]),
+    "ccfv_sweep_plan": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_int),
+                                  C.POINTER(C.c_int)]),
     "ccfv_step_noalloc": (C.c_int, [C.POINTER(Grid), C.c_void_p, C.c_double, C.c_double,
                                     C.c_void_p]),
 }
@@ -269,6 +271,22 @@ class Solver:
         self._chk(lib().ccfv_autotune(self._h, dt, int(precision), C.byref(seg),
                                       _stream_ptr(stream)))
         return seg.value
+
+    SWEEP_NAMES = ("general", "uniform", "filter", "source")
+
+    def sweep_plan(self, dt, precision=FP64):
+        """Kernel variant and segment length of the three sub-steps of a step
+        of dt: [(variant name, cells per CTA)] * 3."""
+        v, sg = (C.c_int * 3)(), (C.c_int * 3)()
+        self._chk(lib().ccfv_sweep_plan(self._h, dt, int(precision), v, sg))
+        return [(self.SWEEP_NAMES[v[i]], sg[i]) for i in range(3)]
+
+    SWEEP_KERNELS = {"general": "sweep_kernel", "uniform": "sweep_fast_kernel",
+                     "filter": "sweep_filter_kernel", "source": "sweep_kernel"}
+
+    def variant_names(self, dt, precision=FP64):
+        """Names of the sweep kernels a step of dt launches (x, y, x)."""
+        return "/".join(self.SWEEP_KERNELS[n] for n, _ in self.sweep_plan(dt, precision))
 
     # -- fields and diagnostics --------------------------------------------
     def exact_ref(self, C_dev, t, stream=None):

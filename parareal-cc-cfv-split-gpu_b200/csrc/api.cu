@@ -218,6 +218,20 @@ int ccfv_autotune(ccfv_ctx *ctx, double dt, int precision, int *segment, void *s
   return rc ? rc : autotune(ctx, dt, precision == CCFV_FP64, (cudaStream_t)stream, segment);
 }
 
+int ccfv_sweep_plan(ccfv_ctx *ctx, double dt, int precision, int variant[3], int segment[3]) {
+  if (!ctx || !(dt > 0.0) || (precision != CCFV_FP64 && precision != CCFV_FP32))
+    return CCFV_ERR_INVALID;
+  for (int kind = 0; kind < 3; ++kind) {
+    const int dir = kind == 1 ? 1 : 0;
+    const double Dt = kind == 1 ? dt : 0.5 * dt;
+    const int dsrc = (kind == 2 && ctx->grid.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
+    const LaunchGeom G = step_geom(ctx->grid, dir, Dt, dsrc, precision == CCFV_FP64);
+    if (variant) variant[kind] = ctx->force_general ? SWEEP_GENERAL : G.variant;
+    if (segment) segment[kind] = G.lc_max;
+  }
+  return CCFV_OK;
+}
+
 uint64_t ccfv_kernel_launches(void) { return launches(); }
 
 const char *ccfv_last_error(ccfv_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }

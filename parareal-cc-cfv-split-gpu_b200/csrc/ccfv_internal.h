@@ -53,6 +53,9 @@ struct SweepField {
   int jmax;              // the field takes part while jstep < jmax (0: always)
   int smax;              // slice-indexed fields: while slice < smax
   int gskip;             // slice-indexed fields: skip slice == nlo (zero increment)
+  int phase;             // slice-indexed fields: 0 every launch, 1 only while the
+                         // instance's nlo < 0 (first coarse sweep), 2 only while
+                         // nlo >= 0 (Parareal iterations)
   double t_step;         // added per launch step: time = ... + jstep * t_step
   double t_slice;        // added per launch slice: time = ... + slice * t_slice
   double vp[4];          // velocity parameters

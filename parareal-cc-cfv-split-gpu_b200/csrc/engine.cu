@@ -579,6 +579,13 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
     ctx->fine_plan_slices = S;
   }
   int status = CCFV_OK;
+  // The first coarse sweep moves whole states and always runs in FP64: FP32
+  // rounding there would seed every wavenumber at ~1e-7 |U|, and Parareal
+  // amplifies the high-wavenumber error modes of advection (and of
+  // Crank-Nicolson coarse steps with K Dt/h^2 >> 1) from one iteration to the
+  // next.  In the iterations FP32 rounding is relative to the increments.
+  StepPlan *iplan = single_plan(ctx, dtc, true, &status);
+  if (!iplan) return status;
   StepPlan *cplan = single_plan(ctx, dtc, g64, &status);
   if (!cplan) return status;
 
@@ -597,16 +604,15 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
     return CCFV_OK;
   };
 
-  // k = 0: coarse sweep U[n+1] = G(U[n])  (T2S4:1271-1280)
+  // k = 0: coarse sweep U[n+1] = G(U[n])  (T2S4:1271-1280), in place on U[n+1]
   for (int n = 0; n < S; ++n) {
-    int rc;
-    if (g64) CK(cudaMemcpyAsync(W, U + (size_t)n * NN, fb, cudaMemcpyDeviceToDevice, st));
-    else if ((rc = convert(ctx, U + (size_t)n * NN, W, NN, st))) return rc;
-    if ((rc = coarse_on_W(n))) return rc;
-    if (g64) CK(cudaMemcpyAsync(U + (size_t)(n + 1) * NN, W, fb, cudaMemcpyDeviceToDevice, st));
-    else if ((rc = convert(ctx, W, U + (size_t)(n + 1) * NN, NN, st))) return rc;
-    if (Gold) CK(cudaMemcpyAsync(Gold + (size_t)(n + 1) * NN, U + (size_t)(n + 1) * NN, fb,
-                                 cudaMemcpyDeviceToDevice, st));
+    double *un1 = U + (size_t)(n + 1) * NN;
+    CK(cudaMemcpyAsync(un1, U + (size_t)n * NN, fb, cudaMemcpyDeviceToDevice, st));
+    for (int i = 0; i < m; ++i) {
+      int rc = run_step_plan(ctx, *iplan, true, 0, 1, o->t0 + n * DT + i * dtc, un1, st);
+      if (rc) return rc;
+    }
+    if (Gold) CK(cudaMemcpyAsync(Gold + (size_t)(n + 1) * NN, un1, fb, cudaMemcpyDeviceToDevice, st));
   }
 
   std::vector<double> hn(2 * (size_t)(S + 1));

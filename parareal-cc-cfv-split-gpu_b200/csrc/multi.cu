@@ -72,14 +72,16 @@ __global__ void __launch_bounds__(BT)
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long first = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double se = 0.0, su = 0.0;
-  if (op == OP_LOAD_W) {
+  if (op == OP_LOAD_W) {  // FP64 W: the first coarse sweep, standard-form G
     const double *src = b.U + (long long)n * b.NN;
-    for (long long i = first; i < cnt; i += stride) wstore(b, i, src[i]);
+    double *w = reinterpret_cast<double *>(b.W);
+    for (long long i = first; i < cnt; i += stride) w[i] = src[i];
   } else if (op == OP_STORE_W) {
     double *dst = b.U + (long long)(n + 1) * b.NN;
     double *gd = b.Gold ? b.Gold + (long long)(n + 1) * b.NN : nullptr;
+    const double *w = reinterpret_cast<const double *>(b.W);
     for (long long i = first; i < cnt; i += stride) {
-      const double v = wload(b, i);
+      const double v = w[i];
       dst[i] = v;
       if (gd) gd[i] = v;
     }
@@ -167,8 +169,8 @@ size_t problem_bytes(const ccfv_grid &g, const ccfv_parareal_opts &o) {
   const size_t fb = sizeof(double) * (size_t)g.nx * g.ny;
   const size_t S = (size_t)std::max(o.n_slices, 1);
   const bool g64 = o.coarse_precision != CCFV_FP32;
-  return fb * (S + 1) * 2 + (o.form == CCFV_FORM_STANDARD ? fb * (S + 1) : 0) +
-         (g64 ? fb : fb / 2) + 4 * 256;
+  (void)g64;  // W holds FP64 states in the first coarse sweep whatever the coarse precision
+  return fb * (S + 1) * 2 + (o.form == CCFV_FORM_STANDARD ? fb * (S + 1) : 0) + fb + 4 * 256;
 }
 
 int problem_setup(Problem &P, const ccfv_problem &p, std::string *err) {
@@ -229,10 +231,10 @@ int MultiEngine::add(const ccfv_problem &pr, int *slot) {
   P->ctx = std::make_unique<ccfv_ctx>();
   P->ctx->grid = P->g;
   P->ctx->device = device_;
-  for (int t = 0; t < 4; ++t) {
+  for (int t = 0; t < 6; ++t) {
     const int dir = t & 1;
     const double Dt = (t < 2 ? P->dt : P->dtc) * (dir == 0 ? 0.5 : 1.0);
-    P->tab[t] = get_table(P->ctx.get(), dir, Dt, t < 2 ? true : P->g64, &rc);
+    P->tab[t] = get_table(P->ctx.get(), dir, Dt, (t < 2 || t >= 4) ? true : P->g64, &rc);
     if (!P->tab[t]) return fail(rc, P->ctx->last_error);
   }
   for (int kind = 0; kind < 3; ++kind)
@@ -257,7 +259,7 @@ int MultiEngine::add(const ccfv_problem &pr, int *slot) {
   P->U = reinterpret_cast<double *>(take(fb * (P->S + 1)));
   P->F = reinterpret_cast<double *>(take(fb * (P->S + 1)));
   P->Gold = P->o.form == CCFV_FORM_STANDARD ? reinterpret_cast<double *>(take(fb * (P->S + 1))) : nullptr;
-  P->W = take(P->g64 ? fb : fb / 2);
+  P->W = take(fb);
   MCK(cudaMemcpyAsync(P->U, P->C0, fb,
                       P->o.mem == CCFV_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st_));
   int s = -1;
@@ -334,15 +336,26 @@ int MultiEngine::rebuild() {
       {  // coarse: the work field W, slice from the launch (t0 + n DT + i dtc)
         const double Dt = kind == 1 ? P->dtc : 0.5 * P->dtc;
         const double ta = kind == 2 ? 0.5 * P->dtc : 0.0, tb = kind == 0 ? 0.5 * P->dtc : P->dtc;
-        SweepField f = make_field(g, dir, Dt, ta + P->o.t0, tb + P->o.t0, P->W, P->tab[2 + dir], dsrc);
-        f.inst = i;
-        f.slice = -1;
-        f.jmax = P->m;
-        f.smax = P->S;
-        f.gskip = P->o.form == CCFV_FORM_DELTA ? 1 : 0;
-        f.t_step = P->dtc;
-        f.t_slice = P->DT;
-        add_field(coarse_, kind, g, f, P->g64);
+        auto coarse_field = [&](const ccfv_grid &gg, const SolverTable *tab, int phase) {
+          SweepField f = make_field(gg, dir, Dt, ta + P->o.t0, tb + P->o.t0, P->W, tab, dsrc);
+          f.inst = i;
+          f.slice = -1;
+          f.jmax = P->m;
+          f.smax = P->S;
+          f.gskip = P->o.form == CCFV_FORM_DELTA ? 1 : 0;
+          f.t_step = P->dtc;
+          f.t_slice = P->DT;
+          f.phase = phase;
+          return f;
+        };
+        if (P->g64) {
+          add_field(coarse_, kind, g, coarse_field(g, P->tab[2 + dir], 0), true);
+        } else {
+          // the first sweep moves states in FP64; the iterations move
+          // increments in FP32
+          add_field(coarse_, kind, g, coarse_field(g, P->tab[4 + dir], 1), true);
+          add_field(coarse_, kind, g, coarse_field(g, P->tab[2 + dir], 2), false);
+        }
       }
     }
   }

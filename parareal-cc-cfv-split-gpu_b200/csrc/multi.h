@@ -28,7 +28,9 @@ struct Problem {
   double *U = nullptr, *F = nullptr, *Gold = nullptr;
   void *W = nullptr;
   std::unique_ptr<ccfv_ctx> ctx;  // owns the solver tables of this grid
-  const SolverTable *tab[4] = {};  // fine x, fine y, coarse x, coarse y
+  // fine x, fine y, coarse x, coarse y (coarse precision), coarse x, y in
+  // FP64 (the first coarse sweep, which always runs in FP64)
+  const SolverTable *tab[6] = {};
   enum { NEW, RUNNING, DONE } state = NEW;
   int k = 0;                 // iterations done
   int converged = 0;

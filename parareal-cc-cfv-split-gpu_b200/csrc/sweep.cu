@@ -85,6 +85,7 @@ __device__ __forceinline__ bool field_active(const SweepField &f, int jstep, int
   if (!nlo) return true;
   const int lo = nlo[f.inst];
   if (f.slice >= 0) return f.slice >= lo;
+  if ((f.phase == 1 && lo >= 0) || (f.phase == 2 && lo < 0)) return false;
   return nslice < f.smax && nslice >= lo + f.gskip;
 }
 __device__ __forceinline__ double field_time(const SweepField &f, double toff, int jstep,

@@ -75,3 +75,66 @@ def test_parareal_forms_converge_to_serial_fine(oracle):
     UT, iters, upd = oracle.parareal(g, C0, t0=0.0, t1=T, nt_fine=nt, n_slices=S,
                                      coarse_steps=1, tol=0.0, kmax=S, form=oracle.FORM_DELTA)
     assert rel_l2(UT, fine) < 1e-13
+
+
+def _simpson_cells(nx, dom, sp):
+    """3x3 Simpson cell averages of f = a exp(-r^2/den) (no time factor)."""
+    x0, x1, y0, y1 = dom
+    dx, dy = (x1 - x0) / nx, (y1 - y0) / nx
+    xc = x0 + (np.arange(nx) + 0.5) * dx
+    yc = y0 + (np.arange(nx) + 0.5) * dy
+    w = np.array([1.0, 4.0, 1.0]) / 6.0
+    out = np.zeros((nx, nx))
+    for a, ox in zip(w, (-0.5, 0.0, 0.5)):
+        for b, oy in zip(w, (-0.5, 0.0, 0.5)):
+            X = (xc + ox * dx)[:, None]
+            Y = (yc + oy * dy)[None, :]
+            out += a * b * sp[0] * np.exp(-((X - sp[1]) ** 2 + (Y - sp[2]) ** 2) / sp[3])
+    return out
+
+
+@pytest.mark.parametrize("scheme,factor", [(1, 1.0), (0, 2.0)], ids=["consistent", "reference"])
+def test_source_without_transport(oracle, scheme, factor):
+    """V = 0, K = 0: every sweep is the identity plus its source quadrature, so
+    C(T) = C0 + T f_h for the consistent scheme.  The reference's RHS weighs
+    the source 0.5 Dt in each of the three sub-steps (x_b_RHS_on_gpu,
+    y_b_RHS_on_gpu, T2S4_Parareal.cu:564-613), which doubles it:
+    C(T) = C0 + 2 T f_h."""
+    N, T, n = 24, 0.3, 6
+    sp = (1.5, 0.4, 0.6, 0.02, 0.0)
+    g = oracle.grid(N, bc=1, vel=1, vp=(0.0, 0.0), K=0.0, scheme=scheme, src=1, sp=sp)
+    C0 = periodic_field(N, 5)
+    out = oracle.run(g, C0, 0.0, T / n, n)
+    want = C0 + factor * T * _simpson_cells(N, (0.0, 1.0, 0.0, 1.0), sp)
+    assert np.abs(out - want).max() < 1e-13
+
+
+@pytest.mark.parametrize("bc", [0, 1])
+def test_source_enters_linearly(oracle, bc):
+    """The step is affine in (C, f): S(C0; f) = S(C0; 0) + S(0; f)."""
+    N, dt = 20, 0.01
+    sp = (2.0, 0.1 if bc == 0 else 0.55, 0.2 if bc == 0 else 0.45, 0.05, 3.0)
+    kw = dict(K=2e-3, scheme=1)
+    if bc == 1:
+        kw.update(bc=1, vel=2, vp=(2 * np.pi, 0.5, 0.5))
+    C0 = periodic_field(N, 8) if bc == 1 else seeded_field(N, 8)
+    a = oracle.run(oracle.grid(N, src=1, sp=sp, **kw), C0, 0.1, dt, 3)
+    b = oracle.run(oracle.grid(N, **kw), C0, 0.1, dt, 3)
+    c = oracle.run(oracle.grid(N, src=1, sp=sp, **kw), np.zeros_like(C0), 0.1, dt, 3)
+    assert np.abs(a - (b + c)).max() < 1e-12 * max(1.0, np.abs(a).max())
+
+
+@pytest.mark.parametrize("form", [0, 1], ids=["standard", "delta"])
+def test_parareal_with_source_converges_to_serial_fine(oracle, form):
+    """With a source the coarse propagator is affine; the delta form moves
+    increments with its linear part, so both forms reach the serial fine
+    solve after as many iterations as slices."""
+    N, T, nt, S = 20, 0.2, 40, 5
+    sp = (3.0, 0.45, 0.55, 0.03, 6.0)
+    g = oracle.grid(N, bc=1, vel=2, vp=(2 * np.pi, 0.5, 0.5), K=1e-3, scheme=1, src=1, sp=sp)
+    C0 = periodic_field(N, 3)
+    fine = oracle.run(g, C0, 0.0, T / nt, nt)
+    UT, it, upd = oracle.parareal(g, C0, t0=0.0, t1=T, nt_fine=nt, n_slices=S,
+                                  coarse_steps=2, tol=0.0, kmax=S, form=form)
+    assert it == S
+    assert rel_l2(UT, fine) < 1e-13
