@@ -80,6 +80,16 @@ enum ccfv_form {
 
 /* Grid and physics.  Replaces the compile-time macros and GPUContext fields
  * of the reference (T2S4_Parareal.cu:27-33, 724-768). */
+/* Source term f(x, y, t) of c_t + div(V c) = K lap c + f.  The reference
+ * keeps the whole source path in its step (get_source_term_on_gpu and the
+ * remapped f in x_b_RHS_on_gpu / y_b_RHS_on_gpu, T2S4_Parareal.cu:142-165,
+ * 564-613, 839-951) with f identically zero (T2S4_Parareal.cu:58-61).
+ * GAUSSIAN: f = p0 exp(-((x-p1)^2 + (y-p2)^2) / p3) cos(p4 t), p3 > 0, as 3x3
+ * Simpson cell averages; f(t_a) is remapped like C and f(t_b) added, with
+ * weight 0.5 Dt per sub-step in the reference scheme (which therefore adds
+ * 2 dt of source per step) and 0.25 Dt in the consistent scheme. */
+enum ccfv_source { CCFV_SRC_NONE = 0, CCFV_SRC_GAUSSIAN = 1 };
+
 typedef struct ccfv_grid {
   int nx, ny;                  /* cells; the reference forces ny = nx      */
   double x_min, x_max;         /* reference: -1, 1                         */
@@ -89,6 +99,8 @@ typedef struct ccfv_grid {
   double vel_params[4];        /* see enum ccfv_velocity                   */
   double K;                    /* diffusivity (reference config key "K")   */
   int scheme;                  /* enum ccfv_scheme (0 = reference)         */
+  int source;                  /* enum ccfv_source (0 = the reference's f=0) */
+  double source_params[5];     /* GAUSSIAN: amplitude, xc, yc, width, omega */
 } ccfv_grid;
 
 typedef struct ccfv_ctx ccfv_ctx;

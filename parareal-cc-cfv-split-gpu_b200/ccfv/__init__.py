@@ -26,6 +26,7 @@ ERR_BUDGET, ERR_NOT_FOUND, ERR_CANCELLED, ERR_TIMEOUT = 6, 7, 8, 9
 BC_COMPAT, BC_PERIODIC = 0, 1
 VEL_REF_ROT4, VEL_CONST, VEL_ROTATION, VEL_SWIRL = 0, 1, 2, 3
 SCHEME_REFERENCE, SCHEME_CONSISTENT = 0, 1
+SRC_NONE, SRC_GAUSSIAN = 0, 1
 FP64, FP32 = 0, 1
 MEM_DEVICE, MEM_HOST = 0, 1
 FORM_STANDARD, FORM_DELTA = 0, 1
@@ -47,6 +48,8 @@ class Grid(C.Structure):
         ("vel_params", C.c_double * 4),
         ("K", C.c_double),
         ("scheme", C.c_int),
+        ("source", C.c_int),
+        ("source_params", C.c_double * 5),
     ]
 
 
@@ -160,7 +163,10 @@ def kernel_launches() -> int:
 
 
 def make_grid(nx, ny=None, *, bc=BC_COMPAT, velocity=VEL_REF_ROT4, vel_params=(0, 0, 0, 0),
-              K=0.0, domain=None, scheme=SCHEME_REFERENCE) -> Grid:
+              K=0.0, domain=None, scheme=SCHEME_REFERENCE, source=SRC_NONE,
+              source_params=(0, 0, 0, 1, 0)) -> Grid:
+    """Grid description (ccfv_grid).  source=SRC_GAUSSIAN adds
+    f = p0 exp(-((x-p1)^2 + (y-p2)^2) / p3) cos(p4 t), source_params = p."""
     ny = nx if ny is None else ny
     if domain is None:
         domain = (-1.0, 1.0, -1.0, 1.0) if bc == BC_COMPAT else (0.0, 1.0, 0.0, 1.0)
@@ -171,6 +177,9 @@ def make_grid(nx, ny=None, *, bc=BC_COMPAT, velocity=VEL_REF_ROT4, vel_params=(0
     for i in range(4):
         g.vel_params[i] = float(vel_params[i]) if i < len(vel_params) else 0.0
     g.K = float(K)
+    g.source = int(source)
+    for i in range(5):
+        g.source_params[i] = float(source_params[i]) if i < len(source_params) else 0.0
     return g
 
 

@@ -13,7 +13,9 @@ The only data exchanged is one N^2 state per rank boundary per iteration
 The final state ends on the last rank and is broadcast to every rank.
 
 The compute backend is pluggable (``CudaSlices`` runs libccfv); the
-exchange and ordering logic is the same for any backend.
+exchange and ordering logic is the same for any backend.  The delta form
+propagates slice increments with the linear part of G: a backend whose grid
+has a source term provides ``coarse_increment`` (G without the source).
 """
 from __future__ import annotations
 
@@ -22,7 +24,7 @@ import math
 import torch
 import torch.distributed as dist
 
-from . import FORM_DELTA, FORM_STANDARD, FP64
+from . import FORM_DELTA, FORM_STANDARD, FP64, SRC_NONE, Solver
 
 
 class CudaSlices:
@@ -32,6 +34,7 @@ class CudaSlices:
         self.s = solver
         self.nx, self.ny = solver.grid.nx, solver.grid.ny
         self.device = torch.device("cuda", solver.device)
+        self._hom = None
 
     def zeros(self, n):
         return torch.zeros(n, self.nx, self.ny, dtype=torch.float64, device=self.device)
@@ -41,6 +44,15 @@ class CudaSlices:
 
     def coarse(self, field, t, DT, m):
         self.s.coarse(field, t, DT, m, FP64)
+
+    def coarse_increment(self, field, t, DT, m):
+        if self.s.grid.source == SRC_NONE:
+            return self.coarse(field, t, DT, m)
+        if self._hom is None:
+            g = type(self.s.grid).from_buffer_copy(self.s.grid)
+            g.source = SRC_NONE
+            self._hom = Solver(g, self.s.device)
+        self._hom.coarse(field, t, DT, m, FP64)
 
     def correct(self, form, U, F, W, Gold=None):
         return self.s.correct(form, U, F, W, Gold)
@@ -103,6 +115,7 @@ def parareal_dist(backend, C0, *, t0, t1, nt_fine, n_slices, coarse_ratio=0, tol
         recv_left(U[0])
         worst = 0.0
         if form == FORM_DELTA:
+            g_inc = getattr(backend, "coarse_increment", backend.coarse)
             W.copy_(U[0] - prev_first)          # increment entering this block
             zero = (r == 0)                     # U[0] never changes: G(0) = 0
             for i in range(n):
@@ -110,7 +123,7 @@ def parareal_dist(backend, C0, *, t0, t1, nt_fine, n_slices, coarse_ratio=0, tol
                     W.zero_()
                     zero = False
                 else:
-                    backend.coarse(W, t0 + (lo + i) * DT, DT, m)
+                    g_inc(W, t0 + (lo + i) * DT, DT, m)
                 du, uu = backend.correct(FORM_DELTA, U[i + 1], F[i], W)
                 worst = max(worst, math.sqrt(du) / math.sqrt(uu) if uu > 0 else math.sqrt(du))
         else:

@@ -17,6 +17,8 @@ bool grid_ok(const ccfv_grid *g) {
   if (g->velocity == CCFV_VEL_SWIRL && g->vel_params[0] == 0.0) return false;
   if (g->scheme != CCFV_SCHEME_REFERENCE && g->scheme != CCFV_SCHEME_CONSISTENT) return false;
   if (!(g->K >= 0.0)) return false;
+  if (g->source != CCFV_SRC_NONE && g->source != CCFV_SRC_GAUSSIAN) return false;
+  if (g->source == CCFV_SRC_GAUSSIAN && !(g->source_params[3] > 0.0)) return false;
   return true;
 }
 
@@ -226,7 +228,8 @@ int ccfv_sweep_plan(ccfv_ctx *ctx, double dt, int precision, int variant[3], int
     const double Dt = kind == 1 ? dt : 0.5 * dt;
     const int dsrc = (kind == 2 && ctx->grid.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
     const LaunchGeom G = step_geom(ctx->grid, dir, Dt, dsrc, precision == CCFV_FP64);
-    if (variant) variant[kind] = ctx->force_general ? SWEEP_GENERAL : G.variant;
+    if (variant)
+      variant[kind] = (ctx->force_general && G.variant != SWEEP_GENERAL_SRC) ? SWEEP_GENERAL : G.variant;
     if (segment) segment[kind] = G.lc_max;
   }
   return CCFV_OK;

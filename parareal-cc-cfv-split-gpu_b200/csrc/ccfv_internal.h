@@ -56,6 +56,10 @@ struct SweepField {
   int phase;             // slice-indexed fields: 0 every launch, 1 only while the
                          // instance's nlo < 0 (first coarse sweep), 2 only while
                          // nlo >= 0 (Parareal iterations)
+  int src;               // source term: 0 none (the reference's f = 0), 1 Gaussian
+  int src_tb;            // 1: the remapped source is f(t_b) too (third sub-step), else f(t_a)
+  double sp[5];          // Gaussian source: sp0 exp(-((x-sp1)^2+(y-sp2)^2)/sp3) cos(sp4 t)
+  double src_w;          // RHS weight of (remapped f(t_a or t_b) + f(t_b))
   double t_step;         // added per launch step: time = ... + jstep * t_step
   double t_slice;        // added per launch slice: time = ... + slice * t_slice
   double vp[4];          // velocity parameters
@@ -72,14 +76,19 @@ struct SweepField {
   const void *tab;         // T[3L]: alpha_k | g_k | z_k (solver factors)
 };
 
+// Shared-memory slot of one descriptor at the head of every sweep kernel's
+// dynamic shared memory (the data behind it stays 64-byte aligned).
+constexpr size_t FD_BYTES = (sizeof(SweepField) + 63) & ~size_t(63);
+
 // Kernel variants: the per-cell kernel (any velocity / boundary / scheme) and
 // the fused stencil kernel (uniform displacement, periodic, derivative of the
 // sweep input).
-enum { SWEEP_GENERAL = 0, SWEEP_FAST = 1, SWEEP_FILTER = 2 };
+// SWEEP_GENERAL_SRC is the per-cell kernel with the source tile staged.
+enum { SWEEP_GENERAL = 0, SWEEP_FAST = 1, SWEEP_FILTER = 2, SWEEP_GENERAL_SRC = 3 };
 constexpr int FILTER_JMAX = 64;  // longest recurrence warm-up of the filter kernel
 
 // Shared-memory bytes of the sweep kernels for a launch.
-size_t sweep_smem_bytes(int lc_max, int halo, bool fp64);
+size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source = false);
 size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64);
 size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64);
 

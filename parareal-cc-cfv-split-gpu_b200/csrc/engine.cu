@@ -203,6 +203,10 @@ SweepField make_field(const ccfv_grid &g, int dir, double Dt, double ta_rel, dou
   f.ta_rel = ta_rel;
   f.tb_rel = tb_rel;
   f.kb = 0.5 * g.K * (Dt / f.h);
+  f.src = g.source;
+  for (int i = 0; i < 5; ++i) f.sp[i] = g.source_params[i];
+  f.src_w = g.source ? (g.scheme == CCFV_SCHEME_REFERENCE ? 0.5 : 0.25) * Dt : 0.0;
+  f.src_tb = 0;  // 1 for the third sub-step (f(t_n+1) remapped): set by the caller
   f.inv12h = 1.0 / (12.0 * f.h);
   f.tab = tab->buf.p;
   f.sm_fac = tab->sm_fac;
@@ -258,8 +262,8 @@ LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64
   G.halo = dsrc ? (sh + 4) + sh + 5 : sh + 5;
   const bool uniform = g.velocity == CCFV_VEL_REF_ROT4 || g.velocity == CCFV_VEL_CONST ||
                        g.velocity == CCFV_VEL_ROTATION;
-  G.variant = SWEEP_GENERAL;
-  if (uniform && g.bc == CCFV_BC_PERIODIC && dsrc == 0) {
+  G.variant = g.source ? SWEEP_GENERAL_SRC : SWEEP_GENERAL;
+  if (!g.source && uniform && g.bc == CCFV_BC_PERIODIC && dsrc == 0) {
     int J = 0;
     if (filter_params(g, dir, Dt, fp64, nullptr, nullptr, &J) && L > 2 * J) {
       G.variant = SWEEP_FILTER;
@@ -352,8 +356,9 @@ static void sweep_kind(int kind, double dt, int *dir, double *Dt, double *ta, do
 }
 
 int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
-                    const std::vector<std::pair<void *, double>> &fields) {
-  const ccfv_grid &g = ctx->grid;
+                    const std::vector<std::pair<void *, double>> &fields, bool homogeneous) {
+  ccfv_grid g = ctx->grid;
+  if (homogeneous) g.source = CCFV_SRC_NONE;
   const int nf = (int)fields.size();
   std::vector<SweepField> h(3 * (size_t)nf);
   for (int kind = 0; kind < 3; ++kind) {
@@ -365,16 +370,18 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
     const SolverTable *tab = get_table(ctx, dir, Dt, fp64, &st);
     if (!tab) return st;
     LaunchGeom G = step_geom(g, dir, Dt, dsrc, fp64);
-    if (ctx->force_general) G.variant = SWEEP_GENERAL;
+    if (ctx->force_general && G.variant != SWEEP_GENERAL_SRC) G.variant = SWEEP_GENERAL;
     if (G.cs > MAX_CLUSTER)
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
-    if (std::max({sweep_smem_bytes(G.lc_max, G.halo, fp64), sweep_fast_smem_bytes(G.lc_max, G.halo, fp64),
+    if (std::max({sweep_smem_bytes(G.lc_max, G.halo, fp64, g.source != 0),
+                  sweep_fast_smem_bytes(G.lc_max, G.halo, fp64),
                   sweep_filter_smem_bytes(G.lc_max, G.halo, fp64)}) > 227 * 1024)
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
     for (int i = 0; i < nf; ++i) {
       SweepField f = make_field(g, dir, Dt, ta + fields[i].second, tb + fields[i].second,
                                 fields[i].first, tab, dsrc);
       if (G.variant == SWEEP_FILTER) filter_field(g, f, fp64);
+      f.src_tb = kind == 2 ? 1 : 0;
       f.group0 = i * f.groups;
       h[(size_t)kind * nf + i] = f;
       plan->groups_per_field[kind] = f.groups;
@@ -405,13 +412,15 @@ int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int
   return CCFV_OK;
 }
 
-static StepPlan *single_plan(ccfv_ctx *ctx, double dt, bool fp64, int *status) {
-  auto key = std::make_tuple(dt, fp64 ? 1 : 0);
+static StepPlan *single_plan(ccfv_ctx *ctx, double dt, bool fp64, int *status,
+                             bool homogeneous = false) {
+  homogeneous = homogeneous && ctx->grid.source != CCFV_SRC_NONE;
+  auto key = std::make_tuple(dt, fp64 ? 1 : 0, homogeneous ? 1 : 0);
   auto it = ctx->step_plans.find(key);
   if (it != ctx->step_plans.end()) return it->second.get();
   auto plan = std::make_unique<StepPlan>();
   std::vector<std::pair<void *, double>> f{{nullptr, 0.0}};
-  int st = build_step_plan(ctx, plan.get(), dt, fp64, f);
+  int st = build_step_plan(ctx, plan.get(), dt, fp64, f, homogeneous);
   if (st != CCFV_OK) {
     *status = st;
     return nullptr;
@@ -588,6 +597,9 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
   if (!iplan) return status;
   StepPlan *cplan = single_plan(ctx, dtc, g64, &status);
   if (!cplan) return status;
+  // the delta form propagates increments: the linear part of G (no source)
+  StepPlan *dplan = o->form == CCFV_FORM_DELTA ? single_plan(ctx, dtc, g64, &status, true) : cplan;
+  if (!dplan) return status;
 
   cudaEvent_t ev0, ev1;
   CK(cudaEventCreate(&ev0));
@@ -596,9 +608,9 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
   const cudaMemcpyKind k_in = o->mem == CCFV_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   CK(cudaMemcpyAsync(U, C0, fb, k_in, st));
 
-  auto coarse_on_W = [&](int n) -> int {
+  auto coarse_on_W = [&](int n, const StepPlan *plan) -> int {
     for (int i = 0; i < m; ++i) {
-      int rc = run_step_plan(ctx, *cplan, g64, 0, 1, o->t0 + n * DT + i * dtc, W, st);
+      int rc = run_step_plan(ctx, *plan, g64, 0, 1, o->t0 + n * DT + i * dtc, W, st);
       if (rc) return rc;
     }
     return CCFV_OK;
@@ -645,12 +657,12 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
       int rc;
       if (o->form == CCFV_FORM_STANDARD) {
         CK(cudaMemcpyAsync(W, U + (size_t)n * NN, fb, cudaMemcpyDeviceToDevice, st));
-        if ((rc = coarse_on_W(n))) return rc;
+        if ((rc = coarse_on_W(n, cplan))) return rc;
         coarse_cu += (double)m * NN;
       } else if (n == nlo) {
         CK(cudaMemsetAsync(W, 0, sizeof(TG) * NN, st));  // G(0) = 0
       } else {
-        if ((rc = coarse_on_W(n))) return rc;
+        if ((rc = coarse_on_W(n, dplan))) return rc;
         coarse_cu += (double)m * NN;
       }
       if ((rc = correction<TG>(ctx, o->form, NN, U + (size_t)(n + 1) * NN,

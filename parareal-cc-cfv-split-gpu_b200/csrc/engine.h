@@ -53,7 +53,7 @@ struct ccfv_ctx {
   int device = 0;
   ccfv::DevBuf status;  // unsigned status word + partial-sum scratch
   std::map<std::tuple<int, double, int>, std::unique_ptr<ccfv::SolverTable>> tables;
-  std::map<std::tuple<double, int>, std::unique_ptr<ccfv::StepPlan>> step_plans;
+  std::map<std::tuple<double, int, int>, std::unique_ptr<ccfv::StepPlan>> step_plans;
   // Parareal slice states and scratch
   ccfv::DevBuf U, F, Gold, W, C64, C32, norms, partial, counter, io, aux;
   size_t slices_cap = 0;
@@ -75,8 +75,11 @@ void filter_field(const ccfv_grid &g, SweepField &f, bool fp64);
 int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen);
 int batch_solve(int n, const ccfv_problem *probs, ccfv_stats *stats, int device,
                 cudaStream_t st, std::string *errmsg);
+// homogeneous: the source term is left out (the linear part of the step,
+// which the delta form of Parareal applies to slice increments).
 int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
-                    const std::vector<std::pair<void *, double>> &fields);
+                    const std::vector<std::pair<void *, double>> &fields,
+                    bool homogeneous = false);
 int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int count,
                   double toff, void *data_override, cudaStream_t st);
 int steps(ccfv_ctx *ctx, void *d_C, bool fp64, double t0, double dt, int nsteps, cudaStream_t st);

@@ -244,7 +244,8 @@ int MultiEngine::add(const ccfv_problem &pr, int *slot) {
       const int dsrc = (kind == 2 && P->g.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
       const LaunchGeom G = step_geom(P->g, dir, Dt, dsrc, level == 0 || P->g64);
       if (G.cs > MAX_CLUSTER) return fail(CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
-      if (std::max({sweep_smem_bytes(G.lc_max, G.halo, true), sweep_fast_smem_bytes(G.lc_max, G.halo, true),
+      if (std::max({sweep_smem_bytes(G.lc_max, G.halo, true, P->g.source != 0),
+                    sweep_fast_smem_bytes(G.lc_max, G.halo, true),
                     sweep_filter_smem_bytes(G.lc_max, G.halo, true)}) > 227 * 1024)
         return fail(CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
     }
@@ -328,6 +329,7 @@ int MultiEngine::rebuild() {
                                     P->F + (size_t)(s + 1) * P->NN, P->tab[dir], dsrc);
           f.inst = i;
           f.slice = s;
+          f.src_tb = kind == 2 ? 1 : 0;
           f.jmax = P->J;
           f.t_step = P->dt;
           add_field(fine_, kind, g, f, true);
@@ -346,15 +348,20 @@ int MultiEngine::rebuild() {
           f.t_step = P->dtc;
           f.t_slice = P->DT;
           f.phase = phase;
+          f.src_tb = kind == 2 ? 1 : 0;
           return f;
         };
-        if (P->g64) {
+        const bool delta_src = g.source != CCFV_SRC_NONE && P->o.form == CCFV_FORM_DELTA;
+        if (P->g64 && !delta_src) {
           add_field(coarse_, kind, g, coarse_field(g, P->tab[2 + dir], 0), true);
         } else {
-          // the first sweep moves states in FP64; the iterations move
-          // increments in FP32
+          // the first sweep moves states: FP64, with the source; the
+          // iterations move increments in the coarse precision (delta form:
+          // with the linear part of G, without the source)
           add_field(coarse_, kind, g, coarse_field(g, P->tab[4 + dir], 1), true);
-          add_field(coarse_, kind, g, coarse_field(g, P->tab[2 + dir], 2), false);
+          ccfv_grid gh = g;
+          if (P->o.form == CCFV_FORM_DELTA) gh.source = CCFV_SRC_NONE;
+          add_field(coarse_, kind, gh, coarse_field(gh, P->tab[2 + dir], 2), P->g64);
         }
       }
     }

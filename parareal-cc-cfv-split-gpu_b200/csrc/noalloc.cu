@@ -32,7 +32,7 @@ namespace ccfv {
 namespace {
 
 constexpr int NOALLOC_MAX_LINE = 4096;
-constexpr size_t NOALLOC_HDR = 1024;  // status word + 3 sweep descriptors
+constexpr size_t NOALLOC_HDR = 2048;  // status word + 3 sweep descriptors
 // solver table of one direction (layout of table_len(): factors, chunk products)
 constexpr size_t NOALLOC_TAB_LEN =
     5 * (size_t)NOALLOC_MAX_LINE + (size_t)MAX_CLUSTER * NCH + (size_t)MAX_CLUSTER * (NCH + 1);
@@ -114,7 +114,9 @@ bool grid_valid(const ccfv_grid *g) {
          g->velocity >= CCFV_VEL_REF_ROT4 && g->velocity <= CCFV_VEL_SWIRL &&
          !(g->velocity == CCFV_VEL_SWIRL && g->vel_params[0] == 0.0) &&
          (g->scheme == CCFV_SCHEME_REFERENCE || g->scheme == CCFV_SCHEME_CONSISTENT) &&
-         g->K >= 0.0;
+         g->K >= 0.0 &&
+         (g->source == CCFV_SRC_NONE ||
+          (g->source == CCFV_SRC_GAUSSIAN && g->source_params[3] > 0.0));
 }
 
 }  // namespace
@@ -169,6 +171,7 @@ extern "C" int ccfv_step_noalloc(const ccfv_grid *grid, double *d_C, double tn, 
     h_fields[kind] = make_field(g, dir, Dt, ta, tb, d_C, &view, dsrc);
     view.buf.p = nullptr;
     h_fields[kind].group0 = 0;
+    h_fields[kind].src_tb = kind == 2 ? 1 : 0;
     LaunchGeom &G = geom[kind];
     G.cs = (L + LC_MAX - 1) / LC_MAX;
     G.lc_max = (L + G.cs - 1) / G.cs;
@@ -176,8 +179,9 @@ extern "C" int ccfv_step_noalloc(const ccfv_grid *grid, double *d_C, double tn, 
     G.halo = dsrc ? (sh + 4) + sh + 5 : sh + 5;
     const bool uniform = g.velocity == CCFV_VEL_REF_ROT4 || g.velocity == CCFV_VEL_CONST ||
                          g.velocity == CCFV_VEL_ROTATION;
-    G.variant = (uniform && g.bc == CCFV_BC_PERIODIC && dsrc == 0) ? SWEEP_FAST : SWEEP_GENERAL;
-    if (std::max(sweep_smem_bytes(G.lc_max, G.halo, true),
+    G.variant = g.source ? SWEEP_GENERAL_SRC
+                : (uniform && g.bc == CCFV_BC_PERIODIC && dsrc == 0) ? SWEEP_FAST : SWEEP_GENERAL;
+    if (std::max(sweep_smem_bytes(G.lc_max, G.halo, true, g.source != 0),
                  sweep_fast_smem_bytes(G.lc_max, G.halo, true)) > 227 * 1024)
       return CCFV_ERR_UNSUPPORTED;
   }

@@ -244,6 +244,27 @@ __device__ __forceinline__ void compat_ghosts(T *c, int base, int lo, int hi, in
   }
 }
 
+// Source f(x, y, t) (the reference's f is identically zero, T2S4:58-61;
+// Gaussian: sp0 exp(-((x-sp1)^2 + (y-sp2)^2) / sp3) cos(sp4 t)).
+__device__ __forceinline__ double src_f(const SweepField &f, double x, double y, double t) {
+  const double dx = x - f.sp[1], dy = y - f.sp[2];
+  return f.sp[0] * exp(-(dx * dx + dy * dy) / f.sp[3]) * cos(f.sp[4] * t);
+}
+
+// 3x3 Simpson cell average of f over cell `pos` of line `gl` at time t
+// (get_source_term_on_gpu, T2S4:142-165).
+__device__ double src_cell(const SweepField &f, int pos, long long gl, double t) {
+  const double s = f.s_min + (pos + 0.5) * f.h, tau = f.t_min + (gl + 0.5) * f.ht;
+  const double x_i = f.dir == 0 ? s : tau, y_j = f.dir == 0 ? tau : s;
+  const double dx = f.dir == 0 ? f.h : f.ht, dy = f.dir == 0 ? f.ht : f.h;
+  const double xm = x_i - 0.5 * dx, xp = x_i + 0.5 * dx, ym = y_j - 0.5 * dy, yp = y_j + 0.5 * dy;
+  return 1.0 / 36.0 *
+         (src_f(f, xm, ym, t) + src_f(f, xp, ym, t) + src_f(f, xm, yp, t) + src_f(f, xp, yp, t) +
+          4.0 * (src_f(f, xm, y_j, t) + src_f(f, xp, y_j, t) + src_f(f, x_i, ym, t) +
+                 src_f(f, x_i, yp, t)) +
+          16.0 * src_f(f, x_i, y_j, t));
+}
+
 // Shared-memory carve-up of the sweep kernel.
 template <typename T>
 struct Smem {
@@ -259,6 +280,7 @@ struct Smem {
   T *aggF;   // [NCH * LPG] chunk forward values
   T *aggR;   // [NCH * LPG] chunk backward values
   T *xch;    // [8 * LPG] cluster exchange: fwdA fwdB bwdA bwdB y0 yL
+  T *Fs;     // [(lc_max + 2H) * PITCH] source cell averages at t_a (source variant only)
   SweepField *fd;
 };
 
@@ -266,7 +288,7 @@ template <typename T>
 __device__ __forceinline__ Smem<T> carve(unsigned char *raw, int lc_max, int H) {
   Smem<T> s;
   s.fd = reinterpret_cast<SweepField *>(raw);
-  T *p = reinterpret_cast<T *>(raw + ((sizeof(SweepField) + 15) & ~size_t(15)));
+  T *p = reinterpret_cast<T *>(raw + FD_BYTES);
   s.C = p;
   p += (lc_max + 2 * H) * PITCH;
   s.B = p;
@@ -284,6 +306,8 @@ __device__ __forceinline__ Smem<T> carve(unsigned char *raw, int lc_max, int H) 
   s.aggR = p;
   p += NCH * LPG;
   s.xch = p;
+  p += 8 * LPG;
+  s.Fs = p;
   return s;
 }
 
@@ -355,6 +379,27 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
   }
   __syncthreads();
   if (!periodic && threadIdx.x < LPG) compat_ghosts(S.C + threadIdx.x, H - p0, p0 - H, p1 + H, L);
+  // source: f(t_a) (f(t_b) in the third sub-step) on the staged rows, remapped
+  // like C (T2S4:846-853, 893-900, 944-951); f(t_b) enters unremapped
+  const double t_src0 = toff + (F.src_tb ? F.tb_rel : F.ta_rel);
+  const double t_src1 = toff + F.tb_rel;
+  if (F.src) {
+    for (int e = threadIdx.x; e < nrows * LPG; e += NTH) {
+      const int row = e / LPG, l = e - row * LPG;
+      int pos = p0 - H + row;
+      T val = T(0);
+      if (periodic) {
+        pos %= L;
+        if (pos < 0) pos += L;
+        val = T(src_cell(F, pos, line0 + l, t_src0));
+      } else if (pos >= 0 && pos < L) {
+        val = T(src_cell(F, pos, line0 + l, t_src0));
+      }
+      S.Fs[row * PITCH + l] = val;
+    }
+    __syncthreads();
+    if (!periodic && threadIdx.x < LPG) compat_ghosts(S.Fs + threadIdx.x, H - p0, p0 - H, p1 + H, L);
+  }
   __syncthreads();
 
   // ---- thread -> (line, chunk) ----
@@ -369,10 +414,21 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
   LineView<T> v{S.C + ln, H - p0, nrows, status};
 
   // ---- phase 1: feet, remap, foot derivative, RHS b ----
-  // b_k = remap_k + 0.5 K Dt/h (D_{k+1} - D_k) (x_b_RHS_on_gpu T2S4:564-580);
-  // the source f is identically zero (T2S4:59-61) and adds nothing.
+  // b_k = remap_k + w (remap(f)_k + f_k) + 0.5 K Dt/h (D_{k+1} - D_k)
+  // (x_b_RHS_on_gpu / y_b_RHS_on_gpu, T2S4:564-613); w = src_w, 0 without a
+  // source (the reference's f is identically zero, T2S4:58-61).
   T *bArr, *qArr;
   {
+    const LineView<T> vf{S.Fs + ln, H - p0, nrows, status};  // read only when F.src
+    const T srcw = T(F.src_w);
+    auto src_term = [&](int k, double fa, double fb) -> T {
+      int kk = k;
+      if (periodic) { kk %= L; if (kk < 0) kk += L; }
+      return srcw * (remap_cell(F, vf, fa, fb) + T(src_cell(F, kk, line0 + ln, t_src1)));
+    };
+    // the shared-foot stencils cover C only; with a source every cell takes
+    // the per-cell path
+    const bool stencil = F.uniform && !F.src;
     int kb = s, ke = e;
     if (c == 0 && (periodic || p0 > 0)) kb = p0 - 1;
     if (c == clast && (periodic || p1 < L)) ke = p1 + 1;
@@ -388,7 +444,7 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
     // per-cell formulas, so the fast and per-cell paths agree to rounding.
     int n0 = 0, klo = 1, khi = 0;
     T w[6], qd[6];
-    if (F.uniform) {
+    if (stencil) {
       const double f0 = edge_foot(F, 0, tau0, tau1, ta, tb);
       const double u = (f0 - F.s_min) / F.h;
       const double fl = floor(u);
@@ -419,7 +475,7 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
     if (F.dsrc == 0) {
       bArr = S.B;
       qArr = S.C;
-      if (F.uniform) {
+      if (stencil) {
         for (int k = kb; k < ke; ++k) {
           T bk;
           if (k >= klo && k <= khi) {
@@ -445,7 +501,9 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
           double fnext = edge_foot(F, k + 1, tau0, tau1, ta, tb);
           T dnext = foot_derivative(F, v, fnext);
           T ic = remap_cell(F, v, fprev, fnext);
-          bArr[(k - p0 + H) * PITCH + ln] = ic + kbc * (dnext - dprev);
+          T bk = ic + kbc * (dnext - dprev);
+          if (F.src) bk += src_term(k, fprev, fnext);
+          bArr[(k - p0 + H) * PITCH + ln] = bk;
           fprev = fnext;
           dprev = dnext;
         }
@@ -461,7 +519,7 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
       const int r0 = q0 + c * m1, r1 = min(q1, r0 + m1);
       for (int k = r0; k < r1; ++k) {
         T ik;
-        if (F.uniform && k >= klo && k <= khi) {
+        if (stencil && k >= klo && k <= khi) {
           const int r = k + n0 + H - p0 - 2;
           const T *cp = S.C + r * PITCH + ln;
           if (r < 0 || r + 5 >= nrows) { atomicOr(status, STATUS_HALO); ik = T(0); }
@@ -485,7 +543,7 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
       qArr = S.B;
       for (int k = kb; k < ke; ++k) {
         T bk;
-        if (F.uniform && k >= klo && k <= khi) {
+        if (stencil && k >= klo && k <= khi) {
           const int r = k + n0 + H - p0 - 2;
           const T *rp = R + r * PITCH + ln;
           if (r < 0 || r + 5 >= nrows) { atomicOr(status, STATUS_HALO); bk = T(0); }
@@ -499,6 +557,7 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
           double fa = edge_foot(F, k, tau0, tau1, ta, tb);
           double fb = edge_foot(F, k + 1, tau0, tau1, ta, tb);
           bk = vr(k) + kbc * (foot_derivative(F, vr, fb) - foot_derivative(F, vr, fa));
+          if (F.src) bk += src_term(k, fa, fb);
         }
         bArr[(k - p0 + H) * PITCH + ln] = bk;
       }
@@ -666,7 +725,7 @@ __device__ __forceinline__ void cp_async_wait_all_committed() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-static_assert(sizeof(SweepField) <= 256 && sizeof(SweepField) % 8 == 0, "descriptor slot");
+static_assert(sizeof(SweepField) % 8 == 0, "descriptor slot");
 
 template <typename T>
 struct FastSmem {
@@ -688,8 +747,8 @@ template <typename T>
 __device__ __forceinline__ FastSmem<T> carve_fast(unsigned char *raw, int lc_max, int H) {
   FastSmem<T> s;
   s.fd = reinterpret_cast<SweepField *>(raw);
-  s.n0 = reinterpret_cast<int *>(raw + 256);
-  T *p = reinterpret_cast<T *>(raw + 256 + 64 * sizeof(int));
+  s.n0 = reinterpret_cast<int *>(raw + FD_BYTES);
+  T *p = reinterpret_cast<T *>(raw + FD_BYTES + 64 * sizeof(int));
   s.C = p; p += (lc_max + 2 * H) * PITCH;
   s.Q = p; p += lc_max * PITCH;
   s.tA = p; p += lc_max;
@@ -1013,8 +1072,8 @@ template <typename T>
 __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max, int H) {
   FiltSmem<T> s;
   s.fd = reinterpret_cast<SweepField *>(raw);
-  s.n0 = reinterpret_cast<int *>(raw + 256);
-  T *p = reinterpret_cast<T *>(raw + 256 + 64 * sizeof(int));
+  s.n0 = reinterpret_cast<int *>(raw + FD_BYTES);
+  T *p = reinterpret_cast<T *>(raw + FD_BYTES + 64 * sizeof(int));
   s.om = p; p += 6 * LPG;
   s.C = p; p += (lc_max + 2 * H) * PITCH;
   s.R = p;
@@ -1222,23 +1281,23 @@ __global__ void __launch_bounds__(NTH, 3)
 
 }  // namespace
 
-size_t sweep_smem_bytes(int lc_max, int halo, bool fp64) {
+size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source) {
   size_t el = fp64 ? 8 : 4;
-  size_t n = 2 * (size_t)(lc_max + 2 * halo) * PITCH +
+  size_t n = (source ? 3 : 2) * (size_t)(lc_max + 2 * halo) * PITCH +
              3 * (size_t)lc_max + 3 * (size_t)NCH * LPG + 8 * (size_t)LPG;
-  return ((sizeof(SweepField) + 15) & ~size_t(15)) + n * el;
+  return FD_BYTES + n * el;
 }
 
 size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64) {
   size_t el = fp64 ? 8 : 4;
-  return 256 + 64 * sizeof(int) + (6 * (size_t)LPG + 2 * (size_t)(lc_max + 2 * halo) * PITCH) * el;
+  return FD_BYTES + 64 * sizeof(int) + (6 * (size_t)LPG + 2 * (size_t)(lc_max + 2 * halo) * PITCH) * el;
 }
 
 size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64) {
   size_t el = fp64 ? 8 : 4;
   size_t n = (size_t)(lc_max + 2 * halo) * PITCH + (size_t)lc_max * PITCH + 5 * (size_t)lc_max +
              2 * (size_t)NCH + 1 + 2 * (size_t)NCH * LPG + 16 * (size_t)LPG;
-  return 256 + 64 * sizeof(int) + n * el;
+  return FD_BYTES + 64 * sizeof(int) + n * el;
 }
 
 template <typename T>
@@ -1248,9 +1307,10 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
                                int nslice, const int *nlo, cudaStream_t stream) {
   const bool fast = (variant == SWEEP_FAST);
   const bool filt = (variant == SWEEP_FILTER);
+  const bool src = (variant == SWEEP_GENERAL_SRC);
   const size_t smem = filt ? sweep_filter_smem_bytes(lc_max, halo, sizeof(T) == 8)
                       : fast ? sweep_fast_smem_bytes(lc_max, halo, sizeof(T) == 8)
-                             : sweep_smem_bytes(lc_max, halo, sizeof(T) == 8);
+                             : sweep_smem_bytes(lc_max, halo, sizeof(T) == 8, src);
   static bool configured = false;
   if (!configured) {
     for (const void *fn : {(const void *)sweep_kernel<T>, (const void *)sweep_fast_kernel<T>,

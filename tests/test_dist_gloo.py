@@ -13,6 +13,7 @@ import torch.multiprocessing as mp
 
 N, T, NT, S, RATIO, KMAX = 24, 0.25, 48, 6, 2, 4
 VP = (2 * np.pi, 0.5, 0.5)
+SP = (2.0, 0.4, 0.6, 0.04, 5.0)  # Gaussian source (time-dependent)
 
 
 class OracleSlices:
@@ -32,6 +33,11 @@ class OracleSlices:
     def coarse(self, field, t, DT, m):
         field.copy_(torch.from_numpy(self.O.coarse(self.g, field.numpy(), t, DT, m)))
 
+    def coarse_increment(self, field, t, DT, m):
+        g = type(self.g).from_buffer_copy(self.g)
+        g.src = 0
+        field.copy_(torch.from_numpy(self.O.coarse(g, field.numpy(), t, DT, m)))
+
     def correct(self, form, U, F, W, Gold=None):
         u, f, w = U.numpy(), F.numpy(), W.numpy()
         if form == 0:  # standard
@@ -47,7 +53,11 @@ class OracleSlices:
         return float((d * d).sum()), float((nv * nv).sum())
 
 
-def _worker(rank, world, port, form, q):
+def _grid(O, src):
+    return O.grid(N, bc=1, vel=2, vp=VP, K=1e-3, scheme=1, src=src, sp=SP)
+
+
+def _worker(rank, world, port, form, src, q):
     import sys
     from pathlib import Path
     root = Path(__file__).resolve().parents[1]
@@ -60,7 +70,7 @@ def _worker(rank, world, port, form, q):
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
                             world_size=world)
     try:
-        g = O.grid(N, bc=1, vel=2, vp=VP, K=1e-3, scheme=1)
+        g = _grid(O, src)
         C0 = torch.from_numpy(periodic_field(N, 4))
         out, st = parareal_dist(OracleSlices(O, g), C0, t0=0.0, t1=T, nt_fine=NT, n_slices=S,
                                 coarse_ratio=RATIO, tol=0.0, kmax=KMAX, form=form)
@@ -75,20 +85,21 @@ def _free_port():
         return s.getsockname()[1]
 
 
+@pytest.mark.parametrize("src", [0, 1], ids=["nosource", "source"])
 @pytest.mark.parametrize("form", [1, 0], ids=["delta", "standard"])
-def test_distributed_parareal_matches_single_process(oracle, form):
+def test_distributed_parareal_matches_single_process(oracle, form, src):
     from conftest import periodic_field
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, form, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, form, src, q)) for r in range(2)]
     for p in procs:
         p.start()
     res = [q.get(timeout=240) for _ in procs]
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    g = oracle.grid(N, bc=1, vel=2, vp=VP, K=1e-3, scheme=1)
+    g = _grid(oracle, src)
     ref, it, upd = oracle.parareal(g, periodic_field(N, 4), t0=0.0, t1=T, nt_fine=NT,
                                    n_slices=S, coarse_steps=(NT // S) // RATIO, tol=0.0,
                                    kmax=KMAX, form=form)

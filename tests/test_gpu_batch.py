@@ -8,6 +8,7 @@ import pytest
 from conftest import periodic_field, rel_l2
 
 pytestmark = pytest.mark.gpu
+SRC = (2.0, 0.4, 0.6, 0.03, 5.0)
 
 
 def dev(a):
@@ -25,10 +26,17 @@ def _problems(ccfv):
         (300, 1, (0.3, 0.4), 1e-4, 6, 60, 2, 0, 1, 0.0),
         (48, 3, (1.5,), 1e-3, 4, 32, 2, 0, 1, 0.0),
         (520, 2, (2 * np.pi, 0.5, 0.5), 5e-4, 8, 128, 4, 1, 1, 0.0),
+        # with a Gaussian source: delta form (increments through G without
+        # it) in FP64 and FP32, standard form
+        (96, 2, (2 * np.pi, 0.5, 0.5), 1e-3, 8, 64, 2, 0, 1, 0.0, SRC),
+        (80, 1, (0.8, -0.4), 1e-3, 8, 64, 2, 1, 1, 0.0, SRC),
+        (72, 2, (2 * np.pi, 0.5, 0.5), 1e-3, 6, 48, 2, 0, 0, 0.0, SRC),
     ]
     probs = []
-    for N, vel, vp, K, S, nt, ratio, prec, form, tol in specs:
-        g = ccfv.make_grid(N, bc=1, velocity=vel, vel_params=vp, K=K, scheme=1)
+    for N, vel, vp, K, S, nt, ratio, prec, form, tol, *src in specs:
+        g = ccfv.make_grid(N, bc=1, velocity=vel, vel_params=vp, K=K, scheme=1,
+                           source=1 if src else 0,
+                           source_params=src[0] if src else (0, 0, 0, 1, 0))
         C0 = periodic_field(N, int(rng.integers(1000)))
         probs.append(dict(grid=g, C0=C0, t0=0.0, t1=0.25, nt_fine=nt, n_slices=S,
                           coarse_ratio=ratio, tol=tol, kmax=3, coarse_precision=prec, form=form))

@@ -60,3 +60,56 @@ def test_parareal_converges_to_serial_fine(oracle, ccfv, prec):
                         tol=tol, kmax=S, coarse_precision=prec, form=ccfv.FORM_DELTA)
     assert st["converged"], st
     assert rel_l2(UT.cpu().numpy(), fine) < 10 * tol, st
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_parareal_with_source_matches_oracle(oracle, ccfv, form):
+    """Time-dependent Gaussian source; the delta form propagates increments
+    with the source-free coarse step."""
+    N, T, nt, S, ratio = 40, 0.25, 96, 12, 4
+    vp, sp = (2 * np.pi, 0.5, 0.5), (2.0, 0.4, 0.6, 0.03, 5.0)
+    C0 = periodic_field(N, 7)
+    g = oracle.grid(N, bc=1, vel=2, vp=vp, K=1e-3, threads=THREADS, scheme=1, src=1, sp=sp)
+    ref, it_o, upd_o = oracle.parareal(g, C0, t0=0.0, t1=T, nt_fine=nt, n_slices=S,
+                                       coarse_steps=(nt // S) // ratio, tol=0.0, kmax=4, form=form)
+    s = ccfv.Solver(ccfv.make_grid(N, bc=1, velocity=2, vel_params=vp, K=1e-3, scheme=1,
+                                   source=1, source_params=sp))
+    UT, st = s.parareal(dev(C0), t0=0.0, t1=T, nt_fine=nt, n_slices=S, coarse_ratio=ratio,
+                        tol=0.0, kmax=4, form=form)
+    assert rel_l2(UT.cpu().numpy(), ref) < 1e-12
+    np.testing.assert_allclose(st["update"], upd_o, rtol=1e-6)
+
+
+def test_parareal_with_source_fp32_coarse_converges(ccfv):
+    N, T, nt, S, ratio, tol = 96, 0.5, 192, 12, 4, 1e-10
+    vp, sp = (2 * np.pi, 0.5, 0.5), (2.0, 0.4, 0.6, 0.03, 5.0)
+    s = ccfv.Solver(ccfv.make_grid(N, bc=1, velocity=2, vel_params=vp, K=1e-3, scheme=1,
+                                   source=1, source_params=sp))
+    C0 = periodic_field(N, 8)
+    fine = s.run(C0, 0.0, T / nt, nt)
+    UT, st = s.parareal(dev(C0), t0=0.0, t1=T, nt_fine=nt, n_slices=S, coarse_ratio=ratio,
+                        tol=tol, kmax=S, coarse_precision=1, form=1)
+    assert st["converged"], st
+    assert rel_l2(UT.cpu().numpy(), fine) < 10 * tol, st
+
+
+def test_fp32_coarse_converges_like_fp64_for_advection(ccfv):
+    """Constant velocity, weak diffusion, 64 slices: FP32 coarse Parareal
+    needs no more than two iterations beyond the FP64 one (its first coarse
+    sweep runs in FP64, so FP32 rounding never seeds the high-wavenumber
+    modes that Parareal amplifies)."""
+    N, S, ratio = 414, 64, 8
+    V = (0.84, -0.16)
+    dt = 0.8 / (N * 0.84)
+    nt = int(np.ceil(1.0 / dt / (S * ratio))) * S * ratio
+    s = ccfv.Solver(ccfv.make_grid(N, bc=1, velocity=1, vel_params=V, K=9e-4, scheme=1))
+    import torch
+    C0 = torch.empty(N, N, dtype=torch.float64, device="cuda")
+    s.gaussians(C0, [[0.5, 0.5, 0.005, 1.0], [0.3, 0.7, 0.01, 0.6]], images=1)
+    it = {}
+    for prec in (0, 1):
+        _, st = s.parareal(C0, t0=0.0, t1=1.0, nt_fine=nt, n_slices=S, coarse_ratio=ratio,
+                           tol=1e-10, kmax=S, coarse_precision=prec, form=1)
+        assert st["converged"], st
+        it[prec] = st["iterations"]
+    assert it[1] <= it[0] + 2, it

@@ -179,3 +179,50 @@ def test_fp32_filter_coarse_close_to_fp64(ccfv):
     s.coarse(a, 0.0, 0.02, 2, ccfv.FP64)
     s.coarse(b, 0.0, 0.02, 2, ccfv.FP32)
     assert rel_l2(host(b), host(a)) < 2e-6
+
+
+SRC_COMPAT = (1.5, 0.3, -0.2, 0.05, 4.0)   # on [-1, 1]^2
+SRC_PERIODIC = (2.0, 0.4, 0.6, 0.03, 5.0)  # on [0, 1]^2
+
+
+@pytest.mark.parametrize("scheme", [0, 1])
+@pytest.mark.parametrize("N", [48, 300])
+def test_compat_source_matches_oracle(oracle, ccfv, scheme, N):
+    """Gaussian source: Simpson cell averages, f(t_a) remapped plus f(t_b) in
+    the right-hand side of every sub-step, with either scheme's weight."""
+    dt = 0.1 * (2.0 / N)
+    C0 = seeded_field(N, 17)
+    g = oracle.grid(N, K=1e-3, threads=THREADS, scheme=scheme, src=1, sp=SRC_COMPAT)
+    ref = oracle.run(g, C0, 0.2, dt, 3)
+    s = ccfv.Solver(ccfv.make_grid(N, K=1e-3, scheme=scheme, source=1, source_params=SRC_COMPAT))
+    c = dev(C0)
+    s.run(c, 0.2, dt, 3)
+    s.check()
+    assert rel_l2(host(c), ref) < TOL
+
+
+@pytest.mark.parametrize("name,vel,vp", PERIODIC, ids=[p[0] for p in PERIODIC])
+@pytest.mark.parametrize("scheme", [0, 1])
+def test_periodic_source_matches_oracle(oracle, ccfv, name, vel, vp, scheme):
+    nx, ny = 96, 80
+    dt = 0.8 / nx / 3.2
+    C0 = periodic_field(nx, 19, ny=ny)
+    g = oracle.grid(nx, ny, bc=1, vel=vel, vp=vp, K=1e-3, threads=THREADS, scheme=scheme, src=1,
+                    sp=SRC_PERIODIC)
+    ref = oracle.run(g, C0, 0.1, dt, 3)
+    s = ccfv.Solver(ccfv.make_grid(nx, ny, bc=1, velocity=vel, vel_params=vp, K=1e-3,
+                                   scheme=scheme, source=1, source_params=SRC_PERIODIC))
+    c = dev(C0)
+    s.run(c, 0.1, dt, 3)
+    s.check()
+    assert rel_l2(host(c), ref) < TOL
+
+
+def test_source_sweep_plan(ccfv):
+    """A grid with a source runs the per-cell source kernel in every sub-step."""
+    s = ccfv.Solver(ccfv.make_grid(128, bc=1, velocity=1, vel_params=(1.0, 0.5), K=1e-3,
+                                   scheme=1, source=1, source_params=SRC_PERIODIC))
+    assert [v for v, _ in s.sweep_plan(1e-3)] == ["source"] * 3
+    s0 = ccfv.Solver(ccfv.make_grid(128, bc=1, velocity=1, vel_params=(1.0, 0.5), K=1e-3,
+                                    scheme=1))
+    assert [v for v, _ in s0.sweep_plan(1e-3)] == ["filter"] * 3
