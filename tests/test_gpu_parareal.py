@@ -80,12 +80,14 @@ def test_parareal_with_source_matches_oracle(oracle, ccfv, form):
     np.testing.assert_allclose(st["update"], upd_o, rtol=1e-6)
 
 
-def test_parareal_with_source_fp32_coarse_converges(ccfv):
-    N, T, nt, S, ratio, tol = 96, 0.5, 192, 12, 4, 1e-10
-    vp, sp = (2 * np.pi, 0.5, 0.5), (2.0, 0.4, 0.6, 0.03, 5.0)
+def test_parareal_with_source_fp32_coarse_converges(oracle, ccfv):
+    """One revolution of a Gaussian hump under a pulsating Gaussian source:
+    FP32-coarse delta-form Parareal converges to the serial fine solve."""
+    N, T, nt, S, ratio, tol = 128, 1.0, 512, 16, 4, 1e-10
+    vp, sp = (2 * np.pi, 0.5, 0.5), (1.0, 0.4, 0.6, 0.02, 2 * np.pi)
     s = ccfv.Solver(ccfv.make_grid(N, bc=1, velocity=2, vel_params=vp, K=1e-3, scheme=1,
                                    source=1, source_params=sp))
-    C0 = periodic_field(N, 8)
+    C0 = oracle.gaussians(oracle.grid(N, bc=1), [0.5], [0.75], [2 * 0.05 ** 2], [1.0], img=1)
     fine = s.run(C0, 0.0, T / nt, nt)
     UT, st = s.parareal(dev(C0), t0=0.0, t1=T, nt_fine=nt, n_slices=S, coarse_ratio=ratio,
                         tol=tol, kmax=S, coarse_precision=1, form=1)
