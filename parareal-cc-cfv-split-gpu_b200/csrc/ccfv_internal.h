@@ -47,6 +47,9 @@ struct SweepField {
                          // transverse coordinate (every foot of a line has the
                          // same displacement): stencil fast path
   int jf;                // filter kernel: recurrence warm-up length J
+  int cta0;              // filter kernel: first CTA of this field in the launch
+  int cs_f;              // filter kernel: CTAs (segments) per line of this field
+  int halo_f;            // filter kernel: staged halo (cells) of this field
   // Batched launches (all zero for single-instance launches):
   int inst;              // instance index into the launch's `nlo` array
   int slice;             // >= 0: fixed slice of this field; -1: the launch's slice

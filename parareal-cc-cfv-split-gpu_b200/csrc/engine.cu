@@ -383,6 +383,9 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
       if (G.variant == SWEEP_FILTER) filter_field(g, f, fp64);
       f.src_tb = kind == 2 ? 1 : 0;
       f.group0 = i * f.groups;
+      f.cta0 = f.group0 * G.cs;
+      f.cs_f = G.cs;
+      f.halo_f = G.halo;
       h[(size_t)kind * nf + i] = f;
       plan->groups_per_field[kind] = f.groups;
     }

@@ -147,21 +147,33 @@ __global__ void __launch_bounds__(BT)
 
 using KKey = std::tuple<int, int, int, int, int>;  // kind, variant, cs, lc bucket, fp64
 
+// Launch classes.  The filter kernel's CTAs are independent and every field
+// carries its own segment count and halo, so all filter fields of a sub-step
+// kind and precision share one class (one launch); the cluster kernels group
+// fields by cluster size and segment-length bucket.
 static void add_field(std::map<KKey, SweepClass> &classes, int kind, const ccfv_grid &g,
                       const SweepField &f0, bool fp64) {
   const LaunchGeom G = step_geom(g, f0.dir, f0.Dt, f0.dsrc, fp64);
-  const int bucket = (G.lc_max + 63) / 64;  // segment-length bucket bounds the staged tile
-  SweepClass &K = classes[KKey{kind, G.variant, G.cs, bucket, fp64 ? 1 : 0}];
+  const bool filt = G.variant == SWEEP_FILTER;
+  const int bucket = filt ? 0 : (G.lc_max + 63) / 64;  // segment-length bucket bounds the tile
+  SweepClass &K = classes[KKey{kind, G.variant, filt ? 0 : G.cs, bucket, fp64 ? 1 : 0}];
   K.kind = kind;
   K.variant = G.variant;
-  K.cs = G.cs;
+  K.cs = filt ? 1 : G.cs;  // filter classes count CTAs in `groups`
   K.fp64 = fp64 ? 1 : 0;
   K.lc_max = std::max(K.lc_max, G.lc_max);
   K.halo = std::max(K.halo, G.halo);
   SweepField f = f0;
-  if (G.variant == SWEEP_FILTER) filter_field(g, f, fp64);
   f.group0 = K.groups;
-  K.groups += f.groups;
+  f.cta0 = K.groups;
+  f.cs_f = G.cs;
+  f.halo_f = G.halo;
+  if (filt) {
+    filter_field(g, f, fp64);
+    K.groups += f.groups * G.cs;
+  } else {
+    K.groups += f.groups;
+  }
   K.h.push_back(f);
 }
 
@@ -301,9 +313,12 @@ int MultiEngine::rebuild() {
   std::vector<BElem> he(n);
   norm_off_.assign(n, 0);
   size_t noff = 0;
+  // finished problems keep their slot (their stats are read later) but leave
+  // the launch classes and the element-wise launches
+  auto live = [&](const Problem *P) { return P && P->state != Problem::DONE; };
   for (int i = 0; i < n; ++i) {
     Problem *P = slots_[i].get();
-    if (!P) {
+    if (!live(P)) {
       std::memset(&he[i], 0, sizeof(BElem));
       continue;
     }
@@ -314,7 +329,7 @@ int MultiEngine::rebuild() {
   hnorms_.assign(std::max<size_t>(noff, 2), 0.0);
   for (int i = 0; i < n; ++i) {
     Problem *P = slots_[i].get();
-    if (!P) continue;
+    if (!live(P)) continue;
     const ccfv_grid &g = P->g;
     he[i] = BElem{P->U, P->F, P->Gold, P->W, P->NN, P->S, P->o.form, P->g64 ? 1 : 0, 0,
                   norms_d_.as<double>() + norm_off_[i]};
@@ -527,6 +542,7 @@ int MultiEngine::iterate(std::vector<int> *finished) {
     if (P->converged || P->k >= P->o.kmax || P->k >= P->S) {
       // after S iterations Parareal equals the serial fine solve exactly
       P->state = Problem::DONE;
+      dirty_ = true;  // drop it from the launch classes
       if (finished) finished->push_back(i);
     }
   }

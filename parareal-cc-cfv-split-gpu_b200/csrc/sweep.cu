@@ -1086,14 +1086,16 @@ __global__ void __launch_bounds__(NTH, 3)
                         double toff, void *data_override, int lc_max, int H, unsigned *status,
                         int jstep, int nslice, const int *nlo, int cs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int rank = (int)(blockIdx.x % cs);
-  const int tile = (int)(blockIdx.x / cs) + group_base;
+  // CTA -> (field, tile of LPG lines, segment): every field carries its own
+  // first CTA, segments per line and halo, so fields of different line
+  // lengths share one launch (lc_max and H size the shared memory only)
+  const int cta = (int)blockIdx.x + group_base;
   FiltSmem<T> S = carve_filt<T>(smem_raw, lc_max, H);
   {
     int lo = 0, hi = nfields - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (__ldg(&fields[mid].group0) <= tile) lo = mid; else hi = mid - 1;
+      if (__ldg(&fields[mid].cta0) <= cta) lo = mid; else hi = mid - 1;
     }
     constexpr int NW8 = (int)(sizeof(SweepField) / 8);
     if (threadIdx.x < NW8)
@@ -1107,7 +1109,11 @@ __global__ void __launch_bounds__(NTH, 3)
   if (!field_active(F, jstep, nslice, nlo)) return;
   toff = field_time(F, toff, jstep, nslice);
   const int L = F.L;
-  const long long line0 = (long long)(tile - F.group0) * LPG;
+  cs = F.cs_f;
+  H = F.halo_f;
+  const int q = cta - F.cta0;
+  const int rank = q % cs;
+  const long long line0 = (long long)(q / cs) * LPG;
   const int Lc = (L + cs - 1) / cs;
   const int p0 = min(L, rank * Lc);
   const int p1 = min(L, p0 + Lc);
@@ -1324,10 +1330,11 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
     configured = true;
   }
   if (groups_total <= 0) return cudaSuccess;
-  if (filt) {  // independent CTAs: no cluster
+  if (filt) {  // independent CTAs: no cluster; group_base and the grid in CTAs
     count_launch();
     sweep_filter_kernel<T><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
-        d_fields, nfields, group_base, toff, data, lc_max, halo, d_status, jstep, nslice, nlo, cs);
+        d_fields, nfields, group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice, nlo,
+        cs);
     return cudaGetLastError();
   }
   cudaLaunchConfig_t cfg = {};
