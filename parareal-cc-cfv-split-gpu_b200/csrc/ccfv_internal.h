@@ -48,7 +48,7 @@ struct SweepField {
                          // same displacement): stencil fast path
   int jf;                // filter kernel: recurrence warm-up length J
   int cta0;              // filter kernel: first CTA of this field in the launch
-  int cs_f;              // filter kernel: CTAs (segments) per line of this field
+                         // (a multiple of the launch's cluster size)
   int halo_f;            // filter kernel: staged halo (cells) of this field
   // Batched launches (all zero for single-instance launches):
   int inst;              // instance index into the launch's `nlo` array

@@ -268,8 +268,10 @@ LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64
     if (filter_params(g, dir, Dt, fp64, nullptr, nullptr, &J) && L > 2 * J) {
       G.variant = SWEEP_FILTER;
       G.halo = J + sh + 6;
-      // independent CTAs: any number per line, segment length from the tuner
-      const int lc = std::max(32, std::min(L, filter_lc(L, fp64)));
+      // segment length from the tuner; the segments of a line form one
+      // cluster (at most MAX_CLUSTER CTAs)
+      const int lc = std::max({32, (L + MAX_CLUSTER - 1) / MAX_CLUSTER,
+                               std::min(L, filter_lc(L, fp64))});
       G.cs = (L + lc - 1) / lc;
       G.lc_max = (L + G.cs - 1) / G.cs;
     } else {
@@ -384,7 +386,6 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
       f.src_tb = kind == 2 ? 1 : 0;
       f.group0 = i * f.groups;
       f.cta0 = f.group0 * G.cs;
-      f.cs_f = G.cs;
       f.halo_f = G.halo;
       h[(size_t)kind * nf + i] = f;
       plan->groups_per_field[kind] = f.groups;

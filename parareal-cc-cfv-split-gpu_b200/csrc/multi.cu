@@ -147,33 +147,28 @@ __global__ void __launch_bounds__(BT)
 
 using KKey = std::tuple<int, int, int, int, int>;  // kind, variant, cs, lc bucket, fp64
 
-// Launch classes.  The filter kernel's CTAs are independent and every field
-// carries its own segment count and halo, so all filter fields of a sub-step
-// kind and precision share one class (one launch); the cluster kernels group
-// fields by cluster size and segment-length bucket.
+// Launch classes: fields of one sub-step kind, kernel variant, precision and
+// cluster size (segments per line).  Filter-kernel fields carry their own
+// segment length and halo, so they share a class across segment lengths; the
+// scan kernels also group by segment-length bucket.
 static void add_field(std::map<KKey, SweepClass> &classes, int kind, const ccfv_grid &g,
                       const SweepField &f0, bool fp64) {
   const LaunchGeom G = step_geom(g, f0.dir, f0.Dt, f0.dsrc, fp64);
   const bool filt = G.variant == SWEEP_FILTER;
   const int bucket = filt ? 0 : (G.lc_max + 63) / 64;  // segment-length bucket bounds the tile
-  SweepClass &K = classes[KKey{kind, G.variant, filt ? 0 : G.cs, bucket, fp64 ? 1 : 0}];
+  SweepClass &K = classes[KKey{kind, G.variant, G.cs, bucket, fp64 ? 1 : 0}];
   K.kind = kind;
   K.variant = G.variant;
-  K.cs = filt ? 1 : G.cs;  // filter classes count CTAs in `groups`
+  K.cs = G.cs;
   K.fp64 = fp64 ? 1 : 0;
   K.lc_max = std::max(K.lc_max, G.lc_max);
   K.halo = std::max(K.halo, G.halo);
   SweepField f = f0;
   f.group0 = K.groups;
-  f.cta0 = K.groups;
-  f.cs_f = G.cs;
+  f.cta0 = K.groups * G.cs;
   f.halo_f = G.halo;
-  if (filt) {
-    filter_field(g, f, fp64);
-    K.groups += f.groups * G.cs;
-  } else {
-    K.groups += f.groups;
-  }
+  if (filt) filter_field(g, f, fp64);
+  K.groups += f.groups;
   K.h.push_back(f);
 }
 

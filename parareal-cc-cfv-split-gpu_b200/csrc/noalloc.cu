@@ -182,7 +182,6 @@ extern "C" int ccfv_step_noalloc(const ccfv_grid *grid, double *d_C, double tn, 
     G.variant = g.source ? SWEEP_GENERAL_SRC
                 : (uniform && g.bc == CCFV_BC_PERIODIC && dsrc == 0) ? SWEEP_FAST : SWEEP_GENERAL;
     h_fields[kind].cta0 = 0;
-    h_fields[kind].cs_f = G.cs;
     h_fields[kind].halo_f = G.halo;
     if (std::max(sweep_smem_bytes(G.lc_max, G.halo, true, g.source != 0),
                  sweep_fast_smem_bytes(G.lc_max, G.halo, true)) > 227 * 1024)

@@ -1086,9 +1086,10 @@ __global__ void __launch_bounds__(NTH, 3)
                         double toff, void *data_override, int lc_max, int H, unsigned *status,
                         int jstep, int nslice, const int *nlo, int cs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  // CTA -> (field, tile of LPG lines, segment): every field carries its own
-  // first CTA, segments per line and halo, so fields of different line
-  // lengths share one launch (lc_max and H size the shared memory only)
+  // CTA -> (field, tile of LPG lines, segment).  The launch's clusters are the
+  // cs segments of one tile; fields carry their first CTA and halo, so fields
+  // of different segment lengths share one launch (lc_max and H size the
+  // shared memory only)
   const int cta = (int)blockIdx.x + group_base;
   FiltSmem<T> S = carve_filt<T>(smem_raw, lc_max, H);
   {
@@ -1109,7 +1110,6 @@ __global__ void __launch_bounds__(NTH, 3)
   if (!field_active(F, jstep, nslice, nlo)) return;
   toff = field_time(F, toff, jstep, nslice);
   const int L = F.L;
-  cs = F.cs_f;
   H = F.halo_f;
   const int q = cta - F.cta0;
   const int rank = q % cs;
@@ -1185,6 +1185,10 @@ __global__ void __launch_bounds__(NTH, 3)
   }
   cp_async_wait_all_committed();
   __syncthreads();
+  // The sweep is in place and the segments of a line are read (halo) by the
+  // neighbouring CTAs of its cluster: this CTA's reads are complete here, and
+  // no CTA of the cluster stores before every CTA has arrived.
+  if (cs > 1) asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
 
   const int ln = lane % LPG;
   const int c = warp * CPW + lane / LPG;
@@ -1245,6 +1249,7 @@ __global__ void __launch_bounds__(NTH, 3)
     }
   }
   __syncthreads();
+  if (cs > 1) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
   // ---- phase 3: backward filter x at p0 .. p1-1 (warm-up J cells) + store ----
   {
     const int m3 = (np + NCH - 1) / NCH;
@@ -1330,11 +1335,10 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
     configured = true;
   }
   if (groups_total <= 0) return cudaSuccess;
-  if (filt) {  // independent CTAs: no cluster; group_base and the grid in CTAs
+  if (filt && cs == 1) {  // whole lines per CTA: no cluster
     count_launch();
-    sweep_filter_kernel<T><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
-        d_fields, nfields, group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice, nlo,
-        cs);
+    sweep_filter_kernel<T><<<(unsigned)groups_total, NTH, smem, stream>>>(
+        d_fields, nfields, group_base, toff, data, lc_max, halo, d_status, jstep, nslice, nlo, 1);
     return cudaGetLastError();
   }
   cudaLaunchConfig_t cfg = {};
@@ -1350,6 +1354,9 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   count_launch();
+  if (filt)  // group_base in CTAs
+    return cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T>, d_fields, nfields, group_base * cs,
+                              toff, data, lc_max, halo, d_status, jstep, nslice, nlo, cs);
   if (fast)
     return cudaLaunchKernelEx(&cfg, sweep_fast_kernel<T>, d_fields, nfields, group_base, toff,
                               data, lc_max, halo, d_status, jstep, nslice, nlo);

@@ -153,7 +153,7 @@ def test_host_memory_run_matches_device(ccfv):
 
 
 @pytest.mark.parametrize("K", [1e-4, 1e-2, 0.5, 5.0])
-@pytest.mark.parametrize("nx", [64, 300, 1024])
+@pytest.mark.parametrize("nx", [64, 300, 1024, 2048])
 def test_periodic_solver_variants_match_oracle(oracle, ccfv, K, nx):
     """Weak diffusion takes the filter kernel (recurrences warmed up over
     J cells, |mu|^J below rounding), strong diffusion the exact chunked-scan
