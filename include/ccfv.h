@@ -219,7 +219,10 @@ int ccfv_batch_solve(int n, const ccfv_problem *problems, ccfv_stats *stats, int
 /* ---- serving ----------------------------------------------------------- */
 /* A request loop with continuous batching: requests of different sizes are
  * admitted in arrival order while their resident slice states fit
- * hbm_budget_bytes (and max_active, if > 0); every epoch all resident
+ * hbm_budget_bytes (and max_active, if > 0; a request of N^2 cells and S
+ * slices holds (3S + 4) N^2 doubles, plus (S + 1) N^2 in the standard form:
+ * U, F and the out-of-place partner of F, and two coarse work fields);
+ * every epoch all resident
  * requests advance by one Parareal iteration in shared launches, new
  * requests join at the next epoch boundary, finished ones return their result
  * to the caller's C_T and release their memory.  The caller keeps C0 / C_T

@@ -31,7 +31,9 @@ constexpr int MAX_CLUSTER = 16;  // non-portable cluster size (lines <= 4096)
 // x-sweep: lines are columns j (s_line = 1, s_pos = ny), positions i.
 // y-sweep: lines are rows i (s_line = ny, s_pos = 1), positions j.
 struct SweepField {
-  void *data;            // T[ny*nx], swept in place
+  void *data;            // T[ny*nx]: swept in place (pp = 0), or buffer A (pp = 1)
+  void *data2;           // pp = 1: buffer B
+  const void *in0;       // pp = 1: input of the first sweep of the sequence
   long long s_pos;       // element stride between positions of a line
   long long s_line;      // element stride between lines
   int L;                 // cells per line
@@ -56,6 +58,11 @@ struct SweepField {
   int jmax;              // the field takes part while jstep < jmax (0: always)
   int smax;              // slice-indexed fields: while slice < smax
   int gskip;             // slice-indexed fields: skip slice == nlo (zero increment)
+  int kind;              // sub-step of the split step: 0 x(dt/2), 1 y(dt), 2 x(dt/2)
+  int pp;                // 1: out-of-place sequence: sweep s = 3 jstep + kind writes A
+                         // when s + par is odd, else B, and reads the other buffer
+                         // (in0 for s = 0); 0: in place on `data`
+  int par;               // pp = 1: parity offset (chosen so the last sweep writes A)
   int phase;             // slice-indexed fields: 0 every launch, 1 only while the
                          // instance's nlo < 0 (first coarse sweep), 2 only while
                          // nlo >= 0 (Parareal iterations)
@@ -99,17 +106,22 @@ size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64);
 // sorted by group0; tiles group_base .. group_base+groups_total-1).  All fields share the cluster size `cs`, their
 // max positions per CTA `lc_max` and the halo `halo`.  `toff` is added to
 // every field's ta_rel/tb_rel (the launch time); `data` (if non-null)
-// replaces fields[0].data (single-field launches).
+// replaces fields[0].data (single-field launches).  `jstep` is the step of an
+// out-of-place sequence (SweepField::pp); `inplace` says whether any field
+// sweeps in place (the filter kernel's segments of a line then form a
+// cluster).
 template <typename T>
 cudaError_t launch_sweep(int variant, const SweepField *d_fields, int nfields, int group_base,
                          int groups_total, int cs, int lc_max, int halo, double toff, void *data,
-                         unsigned *d_status, cudaStream_t stream);
+                         unsigned *d_status, cudaStream_t stream, int jstep = 0,
+                         bool inplace = true);
 
 // Batched form: `jstep` / `nslice` select the step and slice of this launch,
 // `nlo[inst]` the first active slice of every instance (see SweepField).
 struct BatchStep {
   int jstep = 0, nslice = 0;
   const int *nlo = nullptr;
+  bool inplace = true;
 };
 template <typename T>
 cudaError_t launch_sweep_batch(int variant, const SweepField *d_fields, int nfields,

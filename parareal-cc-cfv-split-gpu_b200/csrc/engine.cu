@@ -287,8 +287,13 @@ int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen) 
   const ccfv_grid &g = ctx->grid;
   const size_t el = fp64 ? 8 : 4;
   const size_t NN = (size_t)g.nx * g.ny;
-  CK(ctx->io.alloc(el * NN));
-  CK(cudaMemsetAsync(ctx->io.p, 0, el * NN, st));
+  CK(ctx->io.alloc(2 * el * NN));
+  CK(cudaMemsetAsync(ctx->io.p, 0, 2 * el * NN, st));
+  // timed as the Parareal engines run it: out of place over a buffer pair
+  std::vector<PlanField> pf(1);
+  pf[0].A = ctx->io.p;
+  pf[0].B = static_cast<unsigned char *>(ctx->io.p) + el * NN;
+  pf[0].in0 = ctx->io.p;
   static const int cand[] = {64, 96, 128, 192, 256, 384, 512};
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
@@ -299,17 +304,16 @@ int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen) 
     if (lc > std::max(g.nx, g.ny) && lc != cand[0]) break;
     g_lc_override = lc;
     StepPlan plan;
-    std::vector<std::pair<void *, double>> f{{nullptr, 0.0}};
-    int rc = build_step_plan(ctx, &plan, dt, fp64, f);
+    int rc = build_step_plan(ctx, &plan, dt, fp64, pf);
     if (rc == CCFV_OK && plan.geom[0].variant != SWEEP_FILTER && plan.geom[1].variant != SWEEP_FILTER) {
       g_lc_override = 0;
       break;  // nothing to tune: this grid does not use the filter kernel
     }
-    if (rc == CCFV_OK) rc = run_step_plan(ctx, plan, fp64, 0, 1, 0.0, ctx->io.p, st);  // warm-up
+    if (rc == CCFV_OK) rc = run_step_plan(ctx, plan, fp64, 0, 1, 0.0, nullptr, st, 0);  // warm-up
     if (rc == CCFV_OK) {
       cudaEventRecord(a, st);
       for (int r = 0; r < 5 && rc == CCFV_OK; ++r)
-        rc = run_step_plan(ctx, plan, fp64, 0, 1, 0.0, ctx->io.p, st);
+        rc = run_step_plan(ctx, plan, fp64, 0, 1, 0.0, nullptr, st, r);
       cudaEventRecord(b, st);
       cudaEventSynchronize(b);
       float ms = 0;
@@ -359,6 +363,16 @@ static void sweep_kind(int kind, double dt, int *dir, double *Dt, double *ta, do
 
 int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
                     const std::vector<std::pair<void *, double>> &fields, bool homogeneous) {
+  std::vector<PlanField> pf(fields.size());
+  for (size_t i = 0; i < fields.size(); ++i) {
+    pf[i].A = fields[i].first;
+    pf[i].t0 = fields[i].second;
+  }
+  return build_step_plan(ctx, plan, dt, fp64, pf, homogeneous);
+}
+
+int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
+                    const std::vector<PlanField> &fields, bool homogeneous) {
   ccfv_grid g = ctx->grid;
   if (homogeneous) g.source = CCFV_SRC_NONE;
   const int nf = (int)fields.size();
@@ -380,8 +394,15 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
                   sweep_filter_smem_bytes(G.lc_max, G.halo, fp64)}) > 227 * 1024)
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
     for (int i = 0; i < nf; ++i) {
-      SweepField f = make_field(g, dir, Dt, ta + fields[i].second, tb + fields[i].second,
-                                fields[i].first, tab, dsrc);
+      const PlanField &pfi = fields[i];
+      SweepField f = make_field(g, dir, Dt, ta + pfi.t0, tb + pfi.t0, pfi.A, tab, dsrc);
+      f.kind = kind;
+      if (pfi.B) {
+        f.pp = 1;
+        f.data2 = pfi.B;
+        f.in0 = pfi.in0;
+        f.par = pfi.par;
+      }
       if (G.variant == SWEEP_FILTER) filter_field(g, f, fp64);
       f.src_tb = kind == 2 ? 1 : 0;
       f.group0 = i * f.groups;
@@ -393,13 +414,14 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
     plan->geom[kind] = G;
   }
   plan->nf = nf;
+  plan->pp = nf > 0 && fields[0].B != nullptr;
   CK(plan->fields.alloc(sizeof(SweepField) * h.size()));
   CK(cudaMemcpy(plan->fields.p, h.data(), sizeof(SweepField) * h.size(), cudaMemcpyHostToDevice));
   return CCFV_OK;
 }
 
 int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int count,
-                  double toff, void *data_override, cudaStream_t st) {
+                  double toff, void *data_override, cudaStream_t st, int jstep) {
   const SweepField *base = plan.fields.as<SweepField>();
   unsigned *status = ctx->status.as<unsigned>();
   for (int kind = 0; kind < 3; ++kind) {
@@ -408,9 +430,11 @@ int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int
     const SweepField *fk = base + (size_t)kind * plan.nf;
     cudaError_t e =
         fp64 ? launch_sweep<double>(G.variant, fk, plan.nf, first * gpf, count * gpf, G.cs,
-                                    G.lc_max, G.halo, toff, data_override, status, st)
+                                    G.lc_max, G.halo, toff, data_override, status, st, jstep,
+                                    !plan.pp)
              : launch_sweep<float>(G.variant, fk, plan.nf, first * gpf, count * gpf, G.cs,
-                                   G.lc_max, G.halo, toff, data_override, status, st);
+                                   G.lc_max, G.halo, toff, data_override, status, st, jstep,
+                                   !plan.pp);
     CK(e);
   }
   return CCFV_OK;
@@ -467,17 +491,19 @@ __device__ __forceinline__ double warp_sum(double v) {
 // U+[n+1] = F + G(e)        (DELTA)
 // fused with the update norms sum (U+ - U)^2 and sum U+^2, reduced
 // deterministically (fixed-order block partials, last block finishes).
-// STANDARD stores G into Gold; DELTA stores the new increment into W.
+// STANDARD stores G into Gold; DELTA stores the new increment into Wd.  G is
+// read from Wg (the buffer the coarse sweep sequence ended in; Wg may be Wd).
 template <typename TG>
 __global__ void __launch_bounds__(RED_THREADS)
     correction_kernel(int form, long long n, double *__restrict__ U, const double *__restrict__ Fv,
-                      double *__restrict__ Gold, TG *__restrict__ W, double *__restrict__ partial,
-                      unsigned *__restrict__ counter, double *__restrict__ out) {
+                      double *__restrict__ Gold, const TG *Wg, TG *Wd,
+                      double *__restrict__ partial, unsigned *__restrict__ counter,
+                      double *__restrict__ out) {
   double se = 0.0, su = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const double uo = U[i];
-    const double gw = (double)W[i];
+    const double gw = (double)Wg[i];
     double un;
     if (form == CCFV_FORM_STANDARD) {
       un = gw + (Fv[i] - Gold[i]);
@@ -487,7 +513,7 @@ __global__ void __launch_bounds__(RED_THREADS)
     }
     const double d = un - uo;
     U[i] = un;
-    if (form != CCFV_FORM_STANDARD) W[i] = (TG)d;
+    if (form != CCFV_FORM_STANDARD) Wd[i] = (TG)d;
     se += d * d;
     su += un * un;
   }
@@ -535,10 +561,10 @@ static int convert(ccfv_ctx *ctx, const S *src, D *dst, long long n, cudaStream_
 
 template <typename TG>
 static int correction(ccfv_ctx *ctx, int form, long long n, double *U, const double *Fv,
-                      double *Gold, TG *W, double *out, cudaStream_t st) {
+                      double *Gold, const TG *Wg, TG *Wd, double *out, cudaStream_t st) {
   count_launch();
   correction_kernel<TG><<<grid_for(n), RED_THREADS, 0, st>>>(
-      form, n, U, Fv, Gold, W, ctx->partial.as<double>(), ctx->counter.as<unsigned>(), out);
+      form, n, U, Fv, Gold, Wg, Wd, ctx->partial.as<double>(), ctx->counter.as<unsigned>(), out);
   CK(cudaGetLastError());
   return CCFV_OK;
 }
@@ -571,24 +597,36 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
   CK(ctx->U.alloc(fb * (S + 1)));
   CK(ctx->F.alloc(fb * (S + 1)));
   if (o->form == CCFV_FORM_STANDARD) CK(ctx->Gold.alloc(fb * (S + 1)));
+  CK(ctx->FS.alloc(fb * S));
   CK(ctx->W.alloc(sizeof(TG) * NN));
+  CK(ctx->W2.alloc(sizeof(TG) * NN));
   CK(ctx->norms.alloc(sizeof(double) * 2 * (S + 1)));
-  double *U = ctx->U.as<double>(), *F = ctx->F.as<double>();
+  double *U = ctx->U.as<double>(), *F = ctx->F.as<double>(), *FS = ctx->FS.as<double>();
   double *Gold = o->form == CCFV_FORM_STANDARD ? ctx->Gold.as<double>() : nullptr;
-  TG *W = ctx->W.as<TG>();
+  TG *W = ctx->W.as<TG>(), *W2 = ctx->W2.as<TG>();
   double *norms = ctx->norms.as<double>();
 
-  // fine plan over all slices: field n = F[n+1], time origin t0 + n*DT
+  // Fine plan over all slices, out of place: slice n's J steps run from U[n]
+  // through the pair F[n+1] / FS[n] and end in F[n+1] (no copy U -> F, no
+  // CTA reads what another CTA of its launch writes); time origin t0 + n DT.
   const double key[4] = {dt, o->t0, DT, (double)S};
+  const void *bufs[3] = {U, F, FS};
   if (!ctx->fine_plan || std::memcmp(key, ctx->fine_plan_key, sizeof(key)) != 0 ||
-      ctx->fine_plan_slices != S) {
+      ctx->fine_plan_slices != S || std::memcmp(bufs, ctx->fine_plan_bufs, sizeof(bufs)) != 0) {
     auto plan = std::make_unique<StepPlan>();
-    std::vector<std::pair<void *, double>> fl;
-    for (int n = 0; n < S; ++n) fl.push_back({F + (size_t)(n + 1) * NN, o->t0 + n * DT});
+    std::vector<PlanField> fl(S);
+    for (int n = 0; n < S; ++n) {
+      fl[n].A = F + (size_t)(n + 1) * NN;
+      fl[n].t0 = o->t0 + n * DT;
+      fl[n].B = FS + (size_t)n * NN;
+      fl[n].in0 = U + (size_t)n * NN;
+      fl[n].par = pp_parity(J);
+    }
     int rc = build_step_plan(ctx, plan.get(), dt, true, fl);
     if (rc) return rc;
     ctx->fine_plan = std::move(plan);
     std::memcpy(ctx->fine_plan_key, key, sizeof(key));
+    std::memcpy(ctx->fine_plan_bufs, bufs, sizeof(bufs));
     ctx->fine_plan_slices = S;
   }
   int status = CCFV_OK;
@@ -599,11 +637,23 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
   // next.  In the iterations FP32 rounding is relative to the increments.
   StepPlan *iplan = single_plan(ctx, dtc, true, &status);
   if (!iplan) return status;
-  StepPlan *cplan = single_plan(ctx, dtc, g64, &status);
-  if (!cplan) return status;
-  // the delta form propagates increments: the linear part of G (no source)
-  StepPlan *dplan = o->form == CCFV_FORM_DELTA ? single_plan(ctx, dtc, g64, &status, true) : cplan;
-  if (!dplan) return status;
+  // Coarse sweeps of the iterations: m steps out of place over W / W2,
+  // starting from W; the result is in W2 when 3m is odd.  The delta form
+  // propagates increments: the linear part of G (no source).
+  StepPlan cplan, hplan;
+  {
+    std::vector<PlanField> f(1);
+    f[0].A = W;
+    f[0].B = W2;
+    f[0].in0 = W;
+    int rc = build_step_plan(ctx, &cplan, dtc, g64, f);
+    if (!rc && o->form == CCFV_FORM_DELTA && g.source != CCFV_SRC_NONE)
+      rc = build_step_plan(ctx, &hplan, dtc, g64, f, true);
+    if (rc) return rc;
+  }
+  const StepPlan *dplan =
+      (o->form == CCFV_FORM_DELTA && g.source != CCFV_SRC_NONE) ? &hplan : &cplan;
+  const TG *Wres = ((3 * m) & 1) ? W2 : W;
 
   cudaEvent_t ev0, ev1;
   CK(cudaEventCreate(&ev0));
@@ -614,7 +664,7 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
 
   auto coarse_on_W = [&](int n, const StepPlan *plan) -> int {
     for (int i = 0; i < m; ++i) {
-      int rc = run_step_plan(ctx, *plan, g64, 0, 1, o->t0 + n * DT + i * dtc, W, st);
+      int rc = run_step_plan(ctx, *plan, g64, 0, 1, o->t0 + n * DT + i * dtc, nullptr, st, i);
       if (rc) return rc;
     }
     return CCFV_OK;
@@ -643,12 +693,10 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
   for (int k = 1; k <= o->kmax; ++k) {
     const int nlo = k - 1;
     const int act = S - nlo;
-    // F-phase
-    CK(cudaMemcpyAsync(F + (size_t)(nlo + 1) * NN, U + (size_t)nlo * NN, fb * act,
-                       cudaMemcpyDeviceToDevice, st));
+    // F-phase: F[n+1] = F(U[n]) for every active slice, out of place
     CK(cudaEventRecord(fa, st));
     for (int j = 0; j < J; ++j) {
-      int rc = run_step_plan(ctx, *ctx->fine_plan, true, nlo, act, j * dt, nullptr, st);
+      int rc = run_step_plan(ctx, *ctx->fine_plan, true, nlo, act, j * dt, nullptr, st, j);
       if (rc) return rc;
     }
     CK(cudaEventRecord(fb_, st));
@@ -659,19 +707,21 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
     CK(cudaMemsetAsync(norms, 0, sizeof(double) * 2 * (S + 1), st));
     for (int n = nlo; n < S; ++n) {
       int rc;
+      const TG *Gn = Wres;  // where this slice's G value ends up
       if (o->form == CCFV_FORM_STANDARD) {
         CK(cudaMemcpyAsync(W, U + (size_t)n * NN, fb, cudaMemcpyDeviceToDevice, st));
-        if ((rc = coarse_on_W(n, cplan))) return rc;
+        if ((rc = coarse_on_W(n, &cplan))) return rc;
         coarse_cu += (double)m * NN;
       } else if (n == nlo) {
         CK(cudaMemsetAsync(W, 0, sizeof(TG) * NN, st));  // G(0) = 0
+        Gn = W;
       } else {
         if ((rc = coarse_on_W(n, dplan))) return rc;
         coarse_cu += (double)m * NN;
       }
       if ((rc = correction<TG>(ctx, o->form, NN, U + (size_t)(n + 1) * NN,
                                F + (size_t)(n + 1) * NN,
-                               Gold ? Gold + (size_t)(n + 1) * NN : nullptr, W,
+                               Gold ? Gold + (size_t)(n + 1) * NN : nullptr, Gn, W,
                                norms + 2 * (n + 1), st)))
         return rc;
     }
@@ -778,7 +828,7 @@ int correct(ccfv_ctx *ctx, int form, double *U, const double *Fv, double *Gold, 
             double *sq_update, double *sq_state, cudaStream_t st) {
   const long long NN = (long long)ctx->grid.nx * ctx->grid.ny;
   double *out = ctx->aux.as<double>() + 8;
-  int rc = correction<double>(ctx, form, NN, U, Fv, Gold, W, out, st);
+  int rc = correction<double>(ctx, form, NN, U, Fv, Gold, W, W, out, st);
   if (rc) return rc;
   double h[2];
   CK(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, st));

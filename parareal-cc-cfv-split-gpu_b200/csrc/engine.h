@@ -44,7 +44,22 @@ struct StepPlan {
   int nf = 0;
   int groups_per_field[3] = {0, 0, 0};
   LaunchGeom geom[3];
+  bool pp = false;        // out-of-place sequence (SweepField::pp)
 };
+
+// One field of a plan: swept in place on A (B == nullptr), or an out-of-place
+// sequence of steps over the pair A/B that starts from in0 and, with parity
+// offset par, ends in A (SweepField::pp).  t0: the field's time origin.
+struct PlanField {
+  void *A = nullptr;
+  double t0 = 0.0;
+  void *B = nullptr;
+  const void *in0 = nullptr;
+  int par = 0;
+};
+// Parity offset that makes a sequence of `steps` split steps (3 sweeps each)
+// end in buffer A.
+inline int pp_parity(int steps) { return (3 * steps) & 1; }
 
 }  // namespace ccfv
 
@@ -56,9 +71,11 @@ struct ccfv_ctx {
   std::map<std::tuple<double, int, int>, std::unique_ptr<ccfv::StepPlan>> step_plans;
   // Parareal slice states and scratch
   ccfv::DevBuf U, F, Gold, W, C64, C32, norms, partial, counter, io, aux;
+  ccfv::DevBuf FS, W2;  // ping-pong partners of the fine slices and the coarse work field
   size_t slices_cap = 0;
   std::unique_ptr<ccfv::StepPlan> fine_plan;
   double fine_plan_key[4] = {0, 0, 0, 0};
+  const void *fine_plan_bufs[3] = {nullptr, nullptr, nullptr};
   int fine_plan_slices = 0;
   std::string last_error;
   bool force_general = false;  // test hook: route every sweep through the per-cell kernel
@@ -80,8 +97,11 @@ int batch_solve(int n, const ccfv_problem *probs, ccfv_stats *stats, int device,
 int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
                     const std::vector<std::pair<void *, double>> &fields,
                     bool homogeneous = false);
+int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
+                    const std::vector<PlanField> &fields, bool homogeneous = false);
+// jstep: the step's index in an out-of-place sequence (selects the buffers).
 int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int count,
-                  double toff, void *data_override, cudaStream_t st);
+                  double toff, void *data_override, cudaStream_t st, int jstep = 0);
 int steps(ccfv_ctx *ctx, void *d_C, bool fp64, double t0, double dt, int nsteps, cudaStream_t st);
 int coarse_fp32(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, cudaStream_t st);
 int fine_slices(ccfv_ctx *ctx, double *d_fields, int n, double t0, double slice_dt, double DT,

@@ -25,19 +25,20 @@ namespace {
 // Per-instance element-wise work of one batched launch.
 struct BElem {
   double *U, *F, *Gold;
-  void *W;
+  void *W;        // coarse input (first sweep: FP64 state; iterations: increment)
+  void *Wres;     // where the coarse sweep sequence ends (W or its partner)
   long long NN;
   int S, form, g64, pad;
   double *norms;  // [2*(S+1)]
 };
 
-enum { OP_LOAD_W = 0, OP_STORE_W = 1, OP_COPY_F = 2, OP_CORRECT = 3, OP_LOAD_W_STD = 4 };
+enum { OP_LOAD_W = 0, OP_STORE_W = 1, OP_CORRECT = 3, OP_LOAD_W_STD = 4 };
 
 constexpr int BT = 256;
 
 __device__ __forceinline__ double wload(const BElem &b, long long i) {
-  return b.g64 ? reinterpret_cast<const double *>(b.W)[i]
-               : (double)reinterpret_cast<const float *>(b.W)[i];
+  return b.g64 ? reinterpret_cast<const double *>(b.Wres)[i]
+               : (double)reinterpret_cast<const float *>(b.Wres)[i];
 }
 __device__ __forceinline__ void wstore(const BElem &b, long long i, double v) {
   if (b.g64) reinterpret_cast<double *>(b.W)[i] = v;
@@ -52,7 +53,7 @@ __global__ void __launch_bounds__(BT)
   const int inst = blockIdx.y;
   const BElem b = d[inst];
   const int lo = nlo[inst];
-  long long n0 = 0, cnt = b.NN;
+  const long long cnt = b.NN;
   if (op == OP_LOAD_W_STD) {  // G-phase: only the standard form restarts G from U
     if (b.form != CCFV_FORM_STANDARD) return;
     op = OP_LOAD_W;
@@ -62,11 +63,6 @@ __global__ void __launch_bounds__(BT)
     case OP_STORE_W:
     case OP_CORRECT:
       if (n >= b.S || n < lo) return;
-      break;
-    case OP_COPY_F:  // F[m+1] <- U[m] for every active slice m >= lo
-      if (lo >= b.S) return;
-      n0 = (long long)lo * b.NN;
-      cnt = (long long)(b.S - lo) * b.NN;
       break;
   }
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -79,21 +75,19 @@ __global__ void __launch_bounds__(BT)
   } else if (op == OP_STORE_W) {
     double *dst = b.U + (long long)(n + 1) * b.NN;
     double *gd = b.Gold ? b.Gold + (long long)(n + 1) * b.NN : nullptr;
-    const double *w = reinterpret_cast<const double *>(b.W);
+    const double *w = reinterpret_cast<const double *>(b.Wres);
     for (long long i = first; i < cnt; i += stride) {
       const double v = w[i];
       dst[i] = v;
       if (gd) gd[i] = v;
     }
-  } else if (op == OP_COPY_F) {
-    const double *src = b.U + n0;
-    double *dst = b.F + n0 + b.NN;
-    for (long long i = first; i < cnt; i += stride) dst[i] = src[i];
   } else {
     double *U = b.U + (long long)(n + 1) * b.NN;
     const double *Fv = b.F + (long long)(n + 1) * b.NN;
     double *Go = b.Gold ? b.Gold + (long long)(n + 1) * b.NN : nullptr;
     const bool zero_g = (b.form == CCFV_FORM_DELTA && n == lo);  // G(0) = 0
+    // G is read from Wres; the new increment goes to W (elementwise, so the
+    // two may be the same buffer)
     for (long long i = first; i < cnt; i += stride) {
       const double uo = U[i];
       const double gw = zero_g ? 0.0 : wload(b, i);
@@ -177,7 +171,9 @@ size_t problem_bytes(const ccfv_grid &g, const ccfv_parareal_opts &o) {
   const size_t S = (size_t)std::max(o.n_slices, 1);
   const bool g64 = o.coarse_precision != CCFV_FP32;
   (void)g64;  // W holds FP64 states in the first coarse sweep whatever the coarse precision
-  return fb * (S + 1) * 2 + (o.form == CCFV_FORM_STANDARD ? fb * (S + 1) : 0) + fb + 4 * 256;
+  // U, F and F's ping-pong partner, Gold (standard form), W and its partner
+  return fb * (S + 1) * 2 + fb * S + (o.form == CCFV_FORM_STANDARD ? fb * (S + 1) : 0) + 2 * fb +
+         6 * 256;
 }
 
 int problem_setup(Problem &P, const ccfv_problem &p, std::string *err) {
@@ -266,8 +262,10 @@ int MultiEngine::add(const ccfv_problem &pr, int *slot) {
   const size_t fb = sizeof(double) * P->NN;
   P->U = reinterpret_cast<double *>(take(fb * (P->S + 1)));
   P->F = reinterpret_cast<double *>(take(fb * (P->S + 1)));
+  P->FS = reinterpret_cast<double *>(take(fb * P->S));
   P->Gold = P->o.form == CCFV_FORM_STANDARD ? reinterpret_cast<double *>(take(fb * (P->S + 1))) : nullptr;
   P->W = take(fb);
+  P->W2 = take(fb);
   MCK(cudaMemcpyAsync(P->U, P->C0, fb,
                       P->o.mem == CCFV_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st_));
   int s = -1;
@@ -326,8 +324,9 @@ int MultiEngine::rebuild() {
     Problem *P = slots_[i].get();
     if (!live(P)) continue;
     const ccfv_grid &g = P->g;
-    he[i] = BElem{P->U, P->F, P->Gold, P->W, P->NN, P->S, P->o.form, P->g64 ? 1 : 0, 0,
-                  norms_d_.as<double>() + norm_off_[i]};
+    // coarse sequences start in W and end in W2 when 3m is odd
+    he[i] = BElem{P->U, P->F, P->Gold, P->W, ((3 * P->m) & 1) ? P->W2 : P->W, P->NN, P->S,
+                  P->o.form, P->g64 ? 1 : 0, 0, norms_d_.as<double>() + norm_off_[i]};
     for (int kind = 0; kind < 3; ++kind) {
       const int dir = kind == 1 ? 1 : 0;
       const int dsrc = (kind == 2 && g.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
@@ -342,6 +341,12 @@ int MultiEngine::rebuild() {
           f.src_tb = kind == 2 ? 1 : 0;
           f.jmax = P->J;
           f.t_step = P->dt;
+          // out of place: U[s] -> ... -> F[s+1] through the pair F[s+1] / FS[s]
+          f.kind = kind;
+          f.pp = 1;
+          f.data2 = P->FS + (size_t)s * P->NN;
+          f.in0 = P->U + (size_t)s * P->NN;
+          f.par = pp_parity(P->J);
           add_field(fine_, kind, g, f, true);
         }
       }
@@ -359,6 +364,11 @@ int MultiEngine::rebuild() {
           f.t_slice = P->DT;
           f.phase = phase;
           f.src_tb = kind == 2 ? 1 : 0;
+          f.kind = kind;
+          f.pp = 1;  // W -> ... -> W or W2 through the pair W / W2
+          f.data2 = P->W2;
+          f.in0 = P->W;
+          f.par = 0;
           return f;
         };
         const bool delta_src = g.source != CCFV_SRC_NONE && P->o.form == CCFV_FORM_DELTA;
@@ -422,6 +432,7 @@ int MultiEngine::sweeps(std::map<KKey, SweepClass> &classes, int kind, int jstep
   bs.jstep = jstep;
   bs.nslice = nslice;
   bs.nlo = nlo_d_.as<int>();
+  bs.inplace = false;  // every batched field sweeps out of place
   unsigned *status = status_.as<unsigned>();
   for (auto &kv : classes) {
     SweepClass &K = kv.second;
@@ -499,7 +510,7 @@ int MultiEngine::iterate(std::vector<int> *finished) {
   }
   if (running) {
     if (int rc = push_nlo()) return rc;
-    if (int rc = elem(OP_COPY_F, 0)) return rc;
+    // F[s+1] = F(U[s]): the fine sequences read U[s] in their first sweep
     for (int j = 0; j < Jmax; ++j)
       for (int kind = 0; kind < 3; ++kind)
         if (int rc = sweeps(fine_, kind, j, 0)) return rc;

@@ -23,10 +23,11 @@ struct Problem {
   double DT = 0, dt = 0, dtc = 0;
   long long NN = 0;
   bool g64 = true;
-  void *mem = nullptr;       // cudaMallocAsync arena: U, F, Gold, W
+  void *mem = nullptr;       // cudaMallocAsync arena: U, F, FS, Gold, W, W2
   size_t bytes = 0;
   double *U = nullptr, *F = nullptr, *Gold = nullptr;
-  void *W = nullptr;
+  double *FS = nullptr;      // ping-pong partner of F[1..S] (out-of-place fine sweeps)
+  void *W = nullptr, *W2 = nullptr;  // coarse work field and its ping-pong partner
   std::unique_ptr<ccfv_ctx> ctx;  // owns the solver tables of this grid
   // fine x, fine y, coarse x, coarse y (coarse precision), coarse x, y in
   // FP64 (the first coarse sweep, which always runs in FP64)

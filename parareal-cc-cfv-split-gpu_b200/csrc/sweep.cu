@@ -93,6 +93,22 @@ __device__ __forceinline__ double field_time(const SweepField &f, double toff, i
   return toff + jstep * f.t_step + (f.slice < 0 ? nslice * f.t_slice : 0.0);
 }
 
+// Input and output of a field in a launch (SweepField::pp): in place, or the
+// ping-pong pair of an out-of-place sweep sequence.  Out of place, no CTA
+// reads what another CTA of the launch writes.
+__device__ __forceinline__ void field_io(const SweepField &f, int jstep, const void **src,
+                                         void **dst) {
+  if (!f.pp) {
+    *src = f.data;
+    *dst = f.data;
+    return;
+  }
+  const int s = 3 * jstep + f.kind;
+  const bool toA = ((s + f.par) & 1) != 0;
+  *dst = toA ? f.data : f.data2;
+  *src = s == 0 ? f.in0 : (toA ? f.data2 : f.data);
+}
+
 // Bounds-checked view of one line in the shared tile, indexed by position.
 template <typename T>
 struct LineView {
@@ -347,7 +363,15 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
   const int np = p1 - p0;
   const int nrows = np + 2 * H;
   const bool periodic = F.bc == BC_PERIODIC;
-  T *gdata = reinterpret_cast<T *>(F.data);
+  const T *gsrc;
+  T *gdst;
+  {
+    const void *vs;
+    void *vd;
+    field_io(F, jstep, &vs, &vd);
+    gsrc = reinterpret_cast<const T *>(vs);
+    gdst = reinterpret_cast<T *>(vd);
+  }
 
   // ---- phase 0: stage the tile (+halo) and the solver factors ----
   {
@@ -366,7 +390,7 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
           if (periodic) { pos %= L; if (pos < 0) pos += L; }
           else ok = false;
         }
-        if (ok) val = gdata[(long long)pos * F.s_pos + gl * F.s_line];
+        if (ok) val = gsrc[(long long)pos * F.s_pos + gl * F.s_line];
       }
       S.C[row * PITCH + ln] = val;
     }
@@ -693,7 +717,7 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
       else { l2 = q / np; row = q - l2 * np; }
       long long gl2 = line0 + l2;
       if (gl2 < F.M)
-        gdata[(long long)(p0 + row) * F.s_pos + gl2 * F.s_line] = qArr[(row + H) * PITCH + l2];
+        gdst[(long long)(p0 + row) * F.s_pos + gl2 * F.s_line] = qArr[(row + H) * PITCH + l2];
     }
   }
   if (cs > 1) cluster.sync();  // keep shared memory alive for remote readers
@@ -804,9 +828,18 @@ __global__ void __launch_bounds__(NTH, 2)
   const int nrows = np + 2 * H;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
+  const T *gsrc;
+  T *gdst;
+  {
+    const void *vs;
+    void *vd;
+    field_io(F, jstep, &vs, &vd);
+    gsrc = reinterpret_cast<const T *>(vs);
+    gdst = reinterpret_cast<T *>(vd);
+  }
   // ---- stage the tile (cp.async, no integer division) ----
   {
-    const T *gdata = reinterpret_cast<const T *>(F.data);
+    const T *gdata = gsrc;
     if (F.s_line == 1) {
       // x-sweep: a warp copies two rows of 16 consecutive doubles per step
       const int ln = lane & (LPG - 1);
@@ -1017,7 +1050,7 @@ __global__ void __launch_bounds__(NTH, 2)
     }
   }
   // ---- backward fix-up + correction + store ----
-  T *gdata = reinterpret_cast<T *>(F.data);
+  T *gdata = gdst;
   {
     const int n = e - s;
     T *qp = S.Q + (s - p0) * PITCH + ln;
@@ -1084,7 +1117,7 @@ template <typename T>
 __global__ void __launch_bounds__(NTH, 3)
     sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
                         double toff, void *data_override, int lc_max, int H, unsigned *status,
-                        int jstep, int nslice, const int *nlo, int cs) {
+                        int jstep, int nslice, const int *nlo, int cs, int clustered) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // CTA -> (field, tile of LPG lines, segment).  The launch's clusters are the
   // cs segments of one tile; fields carry their first CTA and halo, so fields
@@ -1122,7 +1155,15 @@ __global__ void __launch_bounds__(NTH, 3)
   const int J = F.jf;
   const T mu = T(F.sm_fac), ic = T(F.sm_inv_den);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  T *gdata = reinterpret_cast<T *>(F.data);
+  const T *gsrc;
+  T *gdata;  // output
+  {
+    const void *vs;
+    void *vd;
+    field_io(F, jstep, &vs, &vd);
+    gsrc = reinterpret_cast<const T *>(vs);
+    gdata = reinterpret_cast<T *>(vd);
+  }
 
   // ---- stage rows p0-H .. p1+H-1 (periodic wrap) ----
   if (F.s_line == 1) {
@@ -1134,7 +1175,7 @@ __global__ void __launch_bounds__(NTH, 3)
       if (pos < 0 || pos >= L) { pos %= L; if (pos < 0) pos += L; }
       T *dst = S.C + row * PITCH + ln;
       if (okl) {
-        const T *src = gdata + (long long)pos * F.s_pos + gl;
+        const T *src = gsrc + (long long)pos * F.s_pos + gl;
         if (sizeof(T) == 8) cp_async8(dst, src); else cp_async4(dst, src);
       } else {
         *dst = T(0);
@@ -1144,7 +1185,7 @@ __global__ void __launch_bounds__(NTH, 3)
     for (int ln = warp; ln < LPG; ln += NW) {
       const long long gl = line0 + ln;
       const bool okl = gl < F.M;
-      const T *lbase = gdata + gl * F.s_line;
+      const T *lbase = gsrc + gl * F.s_line;
       for (int row = lane; row < nrows; row += 32) {
         int pos = p0 - H + row;
         if (pos < 0 || pos >= L) { pos %= L; if (pos < 0) pos += L; }
@@ -1185,10 +1226,11 @@ __global__ void __launch_bounds__(NTH, 3)
   }
   cp_async_wait_all_committed();
   __syncthreads();
-  // The sweep is in place and the segments of a line are read (halo) by the
-  // neighbouring CTAs of its cluster: this CTA's reads are complete here, and
-  // no CTA of the cluster stores before every CTA has arrived.
-  if (cs > 1) asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+  // In place, the segments of a line are read (halo) by the neighbouring CTAs
+  // of its cluster: this CTA's reads are complete here, and no CTA of the
+  // cluster stores before every CTA has arrived.  Out of place (ping-pong),
+  // the launch has no clusters and needs no barrier.
+  if (clustered) asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
 
   const int ln = lane % LPG;
   const int c = warp * CPW + lane / LPG;
@@ -1249,7 +1291,7 @@ __global__ void __launch_bounds__(NTH, 3)
     }
   }
   __syncthreads();
-  if (cs > 1) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
+  if (clustered) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
   // ---- phase 3: backward filter x at p0 .. p1-1 (warm-up J cells) + store ----
   {
     const int m3 = (np + NCH - 1) / NCH;
@@ -1315,7 +1357,7 @@ template <typename T>
 static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfields,
                                int group_base, int groups_total, int cs, int lc_max, int halo,
                                double toff, void *data, unsigned *d_status, int jstep,
-                               int nslice, const int *nlo, cudaStream_t stream) {
+                               int nslice, const int *nlo, bool inplace, cudaStream_t stream) {
   const bool fast = (variant == SWEEP_FAST);
   const bool filt = (variant == SWEEP_FILTER);
   const bool src = (variant == SWEEP_GENERAL_SRC);
@@ -1335,10 +1377,11 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
     configured = true;
   }
   if (groups_total <= 0) return cudaSuccess;
-  if (filt && cs == 1) {  // whole lines per CTA: no cluster
+  if (filt && (cs == 1 || !inplace)) {  // whole lines per CTA, or out of place: no cluster
     count_launch();
-    sweep_filter_kernel<T><<<(unsigned)groups_total, NTH, smem, stream>>>(
-        d_fields, nfields, group_base, toff, data, lc_max, halo, d_status, jstep, nslice, nlo, 1);
+    sweep_filter_kernel<T><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
+        d_fields, nfields, group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
+        nlo, cs, 0);
     return cudaGetLastError();
   }
   cudaLaunchConfig_t cfg = {};
@@ -1356,7 +1399,7 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   count_launch();
   if (filt)  // group_base in CTAs
     return cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T>, d_fields, nfields, group_base * cs,
-                              toff, data, lc_max, halo, d_status, jstep, nslice, nlo, cs);
+                              toff, data, lc_max, halo, d_status, jstep, nslice, nlo, cs, 1);
   if (fast)
     return cudaLaunchKernelEx(&cfg, sweep_fast_kernel<T>, d_fields, nfields, group_base, toff,
                               data, lc_max, halo, d_status, jstep, nslice, nlo);
@@ -1367,9 +1410,9 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
 template <typename T>
 cudaError_t launch_sweep(int variant, const SweepField *d_fields, int nfields, int group_base,
                          int groups_total, int cs, int lc_max, int halo, double toff, void *data,
-                         unsigned *d_status, cudaStream_t stream) {
+                         unsigned *d_status, cudaStream_t stream, int jstep, bool inplace) {
   return launch_impl<T>(variant, d_fields, nfields, group_base, groups_total, cs, lc_max, halo,
-                        toff, data, d_status, 0, 0, nullptr, stream);
+                        toff, data, d_status, jstep, 0, nullptr, inplace, stream);
 }
 
 template <typename T>
@@ -1377,13 +1420,13 @@ cudaError_t launch_sweep_batch(int variant, const SweepField *d_fields, int nfie
                                int group_base, int groups_total, int cs, int lc_max, int halo,
                                const BatchStep &bs, unsigned *d_status, cudaStream_t stream) {
   return launch_impl<T>(variant, d_fields, nfields, group_base, groups_total, cs, lc_max, halo,
-                        0.0, nullptr, d_status, bs.jstep, bs.nslice, bs.nlo, stream);
+                        0.0, nullptr, d_status, bs.jstep, bs.nslice, bs.nlo, bs.inplace, stream);
 }
 
 template cudaError_t launch_sweep<double>(int, const SweepField *, int, int, int, int, int, int,
-                                          double, void *, unsigned *, cudaStream_t);
+                                          double, void *, unsigned *, cudaStream_t, int, bool);
 template cudaError_t launch_sweep<float>(int, const SweepField *, int, int, int, int, int, int,
-                                         double, void *, unsigned *, cudaStream_t);
+                                         double, void *, unsigned *, cudaStream_t, int, bool);
 template cudaError_t launch_sweep_batch<double>(int, const SweepField *, int, int, int, int, int,
                                                 int, const BatchStep &, unsigned *, cudaStream_t);
 template cudaError_t launch_sweep_batch<float>(int, const SweepField *, int, int, int, int, int,

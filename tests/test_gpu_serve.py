@@ -65,9 +65,10 @@ def test_server_results_equal_alone_and_late_arrivals_overlap(ccfv):
 
 def test_server_budget_admission_and_rejection(ccfv):
     small = _req(ccfv, 64, 1, (1.0, 0.5), 1e-3, 1)
-    # slice states U and F plus the coarse work field, which holds FP64 states
-    # during the first coarse sweep whatever the coarse precision
-    need = (2 * (small["n_slices"] + 1) * 64 * 64 + 64 * 64) * 8 + 4096
+    # slice states U and F, F's out-of-place partner (S fields), and the coarse
+    # work field and its partner (FP64-sized: the first coarse sweep is FP64)
+    S = small["n_slices"]
+    need = (2 * (S + 1) + S + 2) * 64 * 64 * 8 + 4096
     srv = ccfv.Server(hbm_budget_bytes=need)  # room for exactly one resident request
     try:
         big = _req(ccfv, 256, 1, (1.0, 0.5), 1e-3, 2)
