@@ -101,6 +101,9 @@ constexpr int FILTER_JMAX = 64;  // longest recurrence warm-up of the filter ker
 size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source = false);
 size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64);
 size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64);
+// Longest segment (cells per CTA along a line) of the filter kernel for a
+// recurrence warm-up of J cells.
+int filter_segment_max(int J);
 
 // Launches one fused sweep over all fields of `d_fields` (device array,
 // sorted by group0; tiles group_base .. group_base+groups_total-1).  All fields share the cluster size `cs`, their

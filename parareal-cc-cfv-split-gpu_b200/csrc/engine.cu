@@ -253,7 +253,7 @@ int filter_lc(int L, bool fp64) {
   return it == g_filter_lc.end() ? LC_MAX : it->second;
 }
 
-LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64) {
+LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64, bool inplace) {
   LaunchGeom G;
   const int L = dir == 0 ? g.nx : g.ny;
   G.cs = (L + LC_MAX - 1) / LC_MAX;
@@ -270,10 +270,18 @@ LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64
       G.halo = J + sh + 6;
       // segment length from the tuner; the segments of a line form one
       // cluster (at most MAX_CLUSTER CTAs)
-      const int lc = std::max({32, (L + MAX_CLUSTER - 1) / MAX_CLUSTER,
-                               std::min(L, filter_lc(L, fp64))});
+      const int lc = std::min(filter_segment_max(J),
+                              std::max({32, (L + MAX_CLUSTER - 1) / MAX_CLUSTER,
+                                        std::min(L, filter_lc(L, fp64))}));
       G.cs = (L + lc - 1) / lc;
       G.lc_max = (L + G.cs - 1) / G.cs;
+      if (inplace && G.cs > MAX_CLUSTER) {  // in place, a line's segments form one cluster
+        G = LaunchGeom();
+        G.cs = (L + LC_MAX - 1) / LC_MAX;
+        G.lc_max = (L + G.cs - 1) / G.cs;
+        G.halo = sh + 5;
+        G.variant = SWEEP_FAST;
+      }
     } else {
       G.variant = SWEEP_FAST;
     }
@@ -385,9 +393,10 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
     int st = CCFV_OK;
     const SolverTable *tab = get_table(ctx, dir, Dt, fp64, &st);
     if (!tab) return st;
-    LaunchGeom G = step_geom(g, dir, Dt, dsrc, fp64);
+    const bool plan_pp = !fields.empty() && fields[0].B != nullptr;
+    LaunchGeom G = step_geom(g, dir, Dt, dsrc, fp64, !plan_pp);
     if (ctx->force_general && G.variant != SWEEP_GENERAL_SRC) G.variant = SWEEP_GENERAL;
-    if (G.cs > MAX_CLUSTER)
+    if (G.cs > MAX_CLUSTER && !(G.variant == SWEEP_FILTER && plan_pp))
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
     if (std::max({sweep_smem_bytes(G.lc_max, G.halo, fp64, g.source != 0),
                   sweep_fast_smem_bytes(G.lc_max, G.halo, fp64),

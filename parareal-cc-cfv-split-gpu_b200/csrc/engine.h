@@ -87,7 +87,10 @@ int set_error(ccfv_ctx *ctx, int code, const std::string &msg);
 const SolverTable *get_table(ccfv_ctx *ctx, int dir, double Dt, bool fp64, int *status);
 SweepField make_field(const ccfv_grid &g, int dir, double Dt, double ta_rel, double tb_rel,
                       void *data, const SolverTable *tab, int dsrc);
-LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64);
+// inplace: the sweep overwrites its input (the filter kernel's segments of a
+// line then form one cluster, at most MAX_CLUSTER CTAs).
+LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64,
+                     bool inplace = true);
 void filter_field(const ccfv_grid &g, SweepField &f, bool fp64);
 int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen);
 int batch_solve(int n, const ccfv_problem *probs, ccfv_stats *stats, int device,

@@ -147,7 +147,7 @@ using KKey = std::tuple<int, int, int, int, int>;  // kind, variant, cs, lc buck
 // scan kernels also group by segment-length bucket.
 static void add_field(std::map<KKey, SweepClass> &classes, int kind, const ccfv_grid &g,
                       const SweepField &f0, bool fp64) {
-  const LaunchGeom G = step_geom(g, f0.dir, f0.Dt, f0.dsrc, fp64);
+  const LaunchGeom G = step_geom(g, f0.dir, f0.Dt, f0.dsrc, fp64, /*inplace=*/false);
   const bool filt = G.variant == SWEEP_FILTER;
   const int bucket = filt ? 0 : (G.lc_max + 63) / 64;  // segment-length bucket bounds the tile
   SweepClass &K = classes[KKey{kind, G.variant, G.cs, bucket, fp64 ? 1 : 0}];
@@ -245,8 +245,9 @@ int MultiEngine::add(const ccfv_problem &pr, int *slot) {
       const int dir = kind == 1 ? 1 : 0;
       const double Dt = (level == 0 ? P->dt : P->dtc) * (dir == 0 ? 0.5 : 1.0);
       const int dsrc = (kind == 2 && P->g.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
-      const LaunchGeom G = step_geom(P->g, dir, Dt, dsrc, level == 0 || P->g64);
-      if (G.cs > MAX_CLUSTER) return fail(CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
+      const LaunchGeom G = step_geom(P->g, dir, Dt, dsrc, level == 0 || P->g64, false);
+      if (G.variant != SWEEP_FILTER && G.cs > MAX_CLUSTER)
+        return fail(CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
       if (std::max({sweep_smem_bytes(G.lc_max, G.halo, true, P->g.source != 0),
                     sweep_fast_smem_bytes(G.lc_max, G.halo, true),
                     sweep_filter_smem_bytes(G.lc_max, G.halo, true)}) > 227 * 1024)

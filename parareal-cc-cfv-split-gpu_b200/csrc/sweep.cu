@@ -1087,15 +1087,25 @@ __global__ void __launch_bounds__(NTH, 2)
 //   w_k = r_k / c - mu w_{k-1},   x_k = w_k - mu x_{k+1},
 // whose periodic wrap-around needs no correction term.  A recurrence started
 // from zero J positions early agrees with the exact one to |mu|^J, and J is
-// chosen on the host so that |mu|^J is below the rounding of T.  Every chunk
-// therefore warms its recurrences up over the J positions before (forward) or
-// after (backward) it: no carries cross threads or CTAs, the CTAs of a line
-// are independent (no cluster), and no factor tables are needed.
+// chosen on the host so that |mu|^J is below the rounding of T.
+//
+// A CTA owns a segment [p0, p1) of 16 lines.  The 16 lanes of a half-warp
+// own one line: lane c holds FCH consecutive positions in registers.  The
+// forward recurrence runs over [p0 - J, p1 + J) (zero start J cells early),
+// the backward one over [p0, p1 + J) (zero start at its end); inside a line
+// the chunks are joined exactly by a 4-step shuffle scan of the chunk maps
+// x -> (-mu)^FCH x + e, so only the segment ends are warmed up.  Every phase
+// of a line stays inside its half-warp: the only CTA barriers are after the
+// staging and before the cooperative store.
+
+constexpr int FCH = 17;  // positions per lane (odd: conflict-free shared-memory columns)
+constexpr int FLANES = 16;
+// Longest segment for a recurrence warm-up J: 16 * FCH >= np + 2J.
+__host__ __device__ constexpr int filter_seg_max(int J) { return FLANES * FCH - 2 * J; }
 
 template <typename T>
 struct FiltSmem {
-  T *C;      // [(lc_max + 2H) * PITCH]  input cells, later w
-  T *R;      // [(lc_max + 2H) * PITCH]  compact RHS M b, later x
+  T *C;      // [(lc_max + 2H) * PITCH]  input cells, then w, then x
   T *om;     // [6 * LPG]
   int *n0;   // [LPG]
   SweepField *fd;
@@ -1108,13 +1118,12 @@ __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max
   s.n0 = reinterpret_cast<int *>(raw + FD_BYTES);
   T *p = reinterpret_cast<T *>(raw + FD_BYTES + 64 * sizeof(int));
   s.om = p; p += 6 * LPG;
-  s.C = p; p += (lc_max + 2 * H) * PITCH;
-  s.R = p;
+  s.C = p;
   return s;
 }
 
 template <typename T>
-__global__ void __launch_bounds__(NTH, 3)
+__global__ void __launch_bounds__(NTH, 2)
     sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
                         double toff, void *data_override, int lc_max, int H, unsigned *status,
                         int jstep, int nslice, const int *nlo, int cs, int clustered) {
@@ -1156,13 +1165,13 @@ __global__ void __launch_bounds__(NTH, 3)
   const T mu = T(F.sm_fac), ic = T(F.sm_inv_den);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const T *gsrc;
-  T *gdata;  // output
+  T *gdst;
   {
     const void *vs;
     void *vd;
     field_io(F, jstep, &vs, &vd);
     gsrc = reinterpret_cast<const T *>(vs);
-    gdata = reinterpret_cast<T *>(vd);
+    gdst = reinterpret_cast<T *>(vd);
   }
 
   // ---- stage rows p0-H .. p1+H-1 (periodic wrap) ----
@@ -1172,7 +1181,8 @@ __global__ void __launch_bounds__(NTH, 3)
     const bool okl = gl < F.M;
     for (int row = warp * 2 + (lane >> 4); row < nrows; row += 2 * NW) {
       int pos = p0 - H + row;
-      if (pos < 0 || pos >= L) { pos %= L; if (pos < 0) pos += L; }
+      if (pos < 0) pos += L;
+      else if (pos >= L) pos -= L;
       T *dst = S.C + row * PITCH + ln;
       if (okl) {
         const T *src = gsrc + (long long)pos * F.s_pos + gl;
@@ -1188,7 +1198,8 @@ __global__ void __launch_bounds__(NTH, 3)
       const T *lbase = gsrc + gl * F.s_line;
       for (int row = lane; row < nrows; row += 32) {
         int pos = p0 - H + row;
-        if (pos < 0 || pos >= L) { pos %= L; if (pos < 0) pos += L; }
+        if (pos < 0) pos += L;
+        else if (pos >= L) pos -= L;
         T *dst = S.C + row * PITCH + ln;
         if (okl) {
           if (sizeof(T) == 8) cp_async8(dst, lbase + pos); else cp_async4(dst, lbase + pos);
@@ -1232,102 +1243,148 @@ __global__ void __launch_bounds__(NTH, 3)
   // the launch has no clusters and needs no barrier.
   if (clustered) asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
 
-  const int ln = lane % LPG;
-  const int c = warp * CPW + lane / LPG;
-  const long long gl = line0 + ln;
+  // ---- one line per half-warp, FCH positions per lane ----
+  const int c = lane & (FLANES - 1);
+  const int ln = warp * 2 + (lane >> 4);
+  const unsigned hmask = 0xffffffffu;  // the warp is converged at every shuffle
+  T *col = S.C + ln;  // this line's column: row r at col[r * PITCH]
+  const int rb = H - p0;  // row of position 0
+  const T mmu = -mu;
+  T pw = T(1);  // (-mu)^FCH
+#pragma unroll
+  for (int i = 0; i < FCH; ++i) pw *= mmu;
 
-  // ---- phase 1: M b at positions p0-J .. p1+J-1 into R (row = pos - p0 + H) ----
+  // forward: w over [qa, qb) = [p0 - J, p1 + J), M b from the staged cells
+  const int qb = p1 + J;
+  if (np + 2 * J > FLANES * FCH) {  // the host keeps segments within filter_seg_max(J)
+    if (threadIdx.x == 0) atomicOr(status, STATUS_HALO);
+    return;
+  }
+  const int k0 = p0 - J + c * FCH;
+  T v[FCH];
   {
-    const int q0 = p0 - J, nq = np + 2 * J;
-    const int m1 = (nq + NCH - 1) / NCH;
-    const int s1 = q0 + min(nq, c * m1), e1 = q0 + min(nq, (c + 1) * m1);
-    if (s1 < e1) {
-      const int n0 = S.n0[ln];
-      const int r0 = (s1 - 1) + n0 - 2 - p0 + H;  // row of tap -2 of cell s1-1
-      const int rlast = e1 + n0 + 3 - p0 + H;     // row of tap +3 of cell e1
-      if (r0 < 0 || rlast >= nrows) {
-        atomicOr(status, STATUS_HALO);
-      } else {
-        const T *omp = S.om + 6 * ln;
-        const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5];
-        const T *cp = S.C + r0 * PITCH + ln;
-        T w0 = cp[0], w1 = cp[PITCH], w2 = cp[2 * PITCH], w3 = cp[3 * PITCH],
-          w4 = cp[4 * PITCH], w5 = cp[5 * PITCH];
-        T bm = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
-        w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[6 * PITCH];
-        T bc = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
-        const T *nxt = cp + 7 * PITCH;
-        T *rp = S.R + (s1 - p0 + H) * PITCH + ln;
-        const int n = e1 - s1;
-#pragma unroll 4
-        for (int i = 0; i < n; ++i) {
-          w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = nxt[i * PITCH];
+    const int n0 = S.n0[ln];
+    const T *omp = S.om + 6 * ln;
+    const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5];
+    // b needs rows k + n0 - 2 .. k + n0 + 3 for k = k0 - 1 .. min(k0 + FCH, qb)
+    const int klast = min(k0 + FCH, qb);
+    const int r0 = k0 - 1 + n0 - 2 + rb;
+    const int rlast = klast + n0 + 3 + rb;
+    bool ok = k0 < qb;
+    if (ok && (r0 < 0 || rlast >= nrows)) {
+      atomicOr(status, STATUS_HALO);
+      ok = false;
+    }
+    T w = T(0);
+    if (ok) {
+      const T *cp = col + r0 * PITCH;
+      T w0 = cp[0], w1 = cp[PITCH], w2 = cp[2 * PITCH], w3 = cp[3 * PITCH], w4 = cp[4 * PITCH],
+        w5 = cp[5 * PITCH];
+      T bm = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
+      w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[6 * PITCH];
+      T bc = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
+      const int nin = klast - k0;  // positions of this chunk inside the range
+#pragma unroll
+      for (int i = 0; i < FCH; ++i) {
+        T mb = T(0);
+        if (i < nin) {
+          w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[(7 + i) * PITCH];
           const T bp = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
-          rp[i * PITCH] = (bp + T(10.0) * bc + bm) * T(1.0 / 12.0);
+          mb = (bp + T(10.0) * bc + bm) * T(1.0 / 12.0);
           bm = bc;
           bc = bp;
         }
+        w = ic * mb + mmu * w;
+        v[i] = w;
       }
+    } else {
+#pragma unroll
+      for (int i = 0; i < FCH; ++i) v[i] = T(0);
+    }
+    // carries: chunk map x -> pw x + e_c, inclusive scan over the line's lanes
+    T sa = pw, sb = v[FCH - 1];
+#pragma unroll
+    for (int d = 1; d < FLANES; d <<= 1) {
+      const T pa = __shfl_up_sync(hmask, sa, d, FLANES);
+      const T pb = __shfl_up_sync(hmask, sb, d, FLANES);
+      if (c >= d) {
+        sb = sa * pb + sb;
+        sa = sa * pa;
+      }
+    }
+    T cin = __shfl_up_sync(hmask, sb, 1, FLANES);
+    if (c == 0) cin = T(0);
+    T pk = mmu;
+#pragma unroll
+    for (int i = 0; i < FCH; ++i) {
+      v[i] += cin * pk;
+      pk *= mmu;
     }
   }
-  __syncthreads();
-  // ---- phase 2: forward filter w at p0 .. p1+J-1 into C (warm-up J cells) ----
+  // every stencil read of this line is done (the shuffles order the lanes)
+  __syncwarp(hmask);
+#pragma unroll
+  for (int i = 0; i < FCH; ++i) {
+    const int k = k0 + i;
+    if (k >= p0 && k < qb) col[(k + rb) * PITCH] = v[i];
+  }
+  __syncwarp(hmask);
+
+  // backward: x over [p0, qb), zero start at qb
+  const int k1 = p0 + c * FCH;
   {
-    const int nq = np + J;
-    const int m2 = (nq + NCH - 1) / NCH;
-    const int s2 = p0 + min(nq, c * m2), e2 = p0 + min(nq, (c + 1) * m2);
-    if (s2 < e2) {
-      const T *rp = S.R + (s2 - J - p0 + H) * PITCH + ln;
-      T w = T(0);
-      for (int i = 0; i < J; ++i) w = ic * rp[i * PITCH] - mu * w;
-      rp += J * PITCH;
-      T *wp = S.C + (s2 - p0 + H) * PITCH + ln;
-      const int n = e2 - s2;
-#pragma unroll 4
-      for (int i = 0; i < n; ++i) {
-        w = ic * rp[i * PITCH] - mu * w;
-        wp[i * PITCH] = w;
+#pragma unroll
+    for (int i = 0; i < FCH; ++i) {
+      const int k = k1 + i;
+      v[i] = (k < qb) ? col[(k + rb) * PITCH] : T(0);
+    }
+    T x = T(0);
+#pragma unroll
+    for (int i = FCH - 1; i >= 0; --i) {
+      x = v[i] + mmu * x;
+      v[i] = x;
+    }
+    T sa = pw, sb = v[0];
+#pragma unroll
+    for (int d = 1; d < FLANES; d <<= 1) {
+      const T pa = __shfl_down_sync(hmask, sa, d, FLANES);
+      const T pb = __shfl_down_sync(hmask, sb, d, FLANES);
+      if (c + d < FLANES) {
+        sb = sa * pb + sb;
+        sa = sa * pa;
       }
     }
+    T cin = __shfl_down_sync(hmask, sb, 1, FLANES);
+    if (c == FLANES - 1) cin = T(0);
+    T pk = mmu;
+#pragma unroll
+    for (int i = FCH - 1; i >= 0; --i) {
+      v[i] += cin * pk;
+      pk *= mmu;
+    }
+  }
+  __syncwarp(hmask);
+#pragma unroll
+  for (int i = 0; i < FCH; ++i) {
+    const int k = k1 + i;
+    if (k < p1) col[(k + rb) * PITCH] = v[i];
   }
   __syncthreads();
   if (clustered) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
-  // ---- phase 3: backward filter x at p0 .. p1-1 (warm-up J cells) + store ----
-  {
-    const int m3 = (np + NCH - 1) / NCH;
-    const int s3 = p0 + min(np, c * m3), e3 = p0 + min(np, (c + 1) * m3);
-    if (s3 < e3) {
-      const T *wp = S.C + (e3 - p0 + H) * PITCH + ln;
-      T x = T(0);
-      for (int i = J - 1; i >= 0; --i) x = wp[i * PITCH] - mu * x;
-      const int n = e3 - s3;
-      wp -= n * PITCH;
-      if (F.s_line == 1) {
-        if (gl < F.M) {
-          T *gp = gdata + (long long)s3 * F.s_pos + gl;
-#pragma unroll 4
-          for (int i = n - 1; i >= 0; --i) {
-            x = wp[i * PITCH] - mu * x;
-            gp[i * F.s_pos] = x;
-          }
-        }
-      } else {
-        T *xp = S.R + (s3 - p0) * PITCH + ln;
-#pragma unroll 4
-        for (int i = n - 1; i >= 0; --i) {
-          x = wp[i * PITCH] - mu * x;
-          xp[i * PITCH] = x;
-        }
-      }
-    }
-  }
-  if (F.s_line != 1) {
-    __syncthreads();
+
+  // ---- cooperative store of rows H .. H+np-1 ----
+  if (F.s_line == 1) {
+    const int l = lane & (LPG - 1);
+    const long long gl = line0 + l;
+    if (gl < F.M)
+      for (int row = warp * 2 + (lane >> 4); row < np; row += 2 * NW)
+        gdst[(long long)(p0 + row) * F.s_pos + gl] = S.C[(row + H) * PITCH + l];
+  } else {
     for (int l2 = warp; l2 < LPG; l2 += NW) {
       const long long gl2 = line0 + l2;
       if (gl2 >= F.M) continue;
-      T *lbase = gdata + gl2 * F.s_line + p0;
-      for (int row = lane; row < np; row += 32) lbase[row] = S.R[row * PITCH + l2];
+      T *lbase = gdst + gl2 * F.s_line + p0;
+      for (int row = lane; row < np; row += 32) lbase[row] = S.C[(row + H) * PITCH + l2];
     }
   }
 }
@@ -1343,8 +1400,10 @@ size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source) {
 
 size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64) {
   size_t el = fp64 ? 8 : 4;
-  return FD_BYTES + 64 * sizeof(int) + (6 * (size_t)LPG + 2 * (size_t)(lc_max + 2 * halo) * PITCH) * el;
+  return FD_BYTES + 64 * sizeof(int) + (6 * (size_t)LPG + (size_t)(lc_max + 2 * halo) * PITCH) * el;
 }
+
+int filter_segment_max(int J) { return filter_seg_max(J); }
 
 size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64) {
   size_t el = fp64 ? 8 : 4;
