@@ -449,15 +449,26 @@ int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int
   return CCFV_OK;
 }
 
-static StepPlan *single_plan(ccfv_ctx *ctx, double dt, bool fp64, int *status,
-                             bool homogeneous = false) {
-  homogeneous = homogeneous && ctx->grid.source != CCFV_SRC_NONE;
-  auto key = std::make_tuple(dt, fp64 ? 1 : 0, homogeneous ? 1 : 0);
+// Plan of one field for the single-field calls: an out-of-place sequence
+// between the caller's field (passed per launch) and a context scratch field.
+static StepPlan *single_plan(ccfv_ctx *ctx, double dt, bool fp64, int *status) {
+  auto key = std::make_tuple(dt, fp64 ? 1 : 0, 0);
   auto it = ctx->step_plans.find(key);
   if (it != ctx->step_plans.end()) return it->second.get();
+  const size_t el = fp64 ? sizeof(double) : sizeof(float);
+  DevBuf &scratch = fp64 ? ctx->pp64 : ctx->pp32;
+  const size_t bytes = el * (size_t)ctx->grid.nx * ctx->grid.ny;
+  if (!scratch.p) {
+    cudaError_t e = scratch.alloc(bytes);
+    if (e != cudaSuccess) {
+      *status = set_error(ctx, CCFV_ERR_NOMEM, cudaGetErrorString(e));
+      return nullptr;
+    }
+  }
   auto plan = std::make_unique<StepPlan>();
-  std::vector<std::pair<void *, double>> f{{nullptr, 0.0}};
-  int st = build_step_plan(ctx, plan.get(), dt, fp64, f, homogeneous);
+  std::vector<PlanField> f(1);
+  f[0].B = scratch.p;  // A and in0: the caller's field (launch override)
+  int st = build_step_plan(ctx, plan.get(), dt, fp64, f);
   if (st != CCFV_OK) {
     *status = st;
     return nullptr;
@@ -467,13 +478,21 @@ static StepPlan *single_plan(ccfv_ctx *ctx, double dt, bool fp64, int *status,
   return res;
 }
 
+// nsteps split steps on one field: 3 nsteps sweeps alternating between the
+// field and the scratch field; an odd count ends in the scratch field and is
+// copied back.
 int steps(ccfv_ctx *ctx, void *d_C, bool fp64, double t0, double dt, int nsteps, cudaStream_t st) {
   int status = CCFV_OK;
   StepPlan *plan = single_plan(ctx, dt, fp64, &status);
   if (!plan) return status;
   for (int n = 0; n < nsteps; ++n) {
-    int rc = run_step_plan(ctx, *plan, fp64, 0, 1, t0 + n * dt, d_C, st);
+    int rc = run_step_plan(ctx, *plan, fp64, 0, 1, t0 + n * dt, d_C, st, n);
     if (rc) return rc;
+  }
+  if ((3 * nsteps) & 1) {
+    const size_t el = fp64 ? sizeof(double) : sizeof(float);
+    CK(cudaMemcpyAsync(d_C, (fp64 ? ctx->pp64 : ctx->pp32).p,
+                       el * (size_t)ctx->grid.nx * ctx->grid.ny, cudaMemcpyDeviceToDevice, st));
   }
   return CCFV_OK;
 }
@@ -638,14 +657,11 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
     std::memcpy(ctx->fine_plan_bufs, bufs, sizeof(bufs));
     ctx->fine_plan_slices = S;
   }
-  int status = CCFV_OK;
   // The first coarse sweep moves whole states and always runs in FP64: FP32
   // rounding there would seed every wavenumber at ~1e-7 |U|, and Parareal
   // amplifies the high-wavenumber error modes of advection (and of
   // Crank-Nicolson coarse steps with K Dt/h^2 >> 1) from one iteration to the
   // next.  In the iterations FP32 rounding is relative to the increments.
-  StepPlan *iplan = single_plan(ctx, dtc, true, &status);
-  if (!iplan) return status;
   // Coarse sweeps of the iterations: m steps out of place over W / W2,
   // starting from W; the result is in W2 when 3m is odd.  The delta form
   // propagates increments: the linear part of G (no source).
@@ -679,14 +695,12 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
     return CCFV_OK;
   };
 
-  // k = 0: coarse sweep U[n+1] = G(U[n])  (T2S4:1271-1280), in place on U[n+1]
+  // k = 0: coarse sweep U[n+1] = G(U[n])  (T2S4:1271-1280), FP64
   for (int n = 0; n < S; ++n) {
     double *un1 = U + (size_t)(n + 1) * NN;
     CK(cudaMemcpyAsync(un1, U + (size_t)n * NN, fb, cudaMemcpyDeviceToDevice, st));
-    for (int i = 0; i < m; ++i) {
-      int rc = run_step_plan(ctx, *iplan, true, 0, 1, o->t0 + n * DT + i * dtc, un1, st);
-      if (rc) return rc;
-    }
+    int rc = steps(ctx, un1, true, o->t0 + n * DT, dtc, m, st);
+    if (rc) return rc;
     if (Gold) CK(cudaMemcpyAsync(Gold + (size_t)(n + 1) * NN, un1, fb, cudaMemcpyDeviceToDevice, st));
   }
 

@@ -72,6 +72,7 @@ struct ccfv_ctx {
   // Parareal slice states and scratch
   ccfv::DevBuf U, F, Gold, W, C64, C32, norms, partial, counter, io, aux;
   ccfv::DevBuf FS, W2;  // ping-pong partners of the fine slices and the coarse work field
+  ccfv::DevBuf pp64, pp32;  // ping-pong partner of single-field calls (FP64, FP32)
   size_t slices_cap = 0;
   std::unique_ptr<ccfv::StepPlan> fine_plan;
   double fine_plan_key[4] = {0, 0, 0, 0};

@@ -348,7 +348,10 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
       if (fields[mid].group0 <= tile) lo = mid; else hi = mid - 1;
     }
     *S.fd = fields[lo];
-    if (data_override) S.fd->data = data_override;
+    if (data_override) {
+      S.fd->data = data_override;
+      if (S.fd->pp) S.fd->in0 = data_override;
+    }
   }
   __syncthreads();
   const SweepField &F = *S.fd;
@@ -814,7 +817,10 @@ __global__ void __launch_bounds__(NTH, 2)
           __ldg(reinterpret_cast<const long long *>(&fields[lo]) + threadIdx.x);
   }
   __syncthreads();
-  if (threadIdx.x == 0 && data_override) S.fd->data = data_override;
+  if (threadIdx.x == 0 && data_override) {
+    S.fd->data = data_override;
+    if (S.fd->pp) S.fd->in0 = data_override;
+  }
   __syncthreads();
   const SweepField &F = *S.fd;
   if (!field_active(F, jstep, nslice, nlo)) return;  // uniform over the cluster
@@ -1146,7 +1152,10 @@ __global__ void __launch_bounds__(NTH, 2)
           __ldg(reinterpret_cast<const long long *>(&fields[lo]) + threadIdx.x);
   }
   __syncthreads();
-  if (threadIdx.x == 0 && data_override) S.fd->data = data_override;
+  if (threadIdx.x == 0 && data_override) {
+    S.fd->data = data_override;
+    if (S.fd->pp) S.fd->in0 = data_override;
+  }
   __syncthreads();
   const SweepField &F = *S.fd;
   if (!field_active(F, jstep, nslice, nlo)) return;
