@@ -32,6 +32,8 @@
 #include <cooperative_groups.h>
 
 #include <climits>
+#include <map>
+#include <mutex>
 #include <cstdio>
 
 #include "ccfv_internal.h"
@@ -751,6 +753,9 @@ __device__ __forceinline__ void cp_async_commit() {
 __device__ __forceinline__ void cp_async_wait_all_committed() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
+__device__ __forceinline__ void cp_async_wait_prior1() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
 
 static_assert(sizeof(SweepField) % 8 == 0, "descriptor slot");
 
@@ -1109,90 +1114,105 @@ constexpr int FLANES = 16;
 // Longest segment for a recurrence warm-up J: 16 * FCH >= np + 2J.
 __host__ __device__ constexpr int filter_seg_max(int J) { return FLANES * FCH - 2 * J; }
 
+// Shared memory of one pipeline stage of the filter kernel.
 template <typename T>
-struct FiltSmem {
-  T *C;      // [(lc_max + 2H) * PITCH]  input cells, then w, then x
-  T *om;     // [6 * LPG]
-  int *n0;   // [LPG]
-  SweepField *fd;
+struct FiltStage {
+  SweepField *fd;  // descriptor of the stage's tile
+  int *n0;         // [LPG] shift of each line's stencil
+  T *om;           // [6 * LPG] stencil weights
+  T *C;            // [(lc_max + 2H) * PITCH] input cells, then w, then x
 };
 
-template <typename T>
-__device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max, int H) {
-  FiltSmem<T> s;
-  s.fd = reinterpret_cast<SweepField *>(raw);
-  s.n0 = reinterpret_cast<int *>(raw + FD_BYTES);
-  T *p = reinterpret_cast<T *>(raw + FD_BYTES + 64 * sizeof(int));
-  s.om = p; p += 6 * LPG;
-  s.C = p;
-  return s;
+__host__ __device__ inline size_t filter_stage_bytes(int lc_max, int H, size_t el) {
+  return (FD_BYTES + 64 * sizeof(int) + (6 * (size_t)LPG + (size_t)(lc_max + 2 * H) * PITCH) * el +
+          15) & ~size_t(15);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(NTH, 2)
-    sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
-                        double toff, void *data_override, int lc_max, int H, unsigned *status,
-                        int jstep, int nslice, const int *nlo, int cs, int clustered) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  // CTA -> (field, tile of LPG lines, segment).  The launch's clusters are the
-  // cs segments of one tile; fields carry their first CTA and halo, so fields
-  // of different segment lengths share one launch (lc_max and H size the
-  // shared memory only)
-  const int cta = (int)blockIdx.x + group_base;
-  FiltSmem<T> S = carve_filt<T>(smem_raw, lc_max, H);
-  {
+__device__ __forceinline__ FiltStage<T> filt_stage(unsigned char *raw, int lc_max, int H, int b) {
+  unsigned char *base = raw + (size_t)b * filter_stage_bytes(lc_max, H, sizeof(T));
+  FiltStage<T> s;
+  s.fd = reinterpret_cast<SweepField *>(base);
+  s.n0 = reinterpret_cast<int *>(base + FD_BYTES);
+  T *p = reinterpret_cast<T *>(base + FD_BYTES + 64 * sizeof(int));
+  s.om = p;
+  s.C = p + 6 * LPG;
+  return s;
+}
+
+// Geometry of one CTA-tile (a segment of 16 lines) of a field.
+struct FiltTile {
+  long long line0;
+  int p0, p1, np, H, nrows;
+};
+
+__device__ __forceinline__ FiltTile filt_tile(const SweepField &F, int cta, int cs) {
+  FiltTile t;
+  const int L = F.L;
+  const int q = cta - F.cta0;
+  const int rank = q % cs;
+  t.line0 = (long long)(q / cs) * LPG;
+  const int Lc = (L + cs - 1) / cs;
+  t.p0 = min(L, rank * Lc);
+  t.p1 = min(L, t.p0 + Lc);
+  t.np = t.p1 - t.p0;
+  t.H = F.halo_f;
+  t.nrows = t.np + 2 * t.H;
+  return t;
+}
+
+// Loads tile `cta`'s descriptor into stage `st` (all threads; ends with a
+// CTA barrier).  Returns whether the tile is active in this launch.
+template <typename T>
+__device__ __forceinline__ bool filt_load_desc(const SweepField *__restrict__ fields, int nfields,
+                                               int cta, void *data_override, int jstep,
+                                               int nslice, const int *nlo, double &toff_f,
+                                               double toff, FiltStage<T> st) {
+  constexpr int NW8 = (int)(sizeof(SweepField) / 8);
+  if (threadIdx.x < NW8) {
     int lo = 0, hi = nfields - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (__ldg(&fields[mid].cta0) <= cta) lo = mid; else hi = mid - 1;
     }
-    constexpr int NW8 = (int)(sizeof(SweepField) / 8);
-    if (threadIdx.x < NW8)
-      reinterpret_cast<long long *>(S.fd)[threadIdx.x] =
-          __ldg(reinterpret_cast<const long long *>(&fields[lo]) + threadIdx.x);
+    reinterpret_cast<long long *>(st.fd)[threadIdx.x] =
+        __ldg(reinterpret_cast<const long long *>(&fields[lo]) + threadIdx.x);
   }
   __syncthreads();
   if (threadIdx.x == 0 && data_override) {
-    S.fd->data = data_override;
-    if (S.fd->pp) S.fd->in0 = data_override;
+    st.fd->data = data_override;
+    if (st.fd->pp) st.fd->in0 = data_override;
   }
   __syncthreads();
-  const SweepField &F = *S.fd;
-  if (!field_active(F, jstep, nslice, nlo)) return;
-  toff = field_time(F, toff, jstep, nslice);
+  if (!field_active(*st.fd, jstep, nslice, nlo)) return false;
+  toff_f = field_time(*st.fd, toff, jstep, nslice);
+  return true;
+}
+
+// Issues the cp.async copies of a tile's rows p0-H .. p1+H-1 (periodic wrap)
+// and computes its lines' stencil weights (threads 0..15).
+template <typename T>
+__device__ __forceinline__ void filt_stage_tile(FiltStage<T> st, const FiltTile &t, int jstep,
+                                                double toff_f) {
+  const SweepField &F = *st.fd;
   const int L = F.L;
-  H = F.halo_f;
-  const int q = cta - F.cta0;
-  const int rank = q % cs;
-  const long long line0 = (long long)(q / cs) * LPG;
-  const int Lc = (L + cs - 1) / cs;
-  const int p0 = min(L, rank * Lc);
-  const int p1 = min(L, p0 + Lc);
-  const int np = p1 - p0;
-  const int nrows = np + 2 * H;
-  const int J = F.jf;
-  const T mu = T(F.sm_fac), ic = T(F.sm_inv_den);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const T *gsrc;
-  T *gdst;
   {
     const void *vs;
     void *vd;
     field_io(F, jstep, &vs, &vd);
     gsrc = reinterpret_cast<const T *>(vs);
-    gdst = reinterpret_cast<T *>(vd);
   }
-
-  // ---- stage rows p0-H .. p1+H-1 (periodic wrap) ----
   if (F.s_line == 1) {
     const int ln = lane & (LPG - 1);
-    const long long gl = line0 + ln;
+    const long long gl = t.line0 + ln;
     const bool okl = gl < F.M;
-    for (int row = warp * 2 + (lane >> 4); row < nrows; row += 2 * NW) {
-      int pos = p0 - H + row;
+    for (int row = warp * 2 + (lane >> 4); row < t.nrows; row += 2 * NW) {
+      int pos = t.p0 - t.H + row;
       if (pos < 0) pos += L;
       else if (pos >= L) pos -= L;
-      T *dst = S.C + row * PITCH + ln;
+      T *dst = st.C + row * PITCH + ln;
       if (okl) {
         const T *src = gsrc + (long long)pos * F.s_pos + gl;
         if (sizeof(T) == 8) cp_async8(dst, src); else cp_async4(dst, src);
@@ -1202,14 +1222,14 @@ __global__ void __launch_bounds__(NTH, 2)
     }
   } else {
     for (int ln = warp; ln < LPG; ln += NW) {
-      const long long gl = line0 + ln;
+      const long long gl = t.line0 + ln;
       const bool okl = gl < F.M;
       const T *lbase = gsrc + gl * F.s_line;
-      for (int row = lane; row < nrows; row += 32) {
-        int pos = p0 - H + row;
+      for (int row = lane; row < t.nrows; row += 32) {
+        int pos = t.p0 - t.H + row;
         if (pos < 0) pos += L;
         else if (pos >= L) pos -= L;
-        T *dst = S.C + row * PITCH + ln;
+        T *dst = st.C + row * PITCH + ln;
         if (okl) {
           if (sizeof(T) == 8) cp_async8(dst, lbase + pos); else cp_async4(dst, lbase + pos);
         } else {
@@ -1218,16 +1238,15 @@ __global__ void __launch_bounds__(NTH, 2)
       }
     }
   }
-  cp_async_commit();
   if (threadIdx.x < LPG) {  // per-line stencil b_k = sum_t om_t C_{k+n0+t}
     const int l = threadIdx.x;
-    const long long gl = line0 + l;
+    const long long gl = t.line0 + l;
     const double tau0 = F.t_min + F.ht * (double)gl;
     const double tau1 = F.t_min + F.ht * (double)(gl + 1);
-    const double f0 = edge_foot(F, 0, tau0, tau1, toff + F.ta_rel, toff + F.tb_rel);
+    const double f0 = edge_foot(F, 0, tau0, tau1, toff_f + F.ta_rel, toff_f + F.tb_rel);
     const double u = (f0 - F.s_min) / F.h;
     const double fl = floor(u);
-    S.n0[l] = (int)fl;
+    st.n0[l] = (int)fl;
     const double x = u - fl, x2 = x * x, x3 = x2 * x;
     const double A = x - 2.0 * x2 + x3, B = x3 - x2, Cc = 3.0 * x2 - 2.0 * x3;
     const double kq = F.kb * F.inv12h;
@@ -1236,7 +1255,7 @@ __global__ void __launch_bounds__(NTH, 2)
     const double pz = 12.0 * x3 - 18.0 * x2 - 24.0 * x + 15.0;
     const double pp1 = -8.0 * x3 + 6.0 * x2 + 18.0 * x - 1.0;
     const double pp2 = 2.0 * x3 - 3.0 * x;
-    T *om = S.om + 6 * l;
+    T *om = st.om + 6 * l;
     om[0] = T(A / 12.0 - kq * pm2);
     om[1] = T((B - 8.0 * A) / 12.0 + kq * (pm2 - pm1));
     om[2] = T(1.0 - Cc - 2.0 * B / 3.0 + kq * (pm1 - pz));
@@ -1244,36 +1263,33 @@ __global__ void __launch_bounds__(NTH, 2)
     om[4] = T((8.0 * B - A) / 12.0 + kq * (pp1 - pp2));
     om[5] = T(-B / 12.0 + kq * pp2);
   }
-  cp_async_wait_all_committed();
-  __syncthreads();
-  // In place, the segments of a line are read (halo) by the neighbouring CTAs
-  // of its cluster: this CTA's reads are complete here, and no CTA of the
-  // cluster stores before every CTA has arrived.  Out of place (ping-pong),
-  // the launch has no clusters and needs no barrier.
-  if (clustered) asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+}
 
-  // ---- one line per half-warp, FCH positions per lane ----
+// Both recurrences of a staged tile; x ends in the tile's rows H .. H+np-1.
+template <typename T>
+__device__ __forceinline__ void filt_solve(FiltStage<T> st, const FiltTile &t, unsigned *status) {
+  const SweepField &F = *st.fd;
+  const int J = F.jf;
+  const T mu = T(F.sm_fac), ic = T(F.sm_inv_den);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int p0 = t.p0, p1 = t.p1, nrows = t.nrows;
   const int c = lane & (FLANES - 1);
   const int ln = warp * 2 + (lane >> 4);
-  const unsigned hmask = 0xffffffffu;  // the warp is converged at every shuffle
-  T *col = S.C + ln;  // this line's column: row r at col[r * PITCH]
-  const int rb = H - p0;  // row of position 0
+  const unsigned fm = 0xffffffffu;  // the warp is converged at every shuffle
+  T *col = st.C + ln;               // this line's column: row r at col[r * PITCH]
+  const int rb = t.H - p0;          // row of position 0
   const T mmu = -mu;
   T pw = T(1);  // (-mu)^FCH
 #pragma unroll
   for (int i = 0; i < FCH; ++i) pw *= mmu;
 
-  // forward: w over [qa, qb) = [p0 - J, p1 + J), M b from the staged cells
+  // forward: w over [p0 - J, qb), qb = p1 + J, M b from the staged cells
   const int qb = p1 + J;
-  if (np + 2 * J > FLANES * FCH) {  // the host keeps segments within filter_seg_max(J)
-    if (threadIdx.x == 0) atomicOr(status, STATUS_HALO);
-    return;
-  }
   const int k0 = p0 - J + c * FCH;
   T v[FCH];
   {
-    const int n0 = S.n0[ln];
-    const T *omp = S.om + 6 * ln;
+    const int n0 = st.n0[ln];
+    const T *omp = st.om + 6 * ln;
     const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5];
     // b needs rows k + n0 - 2 .. k + n0 + 3 for k = k0 - 1 .. min(k0 + FCH, qb)
     const int klast = min(k0 + FCH, qb);
@@ -1314,14 +1330,14 @@ __global__ void __launch_bounds__(NTH, 2)
     T sa = pw, sb = v[FCH - 1];
 #pragma unroll
     for (int d = 1; d < FLANES; d <<= 1) {
-      const T pa = __shfl_up_sync(hmask, sa, d, FLANES);
-      const T pb = __shfl_up_sync(hmask, sb, d, FLANES);
+      const T pa = __shfl_up_sync(fm, sa, d, FLANES);
+      const T pb = __shfl_up_sync(fm, sb, d, FLANES);
       if (c >= d) {
         sb = sa * pb + sb;
         sa = sa * pa;
       }
     }
-    T cin = __shfl_up_sync(hmask, sb, 1, FLANES);
+    T cin = __shfl_up_sync(fm, sb, 1, FLANES);
     if (c == 0) cin = T(0);
     T pk = mmu;
 #pragma unroll
@@ -1331,13 +1347,13 @@ __global__ void __launch_bounds__(NTH, 2)
     }
   }
   // every stencil read of this line is done (the shuffles order the lanes)
-  __syncwarp(hmask);
+  __syncwarp(fm);
 #pragma unroll
   for (int i = 0; i < FCH; ++i) {
     const int k = k0 + i;
     if (k >= p0 && k < qb) col[(k + rb) * PITCH] = v[i];
   }
-  __syncwarp(hmask);
+  __syncwarp(fm);
 
   // backward: x over [p0, qb), zero start at qb
   const int k1 = p0 + c * FCH;
@@ -1356,14 +1372,14 @@ __global__ void __launch_bounds__(NTH, 2)
     T sa = pw, sb = v[0];
 #pragma unroll
     for (int d = 1; d < FLANES; d <<= 1) {
-      const T pa = __shfl_down_sync(hmask, sa, d, FLANES);
-      const T pb = __shfl_down_sync(hmask, sb, d, FLANES);
+      const T pa = __shfl_down_sync(fm, sa, d, FLANES);
+      const T pb = __shfl_down_sync(fm, sb, d, FLANES);
       if (c + d < FLANES) {
         sb = sa * pb + sb;
         sa = sa * pa;
       }
     }
-    T cin = __shfl_down_sync(hmask, sb, 1, FLANES);
+    T cin = __shfl_down_sync(fm, sb, 1, FLANES);
     if (c == FLANES - 1) cin = T(0);
     T pk = mmu;
 #pragma unroll
@@ -1372,30 +1388,104 @@ __global__ void __launch_bounds__(NTH, 2)
       pk *= mmu;
     }
   }
-  __syncwarp(hmask);
+  __syncwarp(fm);
 #pragma unroll
   for (int i = 0; i < FCH; ++i) {
     const int k = k1 + i;
     if (k < p1) col[(k + rb) * PITCH] = v[i];
   }
-  __syncthreads();
-  if (clustered) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
+}
 
-  // ---- cooperative store of rows H .. H+np-1 ----
+// Cooperative store of a solved tile (rows H .. H+np-1 of the stage).
+template <typename T>
+__device__ __forceinline__ void filt_store(FiltStage<T> st, const FiltTile &t, int jstep) {
+  const SweepField &F = *st.fd;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T *gdst;
+  {
+    const void *vs;
+    void *vd;
+    field_io(F, jstep, &vs, &vd);
+    gdst = reinterpret_cast<T *>(vd);
+  }
   if (F.s_line == 1) {
     const int l = lane & (LPG - 1);
-    const long long gl = line0 + l;
+    const long long gl = t.line0 + l;
     if (gl < F.M)
-      for (int row = warp * 2 + (lane >> 4); row < np; row += 2 * NW)
-        gdst[(long long)(p0 + row) * F.s_pos + gl] = S.C[(row + H) * PITCH + l];
+      for (int row = warp * 2 + (lane >> 4); row < t.np; row += 2 * NW)
+        gdst[(long long)(t.p0 + row) * F.s_pos + gl] = st.C[(row + t.H) * PITCH + l];
   } else {
     for (int l2 = warp; l2 < LPG; l2 += NW) {
-      const long long gl2 = line0 + l2;
+      const long long gl2 = t.line0 + l2;
       if (gl2 >= F.M) continue;
-      T *lbase = gdst + gl2 * F.s_line + p0;
-      for (int row = lane; row < np; row += 32) lbase[row] = S.C[(row + H) * PITCH + l2];
+      T *lbase = gdst + gl2 * F.s_line + t.p0;
+      for (int row = lane; row < t.np; row += 32) lbase[row] = st.C[(row + t.H) * PITCH + l2];
     }
   }
+}
+
+// Persistent over the launch's CTA-tiles (stride gridDim.x) with two
+// pipeline stages: the next tile's descriptor, cells and stencil weights are
+// fetched while the current tile is solved and stored.  In place
+// (`clustered`), the grid has one CTA per tile and the segments of a line
+// form a cluster: every CTA arrives once its staging reads have landed and
+// waits before its store.
+template <typename T>
+__global__ void __launch_bounds__(NTH, 2)
+    sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
+                        double toff, void *data_override, int lc_max, int H, unsigned *status,
+                        int jstep, int nslice, const int *nlo, int cs, int clustered,
+                        int total) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto stage = [&](int which) { return filt_stage<T>(smem_raw, lc_max, H, which); };
+  int cur = (int)blockIdx.x;
+  if (cur >= total) return;
+  double tf = 0.0;
+  bool act = filt_load_desc<T>(fields, nfields, cur + group_base, data_override, jstep, nslice,
+                               nlo, tf, toff, stage(0));
+  FiltTile tl{};
+  if (act) {
+    tl = filt_tile(*stage(0).fd, cur + group_base, cs);
+    filt_stage_tile<T>(stage(0), tl, jstep, tf);
+  }
+  cp_async_commit();
+  int b = 0;
+  while (true) {
+    const int nxt = cur + (int)gridDim.x;
+    bool nact = false;
+    FiltTile nt{};
+    if (nxt < total) {
+      const FiltStage<T> sn = stage(b ^ 1);
+      nact = filt_load_desc<T>(fields, nfields, nxt + group_base, data_override, jstep, nslice,
+                               nlo, tf, toff, sn);
+      if (nact) {
+        nt = filt_tile(*sn.fd, nxt + group_base, cs);
+        filt_stage_tile<T>(sn, nt, jstep, tf);
+      }
+    }
+    cp_async_commit();
+    cp_async_wait_prior1();
+    __syncthreads();
+    if (act) {
+      const FiltStage<T> sc = stage(b);
+      if (clustered) asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+      if (tl.np + 2 * sc.fd->jf > FLANES * FCH) {  // the host keeps segments shorter
+        if (threadIdx.x == 0) atomicOr(status, STATUS_HALO);
+      } else {
+        filt_solve<T>(sc, tl, status);
+      }
+      __syncthreads();
+      if (clustered) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
+      filt_store<T>(sc, tl, jstep);
+    }
+    if (nxt >= total) break;
+    __syncthreads();  // stage b is free for the tile after next
+    cur = nxt;
+    act = nact;
+    tl = nt;
+    b ^= 1;
+  }
+  cp_async_wait_all_committed();
 }
 
 }  // namespace
@@ -1408,8 +1498,7 @@ size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source) {
 }
 
 size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64) {
-  size_t el = fp64 ? 8 : 4;
-  return FD_BYTES + 64 * sizeof(int) + (6 * (size_t)LPG + (size_t)(lc_max + 2 * halo) * PITCH) * el;
+  return 2 * filter_stage_bytes(lc_max, halo, fp64 ? 8 : 4);  // two pipeline stages
 }
 
 int filter_segment_max(int J) { return filter_seg_max(J); }
@@ -1446,10 +1535,33 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   }
   if (groups_total <= 0) return cudaSuccess;
   if (filt && (cs == 1 || !inplace)) {  // whole lines per CTA, or out of place: no cluster
+    // persistent: as many CTAs as fit on the device, each looping over tiles
+    const int total = groups_total * cs;
+    int resident = 0;
+    {
+      static std::mutex mu;
+      static std::map<std::pair<int, size_t>, int> cache;  // (device, smem) -> CTAs on the device
+      int dev = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e != cudaSuccess) return e;
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = cache.find({dev, smem});
+      if (it == cache.end()) {
+        int sms = 0, per_sm = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess)
+          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_filter_kernel<T>, NTH,
+                                                            smem);
+        if (e != cudaSuccess) return e;
+        it = cache.emplace(std::make_pair(dev, smem), std::max(1, per_sm) * std::max(1, sms)).first;
+      }
+      resident = it->second;
+    }
+    const int grid = std::max(1, std::min(total, resident));
     count_launch();
-    sweep_filter_kernel<T><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
+    sweep_filter_kernel<T><<<(unsigned)grid, NTH, smem, stream>>>(
         d_fields, nfields, group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
-        nlo, cs, 0);
+        nlo, cs, 0, total);
     return cudaGetLastError();
   }
   cudaLaunchConfig_t cfg = {};
@@ -1467,7 +1579,8 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   count_launch();
   if (filt)  // group_base in CTAs
     return cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T>, d_fields, nfields, group_base * cs,
-                              toff, data, lc_max, halo, d_status, jstep, nslice, nlo, cs, 1);
+                              toff, data, lc_max, halo, d_status, jstep, nslice, nlo, cs, 1,
+                              groups_total * cs);
   if (fast)
     return cudaLaunchKernelEx(&cfg, sweep_fast_kernel<T>, d_fields, nfields, group_base, toff,
                               data, lc_max, halo, d_status, jstep, nslice, nlo);
