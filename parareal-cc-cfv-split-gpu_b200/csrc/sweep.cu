@@ -1114,18 +1114,30 @@ constexpr int FLANES = 16;
 // Longest segment for a recurrence warm-up J: 16 * FCH >= np + 2J.
 __host__ __device__ constexpr int filter_seg_max(int J) { return FLANES * FCH - 2 * J; }
 
-// Shared memory of one pipeline stage of the filter kernel.
+// Shared memory of one pipeline stage of the filter kernel.  Cells are stored
+// [row][line] with pitch FP_X (x-sweeps in FP64: 16-byte aligned line pairs
+// for vector copies) or FP_Y (odd: conflict-free transposed staging).  A
+// half-warp walks a line column with rows 17 apart per lane, which is free of
+// bank conflicts for both pitches.  The stage has rows for the longest
+// possible chunk walk, so the solve loops need no bounds predicates.
+constexpr int FP_X = LPG + 2;
+constexpr int FP_Y = LPG + 1;
+
 template <typename T>
 struct FiltStage {
   SweepField *fd;  // descriptor of the stage's tile
   int *n0;         // [LPG] shift of each line's stencil
   T *om;           // [6 * LPG] stencil weights
-  T *C;            // [(lc_max + 2H) * PITCH] input cells, then w, then x
+  T *C;            // [rows * pitch] input cells, then w, then x
+  int rows;        // rows of C
 };
 
+__host__ __device__ inline int filter_stage_rows(int lc_max, int H) {
+  return (lc_max > FLANES * FCH ? lc_max : FLANES * FCH) + 2 * H + 8;
+}
 __host__ __device__ inline size_t filter_stage_bytes(int lc_max, int H, size_t el) {
-  return (FD_BYTES + 64 * sizeof(int) + (6 * (size_t)LPG + (size_t)(lc_max + 2 * H) * PITCH) * el +
-          15) & ~size_t(15);
+  return (FD_BYTES + 64 * sizeof(int) + 6 * LPG * el +
+          (size_t)filter_stage_rows(lc_max, H) * FP_X * el + 15) & ~size_t(15);
 }
 
 template <typename T>
@@ -1136,7 +1148,9 @@ __device__ __forceinline__ FiltStage<T> filt_stage(unsigned char *raw, int lc_ma
   s.n0 = reinterpret_cast<int *>(base + FD_BYTES);
   T *p = reinterpret_cast<T *>(base + FD_BYTES + 64 * sizeof(int));
   s.om = p;
-  s.C = p + 6 * LPG;
+  s.C = reinterpret_cast<T *>(
+      (reinterpret_cast<uintptr_t>(p + 6 * LPG) + 15) & ~uintptr_t(15));  // 16-byte rows
+  s.rows = filter_stage_rows(lc_max, H);
   return s;
 }
 
@@ -1189,30 +1203,57 @@ __device__ __forceinline__ bool filt_load_desc(const SweepField *__restrict__ fi
   return true;
 }
 
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+
+// Whether a tile's x-sweep moves line pairs as 16-byte vectors (FP64, even
+// line stride, 16-byte aligned buffers).
+template <typename T>
+__device__ __forceinline__ bool filt_vec(const SweepField &F, const void *g) {
+  return sizeof(T) == 8 && F.s_line == 1 && (F.s_pos & 1) == 0 &&
+         (reinterpret_cast<uintptr_t>(g) & 15) == 0;
+}
+
 // Issues the cp.async copies of a tile's rows p0-H .. p1+H-1 (periodic wrap)
 // and computes its lines' stencil weights (threads 0..15).
-template <typename T>
-__device__ __forceinline__ void filt_stage_tile(FiltStage<T> st, const FiltTile &t, int jstep,
-                                                double toff_f) {
+template <typename T, int P>
+__device__ __forceinline__ void filt_stage_tile(FiltStage<T> st, const FiltTile &t,
+                                                const T *gsrc, double toff_f) {
   const SweepField &F = *st.fd;
   const int L = F.L;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const T *gsrc;
-  {
-    const void *vs;
-    void *vd;
-    field_io(F, jstep, &vs, &vd);
-    gsrc = reinterpret_cast<const T *>(vs);
-  }
-  if (F.s_line == 1) {
+  if (P == FP_X) {  // x-sweep, line pairs as 16-byte vectors
+    const int pr = threadIdx.x & 7, rs = threadIdx.x >> 3;
+    const long long gl = t.line0 + 2 * pr;
+    const bool ok2 = gl + 1 < F.M, ok1 = gl < F.M;
+    for (int row = rs; row < t.nrows; row += NTH / 8) {
+      int pos = t.p0 - t.H + row;
+      if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
+        pos %= L;
+        if (pos < 0) pos += L;
+      }
+      T *dst = st.C + row * P + 2 * pr;
+      const T *src = gsrc + (long long)pos * F.s_pos + gl;
+      if (ok2) {
+        cp_async16(dst, src);
+      } else {
+        dst[0] = ok1 ? src[0] : T(0);
+        dst[1] = T(0);
+      }
+    }
+  } else if (F.s_line == 1) {
     const int ln = lane & (LPG - 1);
     const long long gl = t.line0 + ln;
     const bool okl = gl < F.M;
     for (int row = warp * 2 + (lane >> 4); row < t.nrows; row += 2 * NW) {
       int pos = t.p0 - t.H + row;
-      if (pos < 0) pos += L;
-      else if (pos >= L) pos -= L;
-      T *dst = st.C + row * PITCH + ln;
+      if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
+        pos %= L;
+        if (pos < 0) pos += L;
+      }
+      T *dst = st.C + row * P + ln;
       if (okl) {
         const T *src = gsrc + (long long)pos * F.s_pos + gl;
         if (sizeof(T) == 8) cp_async8(dst, src); else cp_async4(dst, src);
@@ -1227,9 +1268,11 @@ __device__ __forceinline__ void filt_stage_tile(FiltStage<T> st, const FiltTile 
       const T *lbase = gsrc + gl * F.s_line;
       for (int row = lane; row < t.nrows; row += 32) {
         int pos = t.p0 - t.H + row;
-        if (pos < 0) pos += L;
-        else if (pos >= L) pos -= L;
-        T *dst = st.C + row * PITCH + ln;
+        if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
+          pos %= L;
+          if (pos < 0) pos += L;
+        }
+        T *dst = st.C + row * P + ln;
         if (okl) {
           if (sizeof(T) == 8) cp_async8(dst, lbase + pos); else cp_async4(dst, lbase + pos);
         } else {
@@ -1266,65 +1309,52 @@ __device__ __forceinline__ void filt_stage_tile(FiltStage<T> st, const FiltTile 
 }
 
 // Both recurrences of a staged tile; x ends in the tile's rows H .. H+np-1.
-template <typename T>
+template <typename T, int P>
 __device__ __forceinline__ void filt_solve(FiltStage<T> st, const FiltTile &t, unsigned *status) {
   const SweepField &F = *st.fd;
   const int J = F.jf;
   const T mu = T(F.sm_fac), ic = T(F.sm_inv_den);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int p0 = t.p0, p1 = t.p1, nrows = t.nrows;
+  const int p0 = t.p0;
   const int c = lane & (FLANES - 1);
   const int ln = warp * 2 + (lane >> 4);
   const unsigned fm = 0xffffffffu;  // the warp is converged at every shuffle
-  T *col = st.C + ln;               // this line's column: row r at col[r * PITCH]
   const int rb = t.H - p0;          // row of position 0
   const T mmu = -mu;
   T pw = T(1);  // (-mu)^FCH
 #pragma unroll
   for (int i = 0; i < FCH; ++i) pw *= mmu;
 
-  // forward: w over [p0 - J, qb), qb = p1 + J, M b from the staged cells
-  const int qb = p1 + J;
+  // forward: w over [p0 - J, qb), qb = p1 + J, M b from the staged cells;
+  // lanes past qb compute on stage rows that are allocated but not staged and
+  // keep M b = 0 there
+  const int qb = t.p1 + J;
   const int k0 = p0 - J + c * FCH;
+  const int n0 = st.n0[ln];
+  const int r0 = k0 - 1 + n0 - 2 + rb;  // row of tap -2 of position k0 - 1
+  const bool ok = r0 >= 0 && r0 + FCH + 7 <= st.rows;
+  if (!ok) atomicOr(status, STATUS_HALO);
   T v[FCH];
   {
-    const int n0 = st.n0[ln];
     const T *omp = st.om + 6 * ln;
     const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5];
-    // b needs rows k + n0 - 2 .. k + n0 + 3 for k = k0 - 1 .. min(k0 + FCH, qb)
-    const int klast = min(k0 + FCH, qb);
-    const int r0 = k0 - 1 + n0 - 2 + rb;
-    const int rlast = klast + n0 + 3 + rb;
-    bool ok = k0 < qb;
-    if (ok && (r0 < 0 || rlast >= nrows)) {
-      atomicOr(status, STATUS_HALO);
-      ok = false;
-    }
+    const T *cp = st.C + (ok ? r0 : 0) * P + ln;
+    T w0 = cp[0], w1 = cp[P], w2 = cp[2 * P], w3 = cp[3 * P], w4 = cp[4 * P], w5 = cp[5 * P];
+    T bm = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
+    w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[6 * P];
+    T bc = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
+    const int nin = ok ? qb - k0 : 0;  // positions of this chunk inside the range
     T w = T(0);
-    if (ok) {
-      const T *cp = col + r0 * PITCH;
-      T w0 = cp[0], w1 = cp[PITCH], w2 = cp[2 * PITCH], w3 = cp[3 * PITCH], w4 = cp[4 * PITCH],
-        w5 = cp[5 * PITCH];
-      T bm = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
-      w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[6 * PITCH];
-      T bc = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
-      const int nin = klast - k0;  // positions of this chunk inside the range
 #pragma unroll
-      for (int i = 0; i < FCH; ++i) {
-        T mb = T(0);
-        if (i < nin) {
-          w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[(7 + i) * PITCH];
-          const T bp = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
-          mb = (bp + T(10.0) * bc + bm) * T(1.0 / 12.0);
-          bm = bc;
-          bc = bp;
-        }
-        w = ic * mb + mmu * w;
-        v[i] = w;
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < FCH; ++i) v[i] = T(0);
+    for (int i = 0; i < FCH; ++i) {
+      w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[(7 + i) * P];
+      const T bp = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
+      T mb = (bp + T(10.0) * bc + bm) * T(1.0 / 12.0);
+      mb = (i < nin) ? mb : T(0);
+      bm = bc;
+      bc = bp;
+      w = ic * mb + mmu * w;
+      v[i] = w;
     }
     // carries: chunk map x -> pw x + e_c, inclusive scan over the line's lanes
     T sa = pw, sb = v[FCH - 1];
@@ -1346,22 +1376,25 @@ __device__ __forceinline__ void filt_solve(FiltStage<T> st, const FiltTile &t, u
       pk *= mmu;
     }
   }
-  // every stencil read of this line is done (the shuffles order the lanes)
+  // every stencil read of this line is done (the shuffles order the lanes);
+  // w of positions k0 .. k0+FCH-1 into this line's column
   __syncwarp(fm);
+  {
+    T *wp = st.C + (k0 + rb) * P + ln;
 #pragma unroll
-  for (int i = 0; i < FCH; ++i) {
-    const int k = k0 + i;
-    if (k >= p0 && k < qb) col[(k + rb) * PITCH] = v[i];
+    for (int i = 0; i < FCH; ++i) wp[i * P] = v[i];
   }
   __syncwarp(fm);
 
   // backward: x over [p0, qb), zero start at qb
   const int k1 = p0 + c * FCH;
   {
+    const T *xp = st.C + (k1 + rb) * P + ln;
+    const int nb = qb - k1;
 #pragma unroll
     for (int i = 0; i < FCH; ++i) {
-      const int k = k1 + i;
-      v[i] = (k < qb) ? col[(k + rb) * PITCH] : T(0);
+      const T val = xp[i * P];
+      v[i] = (i < nb) ? val : T(0);
     }
     T x = T(0);
 #pragma unroll
@@ -1389,39 +1422,54 @@ __device__ __forceinline__ void filt_solve(FiltStage<T> st, const FiltTile &t, u
     }
   }
   __syncwarp(fm);
+  {
+    T *wp = st.C + (k1 + rb) * P + ln;
 #pragma unroll
-  for (int i = 0; i < FCH; ++i) {
-    const int k = k1 + i;
-    if (k < p1) col[(k + rb) * PITCH] = v[i];
+    for (int i = 0; i < FCH; ++i) wp[i * P] = v[i];
   }
 }
 
 // Cooperative store of a solved tile (rows H .. H+np-1 of the stage).
-template <typename T>
-__device__ __forceinline__ void filt_store(FiltStage<T> st, const FiltTile &t, int jstep) {
+template <typename T, int P>
+__device__ __forceinline__ void filt_store(FiltStage<T> st, const FiltTile &t, T *gdst) {
   const SweepField &F = *st.fd;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  T *gdst;
-  {
-    const void *vs;
-    void *vd;
-    field_io(F, jstep, &vs, &vd);
-    gdst = reinterpret_cast<T *>(vd);
-  }
-  if (F.s_line == 1) {
+  if (P == FP_X) {  // x-sweep, line pairs as 16-byte vectors
+    const int pr = threadIdx.x & 7, rs = threadIdx.x >> 3;
+    const long long gl = t.line0 + 2 * pr;
+    const bool ok2 = gl + 1 < F.M, ok1 = gl < F.M;
+    for (int row = rs; row < t.np; row += NTH / 8) {
+      const T *src = st.C + (row + t.H) * P + 2 * pr;
+      T *dst = gdst + (long long)(t.p0 + row) * F.s_pos + gl;
+      if (ok2) {
+        *reinterpret_cast<double2 *>(dst) = *reinterpret_cast<const double2 *>(src);
+      } else if (ok1) {
+        dst[0] = src[0];
+      }
+    }
+  } else if (F.s_line == 1) {
     const int l = lane & (LPG - 1);
     const long long gl = t.line0 + l;
     if (gl < F.M)
       for (int row = warp * 2 + (lane >> 4); row < t.np; row += 2 * NW)
-        gdst[(long long)(t.p0 + row) * F.s_pos + gl] = st.C[(row + t.H) * PITCH + l];
+        gdst[(long long)(t.p0 + row) * F.s_pos + gl] = st.C[(row + t.H) * P + l];
   } else {
     for (int l2 = warp; l2 < LPG; l2 += NW) {
       const long long gl2 = t.line0 + l2;
       if (gl2 >= F.M) continue;
       T *lbase = gdst + gl2 * F.s_line + t.p0;
-      for (int row = lane; row < t.np; row += 32) lbase[row] = st.C[(row + t.H) * PITCH + l2];
+      for (int row = lane; row < t.np; row += 32) lbase[row] = st.C[(row + t.H) * P + l2];
     }
   }
+}
+
+// Stage pitch of a tile: FP_X when its cells move as 16-byte line pairs.
+template <typename T>
+__device__ __forceinline__ bool filt_xvec(const SweepField &F, int jstep) {
+  const void *vs;
+  void *vd;
+  field_io(F, jstep, &vs, &vd);
+  return filt_vec<T>(F, vs) && filt_vec<T>(F, vd);
 }
 
 // Persistent over the launch's CTA-tiles (stride gridDim.x) with two
@@ -1438,21 +1486,31 @@ __global__ void __launch_bounds__(NTH, 2)
                         int total) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   auto stage = [&](int which) { return filt_stage<T>(smem_raw, lc_max, H, which); };
+  auto issue = [&](FiltStage<T> sg, const FiltTile &tt, double tf, bool xv) {
+    const void *vs;
+    void *vd;
+    field_io(*sg.fd, jstep, &vs, &vd);
+    if (xv) filt_stage_tile<T, FP_X>(sg, tt, reinterpret_cast<const T *>(vs), tf);
+    else filt_stage_tile<T, FP_Y>(sg, tt, reinterpret_cast<const T *>(vs), tf);
+  };
   int cur = (int)blockIdx.x;
   if (cur >= total) return;
   double tf = 0.0;
   bool act = filt_load_desc<T>(fields, nfields, cur + group_base, data_override, jstep, nslice,
                                nlo, tf, toff, stage(0));
   FiltTile tl{};
+  bool xv = false;
   if (act) {
-    tl = filt_tile(*stage(0).fd, cur + group_base, cs);
-    filt_stage_tile<T>(stage(0), tl, jstep, tf);
+    const FiltStage<T> s0 = stage(0);
+    tl = filt_tile(*s0.fd, cur + group_base, cs);
+    xv = filt_xvec<T>(*s0.fd, jstep);
+    issue(s0, tl, tf, xv);
   }
   cp_async_commit();
   int b = 0;
   while (true) {
     const int nxt = cur + (int)gridDim.x;
-    bool nact = false;
+    bool nact = false, nxv = false;
     FiltTile nt{};
     if (nxt < total) {
       const FiltStage<T> sn = stage(b ^ 1);
@@ -1460,7 +1518,8 @@ __global__ void __launch_bounds__(NTH, 2)
                                nlo, tf, toff, sn);
       if (nact) {
         nt = filt_tile(*sn.fd, nxt + group_base, cs);
-        filt_stage_tile<T>(sn, nt, jstep, tf);
+        nxv = filt_xvec<T>(*sn.fd, jstep);
+        issue(sn, nt, tf, nxv);
       }
     }
     cp_async_commit();
@@ -1471,17 +1530,24 @@ __global__ void __launch_bounds__(NTH, 2)
       if (clustered) asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
       if (tl.np + 2 * sc.fd->jf > FLANES * FCH) {  // the host keeps segments shorter
         if (threadIdx.x == 0) atomicOr(status, STATUS_HALO);
+      } else if (xv) {
+        filt_solve<T, FP_X>(sc, tl, status);
       } else {
-        filt_solve<T>(sc, tl, status);
+        filt_solve<T, FP_Y>(sc, tl, status);
       }
       __syncthreads();
       if (clustered) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
-      filt_store<T>(sc, tl, jstep);
+      const void *vs;
+      void *vd;
+      field_io(*sc.fd, jstep, &vs, &vd);
+      if (xv) filt_store<T, FP_X>(sc, tl, reinterpret_cast<T *>(vd));
+      else filt_store<T, FP_Y>(sc, tl, reinterpret_cast<T *>(vd));
     }
     if (nxt >= total) break;
     __syncthreads();  // stage b is free for the tile after next
     cur = nxt;
     act = nact;
+    xv = nxv;
     tl = nt;
     b ^= 1;
   }
