@@ -1160,12 +1160,19 @@ struct FiltTile {
   int p0, p1, np, H, nrows;
 };
 
-__device__ __forceinline__ FiltTile filt_tile(const SweepField &F, int cta, int cs) {
+// Clustered launches keep a tile's segments in consecutive CTAs (one
+// cluster).  Otherwise x-sweep tiles are ordered segment-major: consecutive
+// CTAs take neighbouring 16-line groups of the same segment, so the CTAs in
+// flight read whole contiguous rows (DRAM page locality); y-sweep lines are
+// contiguous already.
+__device__ __forceinline__ FiltTile filt_tile(const SweepField &F, int cta, int cs,
+                                              bool clustered) {
   FiltTile t;
   const int L = F.L;
   const int q = cta - F.cta0;
-  const int rank = q % cs;
-  t.line0 = (long long)(q / cs) * LPG;
+  const bool segmajor = !clustered && F.s_line == 1;
+  const int rank = segmajor ? q / F.groups : q % cs;
+  t.line0 = (long long)(segmajor ? q % F.groups : q / cs) * LPG;
   const int Lc = (L + cs - 1) / cs;
   t.p0 = min(L, rank * Lc);
   t.p1 = min(L, t.p0 + Lc);
@@ -1502,7 +1509,7 @@ __global__ void __launch_bounds__(NTH, 2)
   bool xv = false;
   if (act) {
     const FiltStage<T> s0 = stage(0);
-    tl = filt_tile(*s0.fd, cur + group_base, cs);
+    tl = filt_tile(*s0.fd, cur + group_base, cs, clustered != 0);
     xv = filt_xvec<T>(*s0.fd, jstep);
     issue(s0, tl, tf, xv);
   }
@@ -1517,7 +1524,7 @@ __global__ void __launch_bounds__(NTH, 2)
       nact = filt_load_desc<T>(fields, nfields, nxt + group_base, data_override, jstep, nslice,
                                nlo, tf, toff, sn);
       if (nact) {
-        nt = filt_tile(*sn.fd, nxt + group_base, cs);
+        nt = filt_tile(*sn.fd, nxt + group_base, cs, clustered != 0);
         nxv = filt_xvec<T>(*sn.fd, jstep);
         issue(sn, nt, tf, nxv);
       }
