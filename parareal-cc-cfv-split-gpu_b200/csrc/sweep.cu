@@ -1127,7 +1127,8 @@ template <typename T>
 struct FiltStage {
   SweepField *fd;  // descriptor of the stage's tile
   int *n0;         // [LPG] shift of each line's stencil
-  T *om;           // [6 * LPG] stencil weights
+  T *om;           // [8 * LPG] weights of w's input: (1/c) M b as an 8-tap stencil of C
+  T *pwt;          // [32] (-mu)^(i+1), i = 0 .. FCH-1
   T *C;            // [rows * pitch] input cells, then w, then x
   int rows;        // rows of C
 };
@@ -1136,7 +1137,7 @@ __host__ __device__ inline int filter_stage_rows(int lc_max, int H) {
   return (lc_max > FLANES * FCH ? lc_max : FLANES * FCH) + 2 * H + 8;
 }
 __host__ __device__ inline size_t filter_stage_bytes(int lc_max, int H, size_t el) {
-  return (FD_BYTES + 64 * sizeof(int) + 6 * LPG * el +
+  return (FD_BYTES + 64 * sizeof(int) + (8 * LPG + 32) * el +
           (size_t)filter_stage_rows(lc_max, H) * FP_X * el + 15) & ~size_t(15);
 }
 
@@ -1148,8 +1149,9 @@ __device__ __forceinline__ FiltStage<T> filt_stage(unsigned char *raw, int lc_ma
   s.n0 = reinterpret_cast<int *>(base + FD_BYTES);
   T *p = reinterpret_cast<T *>(base + FD_BYTES + 64 * sizeof(int));
   s.om = p;
+  s.pwt = p + 8 * LPG;
   s.C = reinterpret_cast<T *>(
-      (reinterpret_cast<uintptr_t>(p + 6 * LPG) + 15) & ~uintptr_t(15));  // 16-byte rows
+      (reinterpret_cast<uintptr_t>(p + 8 * LPG + 32) + 15) & ~uintptr_t(15));  // 16-byte rows
   s.rows = filter_stage_rows(lc_max, H);
   return s;
 }
@@ -1305,13 +1307,31 @@ __device__ __forceinline__ void filt_stage_tile(FiltStage<T> st, const FiltTile 
     const double pz = 12.0 * x3 - 18.0 * x2 - 24.0 * x + 15.0;
     const double pp1 = -8.0 * x3 + 6.0 * x2 + 18.0 * x - 1.0;
     const double pp2 = 2.0 * x3 - 3.0 * x;
-    T *om = st.om + 6 * l;
-    om[0] = T(A / 12.0 - kq * pm2);
-    om[1] = T((B - 8.0 * A) / 12.0 + kq * (pm2 - pm1));
-    om[2] = T(1.0 - Cc - 2.0 * B / 3.0 + kq * (pm1 - pz));
-    om[3] = T(Cc + 2.0 * A / 3.0 + kq * (pz - pp1));
-    om[4] = T((8.0 * B - A) / 12.0 + kq * (pp1 - pp2));
-    om[5] = T(-B / 12.0 + kq * pp2);
+    // b_k = sum_{j<6} o_j C_{k+n0-2+j}; the input of w is (1/c) M b with
+    // M b_k = (b_{k-1} + 10 b_k + b_{k+1}) / 12 = sum_{m=-3..4} W_m C_{k+n0+m}
+    double o[6];
+    o[0] = A / 12.0 - kq * pm2;
+    o[1] = (B - 8.0 * A) / 12.0 + kq * (pm2 - pm1);
+    o[2] = 1.0 - Cc - 2.0 * B / 3.0 + kq * (pm1 - pz);
+    o[3] = Cc + 2.0 * A / 3.0 + kq * (pz - pp1);
+    o[4] = (8.0 * B - A) / 12.0 + kq * (pp1 - pp2);
+    o[5] = -B / 12.0 + kq * pp2;
+    const double icw = F.sm_inv_den / 12.0;
+    T *om = st.om + 8 * l;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {  // tap m - 3
+      const double a = (m >= 0 && m < 6) ? o[m] : 0.0;           // from b_{k-1}
+      const double bb = (m >= 1 && m < 7) ? o[m - 1] : 0.0;      // from b_k
+      const double cc = (m >= 2) ? o[m - 2] : 0.0;                // from b_{k+1}
+      om[m] = T(icw * (a + 10.0 * bb + cc));
+    }
+  } else if (threadIdx.x == LPG) {
+    const T mmu = T(-F.sm_fac);
+    T pk = mmu;
+    for (int i = 0; i < FCH; ++i) {
+      st.pwt[i] = pk;
+      pk *= mmu;
+    }
   }
 }
 
@@ -1320,7 +1340,7 @@ template <typename T, int P>
 __device__ __forceinline__ void filt_solve(FiltStage<T> st, const FiltTile &t, unsigned *status) {
   const SweepField &F = *st.fd;
   const int J = F.jf;
-  const T mu = T(F.sm_fac), ic = T(F.sm_inv_den);
+  const T mu = T(F.sm_fac);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int p0 = t.p0;
   const int c = lane & (FLANES - 1);
@@ -1328,40 +1348,33 @@ __device__ __forceinline__ void filt_solve(FiltStage<T> st, const FiltTile &t, u
   const unsigned fm = 0xffffffffu;  // the warp is converged at every shuffle
   const int rb = t.H - p0;          // row of position 0
   const T mmu = -mu;
-  T pw = T(1);  // (-mu)^FCH
-#pragma unroll
-  for (int i = 0; i < FCH; ++i) pw *= mmu;
+  const T pw = st.pwt[FCH - 1];     // (-mu)^FCH
 
-  // forward: w over [p0 - J, qb), qb = p1 + J, M b from the staged cells;
-  // lanes past qb compute on stage rows that are allocated but not staged and
-  // keep M b = 0 there
+  // forward: w_k = (1/c) M b_k - mu w_{k-1} over [p0 - J, qb), qb = p1 + J.
+  // Lanes past qb walk stage rows that are allocated but not staged: their
+  // values only flow further right and are masked by the backward load.
   const int qb = t.p1 + J;
   const int k0 = p0 - J + c * FCH;
   const int n0 = st.n0[ln];
-  const int r0 = k0 - 1 + n0 - 2 + rb;  // row of tap -2 of position k0 - 1
+  const int r0 = k0 + n0 - 3 + rb;  // row of tap -3 of position k0
   const bool ok = r0 >= 0 && r0 + FCH + 7 <= st.rows;
   if (!ok) atomicOr(status, STATUS_HALO);
   T v[FCH];
   {
-    const T *omp = st.om + 6 * ln;
-    const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5];
+    const T *omp = st.om + 8 * ln;
+    const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5],
+            o6 = omp[6], o7 = omp[7];
     const T *cp = st.C + (ok ? r0 : 0) * P + ln;
-    T w0 = cp[0], w1 = cp[P], w2 = cp[2 * P], w3 = cp[3 * P], w4 = cp[4 * P], w5 = cp[5 * P];
-    T bm = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
-    w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[6 * P];
-    T bc = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
-    const int nin = ok ? qb - k0 : 0;  // positions of this chunk inside the range
+    T w0 = cp[0], w1 = cp[P], w2 = cp[2 * P], w3 = cp[3 * P], w4 = cp[4 * P], w5 = cp[5 * P],
+      w6 = cp[6 * P], w7;
     T w = T(0);
 #pragma unroll
     for (int i = 0; i < FCH; ++i) {
-      w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[(7 + i) * P];
-      const T bp = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
-      T mb = (bp + T(10.0) * bc + bm) * T(1.0 / 12.0);
-      mb = (i < nin) ? mb : T(0);
-      bm = bc;
-      bc = bp;
-      w = ic * mb + mmu * w;
+      w7 = cp[(7 + i) * P];
+      const T mb = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5 + o6 * w6 + o7 * w7;
+      w = mb + mmu * w;
       v[i] = w;
+      w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6; w6 = w7;
     }
     // carries: chunk map x -> pw x + e_c, inclusive scan over the line's lanes
     T sa = pw, sb = v[FCH - 1];
@@ -1376,12 +1389,8 @@ __device__ __forceinline__ void filt_solve(FiltStage<T> st, const FiltTile &t, u
     }
     T cin = __shfl_up_sync(fm, sb, 1, FLANES);
     if (c == 0) cin = T(0);
-    T pk = mmu;
 #pragma unroll
-    for (int i = 0; i < FCH; ++i) {
-      v[i] += cin * pk;
-      pk *= mmu;
-    }
+    for (int i = 0; i < FCH; ++i) v[i] += cin * st.pwt[i];
   }
   // every stencil read of this line is done (the shuffles order the lanes);
   // w of positions k0 .. k0+FCH-1 into this line's column
@@ -1421,12 +1430,8 @@ __device__ __forceinline__ void filt_solve(FiltStage<T> st, const FiltTile &t, u
     }
     T cin = __shfl_down_sync(fm, sb, 1, FLANES);
     if (c == FLANES - 1) cin = T(0);
-    T pk = mmu;
 #pragma unroll
-    for (int i = FCH - 1; i >= 0; --i) {
-      v[i] += cin * pk;
-      pk *= mmu;
-    }
+    for (int i = 0; i < FCH; ++i) v[i] += cin * st.pwt[FCH - 1 - i];
   }
   __syncwarp(fm);
   {
