@@ -18,7 +18,9 @@ from pathlib import Path
 import numpy as np
 
 PKG_DIR = Path(__file__).resolve().parents[1]
-LIB_PATH = PKG_DIR / "lib" / "libccfv.so"
+# CCFV_LIBRARY selects another build of libccfv (same C ABI), e.g. for A/B timing.
+LIB_PATH = Path(os.environ["CCFV_LIBRARY"]) if os.environ.get("CCFV_LIBRARY") else \
+    PKG_DIR / "lib" / "libccfv.so"
 HEADER = PKG_DIR.parent / "include" / "ccfv.h"
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_HALO = 0, 1, 2, 3, 4, 5

@@ -1184,32 +1184,38 @@ __device__ __forceinline__ FiltTile filt_tile(const SweepField &F, int cta, int 
   return t;
 }
 
-// Loads tile `cta`'s descriptor into stage `st` (all threads; ends with a
-// CTA barrier).  Returns whether the tile is active in this launch.
+// Makes stage `st` hold the descriptor of field `fi` (copied only when the
+// stage holds another field; all threads; ends with a CTA barrier when it
+// copies).  Returns whether the field takes part in this launch step.
 template <typename T>
-__device__ __forceinline__ bool filt_load_desc(const SweepField *__restrict__ fields, int nfields,
-                                               int cta, void *data_override, int jstep,
-                                               int nslice, const int *nlo, double &toff_f,
-                                               double toff, FiltStage<T> st) {
-  constexpr int NW8 = (int)(sizeof(SweepField) / 8);
-  if (threadIdx.x < NW8) {
-    int lo = 0, hi = nfields - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (__ldg(&fields[mid].cta0) <= cta) lo = mid; else hi = mid - 1;
+__device__ __forceinline__ bool filt_desc(const SweepField *__restrict__ fields, int fi,
+                                          int &held, void *data_override, int jstep, int nslice,
+                                          const int *nlo, double &toff_f, double toff,
+                                          FiltStage<T> st) {
+  if (held != fi) {
+    constexpr int NW8 = (int)(sizeof(SweepField) / 8);
+    if (threadIdx.x < NW8)
+      reinterpret_cast<long long *>(st.fd)[threadIdx.x] =
+          __ldg(reinterpret_cast<const long long *>(&fields[fi]) + threadIdx.x);
+    __syncthreads();
+    if (threadIdx.x == 0 && data_override) {
+      st.fd->data = data_override;
+      if (st.fd->pp) st.fd->in0 = data_override;
     }
-    reinterpret_cast<long long *>(st.fd)[threadIdx.x] =
-        __ldg(reinterpret_cast<const long long *>(&fields[lo]) + threadIdx.x);
+    __syncthreads();
+    held = fi;
   }
-  __syncthreads();
-  if (threadIdx.x == 0 && data_override) {
-    st.fd->data = data_override;
-    if (st.fd->pp) st.fd->in0 = data_override;
-  }
-  __syncthreads();
   if (!field_active(*st.fd, jstep, nslice, nlo)) return false;
   toff_f = field_time(*st.fd, toff, jstep, nslice);
   return true;
+}
+
+// Field of CTA-tile `cta`, advancing from `fi` (a CTA's tiles come in
+// increasing order, so this is usually zero or one step).
+__device__ __forceinline__ int filt_field(const SweepField *__restrict__ fields, int nfields,
+                                          int fi, int cta) {
+  while (fi + 1 < nfields && __ldg(&fields[fi + 1].cta0) <= cta) ++fi;
+  return fi;
 }
 
 __device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
@@ -1507,9 +1513,20 @@ __global__ void __launch_bounds__(NTH, 2)
   };
   int cur = (int)blockIdx.x;
   if (cur >= total) return;
+  int fi = 0;  // field of the latest tile: binary search once, then advance
+  {
+    int lo = 0, hi = nfields - 1;
+    const int cta = cur + group_base;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(&fields[mid].cta0) <= cta) lo = mid; else hi = mid - 1;
+    }
+    fi = lo;
+  }
+  int held0 = -1, held1 = -1;  // field whose descriptor each stage holds
   double tf = 0.0;
-  bool act = filt_load_desc<T>(fields, nfields, cur + group_base, data_override, jstep, nslice,
-                               nlo, tf, toff, stage(0));
+  bool act = filt_desc<T>(fields, fi, held0, data_override, jstep, nslice, nlo, tf, toff,
+                          stage(0));
   FiltTile tl{};
   bool xv = false;
   if (act) {
@@ -1526,8 +1543,10 @@ __global__ void __launch_bounds__(NTH, 2)
     FiltTile nt{};
     if (nxt < total) {
       const FiltStage<T> sn = stage(b ^ 1);
-      nact = filt_load_desc<T>(fields, nfields, nxt + group_base, data_override, jstep, nslice,
-                               nlo, tf, toff, sn);
+      fi = filt_field(fields, nfields, fi, nxt + group_base);
+      int h = b ? held0 : held1;
+      nact = filt_desc<T>(fields, fi, h, data_override, jstep, nslice, nlo, tf, toff, sn);
+      if (b) held0 = h; else held1 = h;
       if (nact) {
         nt = filt_tile(*sn.fd, nxt + group_base, cs, clustered != 0);
         nxv = filt_xvec<T>(*sn.fd, jstep);
