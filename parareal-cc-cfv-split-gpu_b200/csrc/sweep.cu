@@ -753,9 +753,6 @@ __device__ __forceinline__ void cp_async_commit() {
 __device__ __forceinline__ void cp_async_wait_all_committed() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
-__device__ __forceinline__ void cp_async_wait_prior1() {
-  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-}
 
 static_assert(sizeof(SweepField) % 8 == 0, "descriptor slot");
 
@@ -1114,161 +1111,92 @@ constexpr int FLANES = 16;
 // Longest segment for a recurrence warm-up J: 16 * FCH >= np + 2J.
 __host__ __device__ constexpr int filter_seg_max(int J) { return FLANES * FCH - 2 * J; }
 
-// Shared memory of one pipeline stage of the filter kernel.  Cells are stored
-// [row][line] with pitch FP_X (x-sweeps in FP64: 16-byte aligned line pairs
-// for vector copies) or FP_Y (odd: conflict-free transposed staging).  A
-// half-warp walks a line column with rows 17 apart per lane, which is free of
-// bank conflicts for both pitches.  The stage has rows for the longest
-// possible chunk walk, so the solve loops need no bounds predicates.
-constexpr int FP_X = LPG + 2;
-constexpr int FP_Y = LPG + 1;
-
 template <typename T>
-struct FiltStage {
-  SweepField *fd;  // descriptor of the stage's tile
-  int *n0;         // [LPG] shift of each line's stencil
-  T *om;           // [8 * LPG] weights of w's input: (1/c) M b as an 8-tap stencil of C
-  T *pwt;          // [32] (-mu)^(i+1), i = 0 .. FCH-1
-  T *C;            // [rows * pitch] input cells, then w, then x
-  int rows;        // rows of C
+struct FiltSmem {
+  T *C;      // [(lc_max + 2H) * PITCH]  input cells, then w, then x
+  T *om;     // [6 * LPG]
+  int *n0;   // [LPG]
+  SweepField *fd;
 };
 
-__host__ __device__ inline int filter_stage_rows(int lc_max, int H) {
-  return (lc_max > FLANES * FCH ? lc_max : FLANES * FCH) + 2 * H + 8;
-}
-__host__ __device__ inline size_t filter_stage_bytes(int lc_max, int H, size_t el) {
-  return (FD_BYTES + 64 * sizeof(int) + (8 * LPG + 32) * el +
-          (size_t)filter_stage_rows(lc_max, H) * FP_X * el + 15) & ~size_t(15);
-}
-
 template <typename T>
-__device__ __forceinline__ FiltStage<T> filt_stage(unsigned char *raw, int lc_max, int H, int b) {
-  unsigned char *base = raw + (size_t)b * filter_stage_bytes(lc_max, H, sizeof(T));
-  FiltStage<T> s;
-  s.fd = reinterpret_cast<SweepField *>(base);
-  s.n0 = reinterpret_cast<int *>(base + FD_BYTES);
-  T *p = reinterpret_cast<T *>(base + FD_BYTES + 64 * sizeof(int));
-  s.om = p;
-  s.pwt = p + 8 * LPG;
-  s.C = reinterpret_cast<T *>(
-      (reinterpret_cast<uintptr_t>(p + 8 * LPG + 32) + 15) & ~uintptr_t(15));  // 16-byte rows
-  s.rows = filter_stage_rows(lc_max, H);
+__device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max, int H) {
+  FiltSmem<T> s;
+  s.fd = reinterpret_cast<SweepField *>(raw);
+  s.n0 = reinterpret_cast<int *>(raw + FD_BYTES);
+  T *p = reinterpret_cast<T *>(raw + FD_BYTES + 64 * sizeof(int));
+  s.om = p; p += 6 * LPG;
+  s.C = p;
   return s;
 }
 
-// Geometry of one CTA-tile (a segment of 16 lines) of a field.
-struct FiltTile {
-  long long line0;
-  int p0, p1, np, H, nrows;
-};
-
-// Clustered launches keep a tile's segments in consecutive CTAs (one
-// cluster).  Otherwise x-sweep tiles are ordered segment-major: consecutive
-// CTAs take neighbouring 16-line groups of the same segment, so the CTAs in
-// flight read whole contiguous rows (DRAM page locality); y-sweep lines are
-// contiguous already.
-__device__ __forceinline__ FiltTile filt_tile(const SweepField &F, int cta, int cs,
-                                              bool clustered) {
-  FiltTile t;
-  const int L = F.L;
-  const int q = cta - F.cta0;
-  const bool segmajor = !clustered && F.s_line == 1;
-  const int rank = segmajor ? q / F.groups : q % cs;
-  t.line0 = (long long)(segmajor ? q % F.groups : q / cs) * LPG;
-  const int Lc = (L + cs - 1) / cs;
-  t.p0 = min(L, rank * Lc);
-  t.p1 = min(L, t.p0 + Lc);
-  t.np = t.p1 - t.p0;
-  t.H = F.halo_f;
-  t.nrows = t.np + 2 * t.H;
-  return t;
-}
-
-// Makes stage `st` hold the descriptor of field `fi` (copied only when the
-// stage holds another field; all threads; ends with a CTA barrier when it
-// copies).  Returns whether the field takes part in this launch step.
 template <typename T>
-__device__ __forceinline__ bool filt_desc(const SweepField *__restrict__ fields, int fi,
-                                          int &held, void *data_override, int jstep, int nslice,
-                                          const int *nlo, double &toff_f, double toff,
-                                          FiltStage<T> st) {
-  if (held != fi) {
+__global__ void __launch_bounds__(NTH, 2)
+    sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
+                        double toff, void *data_override, int lc_max, int H, unsigned *status,
+                        int jstep, int nslice, const int *nlo, int cs, int clustered) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // CTA -> (field, tile of LPG lines, segment).  The launch's clusters are the
+  // cs segments of one tile; fields carry their first CTA and halo, so fields
+  // of different segment lengths share one launch (lc_max and H size the
+  // shared memory only)
+  const int cta = (int)blockIdx.x + group_base;
+  FiltSmem<T> S = carve_filt<T>(smem_raw, lc_max, H);
+  {
+    int lo = 0, hi = nfields - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(&fields[mid].cta0) <= cta) lo = mid; else hi = mid - 1;
+    }
     constexpr int NW8 = (int)(sizeof(SweepField) / 8);
     if (threadIdx.x < NW8)
-      reinterpret_cast<long long *>(st.fd)[threadIdx.x] =
-          __ldg(reinterpret_cast<const long long *>(&fields[fi]) + threadIdx.x);
-    __syncthreads();
-    if (threadIdx.x == 0 && data_override) {
-      st.fd->data = data_override;
-      if (st.fd->pp) st.fd->in0 = data_override;
-    }
-    __syncthreads();
-    held = fi;
+      reinterpret_cast<long long *>(S.fd)[threadIdx.x] =
+          __ldg(reinterpret_cast<const long long *>(&fields[lo]) + threadIdx.x);
   }
-  if (!field_active(*st.fd, jstep, nslice, nlo)) return false;
-  toff_f = field_time(*st.fd, toff, jstep, nslice);
-  return true;
-}
-
-// Field of CTA-tile `cta`, advancing from `fi` (a CTA's tiles come in
-// increasing order, so this is usually zero or one step).
-__device__ __forceinline__ int filt_field(const SweepField *__restrict__ fields, int nfields,
-                                          int fi, int cta) {
-  while (fi + 1 < nfields && __ldg(&fields[fi + 1].cta0) <= cta) ++fi;
-  return fi;
-}
-
-__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
-  unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
-}
-
-// Whether a tile's x-sweep moves line pairs as 16-byte vectors (FP64, even
-// line stride, 16-byte aligned buffers).
-template <typename T>
-__device__ __forceinline__ bool filt_vec(const SweepField &F, const void *g) {
-  return sizeof(T) == 8 && F.s_line == 1 && (F.s_pos & 1) == 0 &&
-         (reinterpret_cast<uintptr_t>(g) & 15) == 0;
-}
-
-// Issues the cp.async copies of a tile's rows p0-H .. p1+H-1 (periodic wrap)
-// and computes its lines' stencil weights (threads 0..15).
-template <typename T, int P>
-__device__ __forceinline__ void filt_stage_tile(FiltStage<T> st, const FiltTile &t,
-                                                const T *gsrc, double toff_f) {
-  const SweepField &F = *st.fd;
+  __syncthreads();
+  if (threadIdx.x == 0 && data_override) {
+    S.fd->data = data_override;
+    if (S.fd->pp) S.fd->in0 = data_override;
+  }
+  __syncthreads();
+  const SweepField &F = *S.fd;
+  if (!field_active(F, jstep, nslice, nlo)) return;
+  toff = field_time(F, toff, jstep, nslice);
   const int L = F.L;
+  H = F.halo_f;
+  const int q = cta - F.cta0;
+  const int rank = q % cs;
+  const long long line0 = (long long)(q / cs) * LPG;
+  const int Lc = (L + cs - 1) / cs;
+  const int p0 = min(L, rank * Lc);
+  const int p1 = min(L, p0 + Lc);
+  const int np = p1 - p0;
+  const int nrows = np + 2 * H;
+  const int J = F.jf;
+  const T mu = T(F.sm_fac), ic = T(F.sm_inv_den);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (P == FP_X) {  // x-sweep, line pairs as 16-byte vectors
-    const int pr = threadIdx.x & 7, rs = threadIdx.x >> 3;
-    const long long gl = t.line0 + 2 * pr;
-    const bool ok2 = gl + 1 < F.M, ok1 = gl < F.M;
-    for (int row = rs; row < t.nrows; row += NTH / 8) {
-      int pos = t.p0 - t.H + row;
-      if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
-        pos %= L;
-        if (pos < 0) pos += L;
-      }
-      T *dst = st.C + row * P + 2 * pr;
-      const T *src = gsrc + (long long)pos * F.s_pos + gl;
-      if (ok2) {
-        cp_async16(dst, src);
-      } else {
-        dst[0] = ok1 ? src[0] : T(0);
-        dst[1] = T(0);
-      }
-    }
-  } else if (F.s_line == 1) {
+  const T *gsrc;
+  T *gdst;
+  {
+    const void *vs;
+    void *vd;
+    field_io(F, jstep, &vs, &vd);
+    gsrc = reinterpret_cast<const T *>(vs);
+    gdst = reinterpret_cast<T *>(vd);
+  }
+
+  // ---- stage rows p0-H .. p1+H-1 (periodic wrap) ----
+  if (F.s_line == 1) {
     const int ln = lane & (LPG - 1);
-    const long long gl = t.line0 + ln;
+    const long long gl = line0 + ln;
     const bool okl = gl < F.M;
-    for (int row = warp * 2 + (lane >> 4); row < t.nrows; row += 2 * NW) {
-      int pos = t.p0 - t.H + row;
+    for (int row = warp * 2 + (lane >> 4); row < nrows; row += 2 * NW) {
+      int pos = p0 - H + row;
       if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
         pos %= L;
         if (pos < 0) pos += L;
       }
-      T *dst = st.C + row * P + ln;
+      T *dst = S.C + row * PITCH + ln;
       if (okl) {
         const T *src = gsrc + (long long)pos * F.s_pos + gl;
         if (sizeof(T) == 8) cp_async8(dst, src); else cp_async4(dst, src);
@@ -1278,16 +1206,16 @@ __device__ __forceinline__ void filt_stage_tile(FiltStage<T> st, const FiltTile 
     }
   } else {
     for (int ln = warp; ln < LPG; ln += NW) {
-      const long long gl = t.line0 + ln;
+      const long long gl = line0 + ln;
       const bool okl = gl < F.M;
       const T *lbase = gsrc + gl * F.s_line;
-      for (int row = lane; row < t.nrows; row += 32) {
-        int pos = t.p0 - t.H + row;
+      for (int row = lane; row < nrows; row += 32) {
+        int pos = p0 - H + row;
         if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
           pos %= L;
           if (pos < 0) pos += L;
         }
-        T *dst = st.C + row * P + ln;
+        T *dst = S.C + row * PITCH + ln;
         if (okl) {
           if (sizeof(T) == 8) cp_async8(dst, lbase + pos); else cp_async4(dst, lbase + pos);
         } else {
@@ -1296,15 +1224,16 @@ __device__ __forceinline__ void filt_stage_tile(FiltStage<T> st, const FiltTile 
       }
     }
   }
+  cp_async_commit();
   if (threadIdx.x < LPG) {  // per-line stencil b_k = sum_t om_t C_{k+n0+t}
     const int l = threadIdx.x;
-    const long long gl = t.line0 + l;
+    const long long gl = line0 + l;
     const double tau0 = F.t_min + F.ht * (double)gl;
     const double tau1 = F.t_min + F.ht * (double)(gl + 1);
-    const double f0 = edge_foot(F, 0, tau0, tau1, toff_f + F.ta_rel, toff_f + F.tb_rel);
+    const double f0 = edge_foot(F, 0, tau0, tau1, toff + F.ta_rel, toff + F.tb_rel);
     const double u = (f0 - F.s_min) / F.h;
     const double fl = floor(u);
-    st.n0[l] = (int)fl;
+    S.n0[l] = (int)fl;
     const double x = u - fl, x2 = x * x, x3 = x2 * x;
     const double A = x - 2.0 * x2 + x3, B = x3 - x2, Cc = 3.0 * x2 - 2.0 * x3;
     const double kq = F.kb * F.inv12h;
@@ -1313,110 +1242,116 @@ __device__ __forceinline__ void filt_stage_tile(FiltStage<T> st, const FiltTile 
     const double pz = 12.0 * x3 - 18.0 * x2 - 24.0 * x + 15.0;
     const double pp1 = -8.0 * x3 + 6.0 * x2 + 18.0 * x - 1.0;
     const double pp2 = 2.0 * x3 - 3.0 * x;
-    // b_k = sum_{j<6} o_j C_{k+n0-2+j}; the input of w is (1/c) M b with
-    // M b_k = (b_{k-1} + 10 b_k + b_{k+1}) / 12 = sum_{m=-3..4} W_m C_{k+n0+m}
-    double o[6];
-    o[0] = A / 12.0 - kq * pm2;
-    o[1] = (B - 8.0 * A) / 12.0 + kq * (pm2 - pm1);
-    o[2] = 1.0 - Cc - 2.0 * B / 3.0 + kq * (pm1 - pz);
-    o[3] = Cc + 2.0 * A / 3.0 + kq * (pz - pp1);
-    o[4] = (8.0 * B - A) / 12.0 + kq * (pp1 - pp2);
-    o[5] = -B / 12.0 + kq * pp2;
-    const double icw = F.sm_inv_den / 12.0;
-    T *om = st.om + 8 * l;
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {  // tap m - 3
-      const double a = (m >= 0 && m < 6) ? o[m] : 0.0;           // from b_{k-1}
-      const double bb = (m >= 1 && m < 7) ? o[m - 1] : 0.0;      // from b_k
-      const double cc = (m >= 2) ? o[m - 2] : 0.0;                // from b_{k+1}
-      om[m] = T(icw * (a + 10.0 * bb + cc));
-    }
-  } else if (threadIdx.x == LPG) {
-    const T mmu = T(-F.sm_fac);
-    T pk = mmu;
-    for (int i = 0; i < FCH; ++i) {
-      st.pwt[i] = pk;
-      pk *= mmu;
-    }
+    T *om = S.om + 6 * l;
+    om[0] = T(A / 12.0 - kq * pm2);
+    om[1] = T((B - 8.0 * A) / 12.0 + kq * (pm2 - pm1));
+    om[2] = T(1.0 - Cc - 2.0 * B / 3.0 + kq * (pm1 - pz));
+    om[3] = T(Cc + 2.0 * A / 3.0 + kq * (pz - pp1));
+    om[4] = T((8.0 * B - A) / 12.0 + kq * (pp1 - pp2));
+    om[5] = T(-B / 12.0 + kq * pp2);
   }
-}
+  cp_async_wait_all_committed();
+  __syncthreads();
+  // In place, the segments of a line are read (halo) by the neighbouring CTAs
+  // of its cluster: this CTA's reads are complete here, and no CTA of the
+  // cluster stores before every CTA has arrived.  Out of place (ping-pong),
+  // the launch has no clusters and needs no barrier.
+  if (clustered) asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
 
-// Both recurrences of a staged tile; x ends in the tile's rows H .. H+np-1.
-template <typename T, int P>
-__device__ __forceinline__ void filt_solve(FiltStage<T> st, const FiltTile &t, unsigned *status) {
-  const SweepField &F = *st.fd;
-  const int J = F.jf;
-  const T mu = T(F.sm_fac);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int p0 = t.p0;
+  // ---- one line per half-warp, FCH positions per lane ----
   const int c = lane & (FLANES - 1);
   const int ln = warp * 2 + (lane >> 4);
-  const unsigned fm = 0xffffffffu;  // the warp is converged at every shuffle
-  const int rb = t.H - p0;          // row of position 0
+  const unsigned hmask = 0xffffffffu;  // the warp is converged at every shuffle
+  T *col = S.C + ln;  // this line's column: row r at col[r * PITCH]
+  const int rb = H - p0;  // row of position 0
   const T mmu = -mu;
-  const T pw = st.pwt[FCH - 1];     // (-mu)^FCH
+  T pw = T(1);  // (-mu)^FCH
+#pragma unroll
+  for (int i = 0; i < FCH; ++i) pw *= mmu;
 
-  // forward: w_k = (1/c) M b_k - mu w_{k-1} over [p0 - J, qb), qb = p1 + J.
-  // Lanes past qb walk stage rows that are allocated but not staged: their
-  // values only flow further right and are masked by the backward load.
-  const int qb = t.p1 + J;
+  // forward: w over [qa, qb) = [p0 - J, p1 + J), M b from the staged cells
+  const int qb = p1 + J;
+  if (np + 2 * J > FLANES * FCH) {  // the host keeps segments within filter_seg_max(J)
+    if (threadIdx.x == 0) atomicOr(status, STATUS_HALO);
+    return;
+  }
   const int k0 = p0 - J + c * FCH;
-  const int n0 = st.n0[ln];
-  const int r0 = k0 + n0 - 3 + rb;  // row of tap -3 of position k0
-  const bool ok = r0 >= 0 && r0 + FCH + 7 <= st.rows;
-  if (!ok) atomicOr(status, STATUS_HALO);
   T v[FCH];
   {
-    const T *omp = st.om + 8 * ln;
-    const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5],
-            o6 = omp[6], o7 = omp[7];
-    const T *cp = st.C + (ok ? r0 : 0) * P + ln;
-    T w0 = cp[0], w1 = cp[P], w2 = cp[2 * P], w3 = cp[3 * P], w4 = cp[4 * P], w5 = cp[5 * P],
-      w6 = cp[6 * P], w7;
+    const int n0 = S.n0[ln];
+    const T *omp = S.om + 6 * ln;
+    const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5];
+    // b needs rows k + n0 - 2 .. k + n0 + 3 for k = k0 - 1 .. min(k0 + FCH, qb)
+    const int klast = min(k0 + FCH, qb);
+    const int r0 = k0 - 1 + n0 - 2 + rb;
+    const int rlast = klast + n0 + 3 + rb;
+    bool ok = k0 < qb;
+    if (ok && (r0 < 0 || rlast >= nrows)) {
+      atomicOr(status, STATUS_HALO);
+      ok = false;
+    }
     T w = T(0);
+    if (ok) {
+      const T *cp = col + r0 * PITCH;
+      T w0 = cp[0], w1 = cp[PITCH], w2 = cp[2 * PITCH], w3 = cp[3 * PITCH], w4 = cp[4 * PITCH],
+        w5 = cp[5 * PITCH];
+      T bm = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
+      w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[6 * PITCH];
+      T bc = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
+      const int nin = klast - k0;  // positions of this chunk inside the range
 #pragma unroll
-    for (int i = 0; i < FCH; ++i) {
-      w7 = cp[(7 + i) * P];
-      const T mb = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5 + o6 * w6 + o7 * w7;
-      w = mb + mmu * w;
-      v[i] = w;
-      w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6; w6 = w7;
+      for (int i = 0; i < FCH; ++i) {
+        T mb = T(0);
+        if (i < nin) {
+          w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[(7 + i) * PITCH];
+          const T bp = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
+          mb = (bp + T(10.0) * bc + bm) * T(1.0 / 12.0);
+          bm = bc;
+          bc = bp;
+        }
+        w = ic * mb + mmu * w;
+        v[i] = w;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < FCH; ++i) v[i] = T(0);
     }
     // carries: chunk map x -> pw x + e_c, inclusive scan over the line's lanes
     T sa = pw, sb = v[FCH - 1];
 #pragma unroll
     for (int d = 1; d < FLANES; d <<= 1) {
-      const T pa = __shfl_up_sync(fm, sa, d, FLANES);
-      const T pb = __shfl_up_sync(fm, sb, d, FLANES);
+      const T pa = __shfl_up_sync(hmask, sa, d, FLANES);
+      const T pb = __shfl_up_sync(hmask, sb, d, FLANES);
       if (c >= d) {
         sb = sa * pb + sb;
         sa = sa * pa;
       }
     }
-    T cin = __shfl_up_sync(fm, sb, 1, FLANES);
+    T cin = __shfl_up_sync(hmask, sb, 1, FLANES);
     if (c == 0) cin = T(0);
+    T pk = mmu;
 #pragma unroll
-    for (int i = 0; i < FCH; ++i) v[i] += cin * st.pwt[i];
+    for (int i = 0; i < FCH; ++i) {
+      v[i] += cin * pk;
+      pk *= mmu;
+    }
   }
-  // every stencil read of this line is done (the shuffles order the lanes);
-  // w of positions k0 .. k0+FCH-1 into this line's column
-  __syncwarp(fm);
-  {
-    T *wp = st.C + (k0 + rb) * P + ln;
+  // every stencil read of this line is done (the shuffles order the lanes)
+  __syncwarp(hmask);
 #pragma unroll
-    for (int i = 0; i < FCH; ++i) wp[i * P] = v[i];
+  for (int i = 0; i < FCH; ++i) {
+    const int k = k0 + i;
+    if (k >= p0 && k < qb) col[(k + rb) * PITCH] = v[i];
   }
-  __syncwarp(fm);
+  __syncwarp(hmask);
 
   // backward: x over [p0, qb), zero start at qb
   const int k1 = p0 + c * FCH;
   {
-    const T *xp = st.C + (k1 + rb) * P + ln;
-    const int nb = qb - k1;
 #pragma unroll
     for (int i = 0; i < FCH; ++i) {
-      const T val = xp[i * P];
-      v[i] = (i < nb) ? val : T(0);
+      const int k = k1 + i;
+      v[i] = (k < qb) ? col[(k + rb) * PITCH] : T(0);
     }
     T x = T(0);
 #pragma unroll
@@ -1427,162 +1362,46 @@ __device__ __forceinline__ void filt_solve(FiltStage<T> st, const FiltTile &t, u
     T sa = pw, sb = v[0];
 #pragma unroll
     for (int d = 1; d < FLANES; d <<= 1) {
-      const T pa = __shfl_down_sync(fm, sa, d, FLANES);
-      const T pb = __shfl_down_sync(fm, sb, d, FLANES);
+      const T pa = __shfl_down_sync(hmask, sa, d, FLANES);
+      const T pb = __shfl_down_sync(hmask, sb, d, FLANES);
       if (c + d < FLANES) {
         sb = sa * pb + sb;
         sa = sa * pa;
       }
     }
-    T cin = __shfl_down_sync(fm, sb, 1, FLANES);
+    T cin = __shfl_down_sync(hmask, sb, 1, FLANES);
     if (c == FLANES - 1) cin = T(0);
+    T pk = mmu;
 #pragma unroll
-    for (int i = 0; i < FCH; ++i) v[i] += cin * st.pwt[FCH - 1 - i];
-  }
-  __syncwarp(fm);
-  {
-    T *wp = st.C + (k1 + rb) * P + ln;
-#pragma unroll
-    for (int i = 0; i < FCH; ++i) wp[i * P] = v[i];
-  }
-}
-
-// Cooperative store of a solved tile (rows H .. H+np-1 of the stage).
-template <typename T, int P>
-__device__ __forceinline__ void filt_store(FiltStage<T> st, const FiltTile &t, T *gdst) {
-  const SweepField &F = *st.fd;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (P == FP_X) {  // x-sweep, line pairs as 16-byte vectors
-    const int pr = threadIdx.x & 7, rs = threadIdx.x >> 3;
-    const long long gl = t.line0 + 2 * pr;
-    const bool ok2 = gl + 1 < F.M, ok1 = gl < F.M;
-    for (int row = rs; row < t.np; row += NTH / 8) {
-      const T *src = st.C + (row + t.H) * P + 2 * pr;
-      T *dst = gdst + (long long)(t.p0 + row) * F.s_pos + gl;
-      if (ok2) {
-        *reinterpret_cast<double2 *>(dst) = *reinterpret_cast<const double2 *>(src);
-      } else if (ok1) {
-        dst[0] = src[0];
-      }
+    for (int i = FCH - 1; i >= 0; --i) {
+      v[i] += cin * pk;
+      pk *= mmu;
     }
-  } else if (F.s_line == 1) {
+  }
+  __syncwarp(hmask);
+#pragma unroll
+  for (int i = 0; i < FCH; ++i) {
+    const int k = k1 + i;
+    if (k < p1) col[(k + rb) * PITCH] = v[i];
+  }
+  __syncthreads();
+  if (clustered) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
+
+  // ---- cooperative store of rows H .. H+np-1 ----
+  if (F.s_line == 1) {
     const int l = lane & (LPG - 1);
-    const long long gl = t.line0 + l;
+    const long long gl = line0 + l;
     if (gl < F.M)
-      for (int row = warp * 2 + (lane >> 4); row < t.np; row += 2 * NW)
-        gdst[(long long)(t.p0 + row) * F.s_pos + gl] = st.C[(row + t.H) * P + l];
+      for (int row = warp * 2 + (lane >> 4); row < np; row += 2 * NW)
+        gdst[(long long)(p0 + row) * F.s_pos + gl] = S.C[(row + H) * PITCH + l];
   } else {
     for (int l2 = warp; l2 < LPG; l2 += NW) {
-      const long long gl2 = t.line0 + l2;
+      const long long gl2 = line0 + l2;
       if (gl2 >= F.M) continue;
-      T *lbase = gdst + gl2 * F.s_line + t.p0;
-      for (int row = lane; row < t.np; row += 32) lbase[row] = st.C[(row + t.H) * P + l2];
+      T *lbase = gdst + gl2 * F.s_line + p0;
+      for (int row = lane; row < np; row += 32) lbase[row] = S.C[(row + H) * PITCH + l2];
     }
   }
-}
-
-// Stage pitch of a tile: FP_X when its cells move as 16-byte line pairs.
-template <typename T>
-__device__ __forceinline__ bool filt_xvec(const SweepField &F, int jstep) {
-  const void *vs;
-  void *vd;
-  field_io(F, jstep, &vs, &vd);
-  return filt_vec<T>(F, vs) && filt_vec<T>(F, vd);
-}
-
-// Persistent over the launch's CTA-tiles (stride gridDim.x) with two
-// pipeline stages: the next tile's descriptor, cells and stencil weights are
-// fetched while the current tile is solved and stored.  In place
-// (`clustered`), the grid has one CTA per tile and the segments of a line
-// form a cluster: every CTA arrives once its staging reads have landed and
-// waits before its store.
-template <typename T>
-__global__ void __launch_bounds__(NTH, 2)
-    sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
-                        double toff, void *data_override, int lc_max, int H, unsigned *status,
-                        int jstep, int nslice, const int *nlo, int cs, int clustered,
-                        int total) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  auto stage = [&](int which) { return filt_stage<T>(smem_raw, lc_max, H, which); };
-  auto issue = [&](FiltStage<T> sg, const FiltTile &tt, double tf, bool xv) {
-    const void *vs;
-    void *vd;
-    field_io(*sg.fd, jstep, &vs, &vd);
-    if (xv) filt_stage_tile<T, FP_X>(sg, tt, reinterpret_cast<const T *>(vs), tf);
-    else filt_stage_tile<T, FP_Y>(sg, tt, reinterpret_cast<const T *>(vs), tf);
-  };
-  int cur = (int)blockIdx.x;
-  if (cur >= total) return;
-  int fi = 0;  // field of the latest tile: binary search once, then advance
-  {
-    int lo = 0, hi = nfields - 1;
-    const int cta = cur + group_base;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (__ldg(&fields[mid].cta0) <= cta) lo = mid; else hi = mid - 1;
-    }
-    fi = lo;
-  }
-  int held0 = -1, held1 = -1;  // field whose descriptor each stage holds
-  double tf = 0.0;
-  bool act = filt_desc<T>(fields, fi, held0, data_override, jstep, nslice, nlo, tf, toff,
-                          stage(0));
-  FiltTile tl{};
-  bool xv = false;
-  if (act) {
-    const FiltStage<T> s0 = stage(0);
-    tl = filt_tile(*s0.fd, cur + group_base, cs, clustered != 0);
-    xv = filt_xvec<T>(*s0.fd, jstep);
-    issue(s0, tl, tf, xv);
-  }
-  cp_async_commit();
-  int b = 0;
-  while (true) {
-    const int nxt = cur + (int)gridDim.x;
-    bool nact = false, nxv = false;
-    FiltTile nt{};
-    if (nxt < total) {
-      const FiltStage<T> sn = stage(b ^ 1);
-      fi = filt_field(fields, nfields, fi, nxt + group_base);
-      int h = b ? held0 : held1;
-      nact = filt_desc<T>(fields, fi, h, data_override, jstep, nslice, nlo, tf, toff, sn);
-      if (b) held0 = h; else held1 = h;
-      if (nact) {
-        nt = filt_tile(*sn.fd, nxt + group_base, cs, clustered != 0);
-        nxv = filt_xvec<T>(*sn.fd, jstep);
-        issue(sn, nt, tf, nxv);
-      }
-    }
-    cp_async_commit();
-    cp_async_wait_prior1();
-    __syncthreads();
-    if (act) {
-      const FiltStage<T> sc = stage(b);
-      if (clustered) asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
-      if (tl.np + 2 * sc.fd->jf > FLANES * FCH) {  // the host keeps segments shorter
-        if (threadIdx.x == 0) atomicOr(status, STATUS_HALO);
-      } else if (xv) {
-        filt_solve<T, FP_X>(sc, tl, status);
-      } else {
-        filt_solve<T, FP_Y>(sc, tl, status);
-      }
-      __syncthreads();
-      if (clustered) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
-      const void *vs;
-      void *vd;
-      field_io(*sc.fd, jstep, &vs, &vd);
-      if (xv) filt_store<T, FP_X>(sc, tl, reinterpret_cast<T *>(vd));
-      else filt_store<T, FP_Y>(sc, tl, reinterpret_cast<T *>(vd));
-    }
-    if (nxt >= total) break;
-    __syncthreads();  // stage b is free for the tile after next
-    cur = nxt;
-    act = nact;
-    xv = nxv;
-    tl = nt;
-    b ^= 1;
-  }
-  cp_async_wait_all_committed();
 }
 
 }  // namespace
@@ -1595,7 +1414,8 @@ size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source) {
 }
 
 size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64) {
-  return 2 * filter_stage_bytes(lc_max, halo, fp64 ? 8 : 4);  // two pipeline stages
+  size_t el = fp64 ? 8 : 4;
+  return FD_BYTES + 64 * sizeof(int) + (6 * (size_t)LPG + (size_t)(lc_max + 2 * halo) * PITCH) * el;
 }
 
 int filter_segment_max(int J) { return filter_seg_max(J); }
@@ -1632,33 +1452,10 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   }
   if (groups_total <= 0) return cudaSuccess;
   if (filt && (cs == 1 || !inplace)) {  // whole lines per CTA, or out of place: no cluster
-    // persistent: as many CTAs as fit on the device, each looping over tiles
-    const int total = groups_total * cs;
-    int resident = 0;
-    {
-      static std::mutex mu;
-      static std::map<std::pair<int, size_t>, int> cache;  // (device, smem) -> CTAs on the device
-      int dev = 0;
-      cudaError_t e = cudaGetDevice(&dev);
-      if (e != cudaSuccess) return e;
-      std::lock_guard<std::mutex> lk(mu);
-      auto it = cache.find({dev, smem});
-      if (it == cache.end()) {
-        int sms = 0, per_sm = 0;
-        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess)
-          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_filter_kernel<T>, NTH,
-                                                            smem);
-        if (e != cudaSuccess) return e;
-        it = cache.emplace(std::make_pair(dev, smem), std::max(1, per_sm) * std::max(1, sms)).first;
-      }
-      resident = it->second;
-    }
-    const int grid = std::max(1, std::min(total, resident));
     count_launch();
-    sweep_filter_kernel<T><<<(unsigned)grid, NTH, smem, stream>>>(
+    sweep_filter_kernel<T><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
         d_fields, nfields, group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
-        nlo, cs, 0, total);
+        nlo, cs, 0);
     return cudaGetLastError();
   }
   cudaLaunchConfig_t cfg = {};
@@ -1676,8 +1473,7 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   count_launch();
   if (filt)  // group_base in CTAs
     return cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T>, d_fields, nfields, group_base * cs,
-                              toff, data, lc_max, halo, d_status, jstep, nslice, nlo, cs, 1,
-                              groups_total * cs);
+                              toff, data, lc_max, halo, d_status, jstep, nslice, nlo, cs, 1);
   if (fast)
     return cudaLaunchKernelEx(&cfg, sweep_fast_kernel<T>, d_fields, nfields, group_base, toff,
                               data, lc_max, halo, d_status, jstep, nslice, nlo);
