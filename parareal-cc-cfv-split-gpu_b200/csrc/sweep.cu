@@ -32,8 +32,6 @@
 #include <cooperative_groups.h>
 
 #include <climits>
-#include <map>
-#include <mutex>
 #include <cstdio>
 
 #include "ccfv_internal.h"
