@@ -302,8 +302,9 @@ int ccfv_step_noalloc(const ccfv_grid *grid, double *d_C, double tn, double dt, 
  * lengths (process-wide).  *segment (optional) receives the choice. */
 int ccfv_autotune(ccfv_ctx *ctx, double dt, int precision, int *segment, void *stream);
 
-/* Which sweep kernel each sub-step of a step of dt runs (introspection; no
- * counterpart in the reference): variant[s] for s = x(dt/2), y(dt), x(dt/2)
+/* Which sweep kernel each sub-step of a step of dt runs in ccfv_step /
+ * ccfv_run and the Parareal engines (introspection; no counterpart in the
+ * reference): variant[s] for s = x(dt/2), y(dt), x(dt/2)
  * is CCFV_SWEEP_GENERAL (per-cell feet), CCFV_SWEEP_UNIFORM (shared-foot
  * stencil with exact chunked scans), CCFV_SWEEP_FILTER (shared-foot stencil
  * with the factored cyclic solve) or CCFV_SWEEP_SOURCE (per-cell, with the

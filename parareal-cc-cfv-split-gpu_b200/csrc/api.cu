@@ -227,7 +227,8 @@ int ccfv_sweep_plan(ccfv_ctx *ctx, double dt, int precision, int variant[3], int
     const int dir = kind == 1 ? 1 : 0;
     const double Dt = kind == 1 ? dt : 0.5 * dt;
     const int dsrc = (kind == 2 && ctx->grid.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
-    const LaunchGeom G = step_geom(ctx->grid, dir, Dt, dsrc, precision == CCFV_FP64);
+    // as ccfv_step/ccfv_run and the Parareal engines sweep: out of place
+    const LaunchGeom G = step_geom(ctx->grid, dir, Dt, dsrc, precision == CCFV_FP64, false);
     if (variant)
       variant[kind] = (ctx->force_general && G.variant != SWEEP_GENERAL_SRC) ? SWEEP_GENERAL : G.variant;
     if (segment) segment[kind] = G.lc_max;

@@ -170,12 +170,10 @@ def test_periodic_solver_variants_match_oracle(oracle, ccfv, K, nx):
     assert rel_l2(host(c), ref) < TOL
 
 
-@pytest.mark.parametrize("K", [1e-4, 1e-3])
-def test_periodic_filter_clusters_2048_match_oracle(oracle, ccfv, K):
-    """Filter kernel with 8 segments per line (one thread-block cluster per
-    16-line tile): the in-place sweep must not let a segment store before
-    its neighbours have staged their halos."""
-    nx = 2048
+@pytest.mark.parametrize("nx,K", [(2048, 1e-4), (2048, 1e-3), (4096, 1e-3)])
+def test_periodic_filter_segments_match_oracle(oracle, ccfv, nx, K):
+    """Filter kernel with 9 and 18 segments per line: single-field calls
+    sweep out of place, so no segment reads what another one writes."""
     vp = (0.9, -1.7)
     dt = 0.8 / nx / 1.7
     C0 = periodic_field(nx, 22)
