@@ -54,11 +54,12 @@ def parse():
     ap.add_argument("--form", default="delta", choices=["standard", "delta"])
     ap.add_argument("--cpu-sample-s", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "step"],
+    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "step", "split"],
                     help="plain: one instance (default workload); batch: a mixed batch of "
                          "instances in shared launches; serve: Poisson arrivals through the "
                          "continuous-batching server; step: serial fine time-stepping of the "
-                         "workload's field (the sweep kernels alone)")
+                         "workload's field (the sweep kernels alone); split: the precision-split "
+                         "case (swirl, 128 slices): FP32 vs FP64 coarse against the serial fine")
     ap.add_argument("--inner", type=int, default=16,
                     help="step mode: fine steps per timed step")
     ap.add_argument("--instances", type=int, default=256)
@@ -681,6 +682,61 @@ def run_step(a, w, ws, rank, local):
             cpu_baseline=cpu, clocks=ck, gpu_launches=launches)))
 
 
+def run_split(a, ws, rank, local):
+    """Precision split: swirling deformation (T = 1.5), nu = 1e-4, four seeded
+    Gaussians, 128 slices, coarse dt = 8 x fine; Parareal with FP32 and with
+    FP64 coarse steps against the serial fine solve (iterations to the
+    tolerance, final error, rate).  Grid side from --n."""
+    import torch
+    import ccfv
+    torch.cuda.set_device(local)
+    N, S, ratio, T, nu = a.n, 128, 8, 1.5, 1e-4
+    dt = 0.8 / N  # swirl speed <= 1
+    nt = int(np.ceil(T / dt / (S * ratio))) * S * ratio
+    rng = np.random.default_rng(a.seed)
+    gs = [[float(rng.uniform(0.25, 0.75)), float(rng.uniform(0.25, 0.75)),
+           2.0 * float(rng.uniform(0.03, 0.1)) ** 2, 1.0] for _ in range(4)]
+    g = ccfv.make_grid(N, bc=ccfv.BC_PERIODIC, velocity=ccfv.VEL_SWIRL, vel_params=(T,), K=nu,
+                       scheme=ccfv.SCHEME_CONSISTENT)
+    s = ccfv.Solver(g, local)
+    C0 = torch.empty(N, N, dtype=torch.float64, device=f"cuda:{local}")
+    s.gaussians(C0, gs, images=1)
+    fine = C0.clone()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    s.run(fine, 0.0, T / nt, nt)
+    e1.record()
+    torch.cuda.synchronize()
+    serial_ms = e0.elapsed_time(e1)
+    res = {}
+    out = torch.empty_like(C0)
+    for name, prec in (("fp64", ccfv.FP64), ("fp32", ccfv.FP32)):
+        e0.record()
+        _, st = s.parareal(C0, out, t0=0.0, t1=T, nt_fine=nt, n_slices=S, coarse_ratio=ratio,
+                           tol=1e-10, kmax=a.kmax, coarse_precision=prec, form=ccfv.FORM_DELTA)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        res[name] = dict(iterations=st["iterations"], converged=st["converged"],
+                         final_update=st["update"][-1] if st["update"] else None,
+                         l2_err_vs_serial_fine=float(torch.linalg.norm(out - fine) /
+                                                     torch.linalg.norm(fine)),
+                         cell_updates_per_s=N * N * nt / (ms * 1e-3), ms=ms,
+                         update=[float("%.3g" % u) for u in st["update"]])
+    if rank == 0:
+        print(json.dumps(dict(
+            metric="parareal_cell_updates_per_s", value=res["fp32"]["cell_updates_per_s"],
+            unit="cell-updates/s", mode="split", n_gpus=ws, steps=1, warmup=0,
+            higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64+f32",
+            data="synthetic",
+            config={"workload": f"precision split: periodic {N}^2, swirling deformation T=1.5, "
+                                f"nu=1e-4, 4 seeded Gaussians, Nt={nt}, 128 slices, coarse dt = "
+                                f"8 x fine, delta form, tol 1e-10 (cap {a.kmax})",
+                    "seed": a.seed},
+            serial_fine_cell_updates_per_s=N * N * nt / (serial_ms * 1e-3),
+            fp32_coarse=res["fp32"], fp64_coarse=res["fp64"])))
+
+
 def main():
     a = parse()
     w = workload(a)
@@ -694,6 +750,8 @@ def main():
             run_serve(a, ws, rank, local)
         elif a.mode == "step":
             run_step(a, w, ws, rank, local)
+        elif a.mode == "split":
+            run_split(a, ws, rank, local)
         else:
             run_ours(a, w, ws, rank, local)
     finally:
