@@ -78,6 +78,40 @@ __device__ __forceinline__ double edge_foot(const SweepField &f, int e, double t
   return 0.5 * (corner_foot(f, s, tau0, ta, tb) + corner_foot(f, s, tau1, ta, tb));
 }
 
+// Edge feet of one line.  The swirling field factors as
+// sin^2(pi s) g(tau) h(t): its line factors g(tau0), g(tau1) and time factors
+// h(ta), h(tb) are computed once per line, and sin^2(pi s) at the edge is
+// shared by both corners, so an edge foot costs three sinpi instead of
+// twelve transcendental calls.  Other fields use edge_foot.
+struct LineFeet {
+  double tau0, tau1, ta, tb;
+  bool swirl;
+  double a0a = 0, a0b = 0, a1a = 0, a1b = 0;  // along-line speed factors: corner line, time
+  __device__ __forceinline__ LineFeet(const SweepField &f, double tau0_, double tau1_, double ta_,
+                                      double tb_)
+      : tau0(tau0_), tau1(tau1_), ta(ta_), tb(tb_), swirl(f.vel == VEL_SWIRL) {
+    if (swirl) {
+      const double sg = f.dir == 0 ? 1.0 : -1.0;
+      const double ca = cospi(ta / f.vp[0]), cb = cospi(tb / f.vp[0]);
+      const double g0 = sg * sinpi(2.0 * tau0), g1 = sg * sinpi(2.0 * tau1);
+      a0a = g0 * ca;
+      a0b = g0 * cb;
+      a1a = g1 * ca;
+      a1b = g1 * cb;
+    }
+  }
+  __device__ __forceinline__ double foot(const SweepField &f, int e) const {
+    if (!swirl) return edge_foot(f, e, tau0, tau1, ta, tb);
+    const double s = f.s_min + f.h * e;
+    const double ss = sinpi(s), s2 = ss * ss;
+    const double w0 = a0b * s2, w1 = a1b * s2;  // speed at the corners at tb
+    const double q0 = sinpi(s - f.Dt * w0), q1 = sinpi(s - f.Dt * w1);
+    const double c0 = s - 0.5 * f.Dt * (w0 + a0a * q0 * q0);
+    const double c1 = s - 0.5 * f.Dt * (w1 + a1a * q1 * q1);
+    return 0.5 * (c0 + c1);
+  }
+};
+
 // Whether a field takes part in a batched launch, and its launch time offset.
 __device__ __forceinline__ bool field_active(const SweepField &f, int jstep, int nslice,
                                              const int *nlo) {
@@ -462,6 +496,7 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
     const double tau0 = F.t_min + F.ht * (double)gl;
     const double tau1 = F.t_min + F.ht * (double)(gl + 1);
     const double ta = toff + F.ta_rel, tb = toff + F.tb_rel;
+    const LineFeet lf(F, tau0, tau1, ta, tb);
     const T kbc = T(F.kb);
     // Uniform displacement: every edge foot of this line sits at e - sigma
     // (position units), -sigma = n0 + xi0.  Remap, foot derivative and RHS
@@ -472,7 +507,7 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
     int n0 = 0, klo = 1, khi = 0;
     T w[6], qd[6];
     if (stencil) {
-      const double f0 = edge_foot(F, 0, tau0, tau1, ta, tb);
+      const double f0 = lf.foot(F, 0);
       const double u = (f0 - F.s_min) / F.h;
       const double fl = floor(u);
       n0 = (int)fl;
@@ -515,17 +550,17 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
               for (int t = 0; t < 6; ++t) bk += (w[t] + qd[t]) * cp[t * PITCH];
             }
           } else {
-            double fa = edge_foot(F, k, tau0, tau1, ta, tb);
-            double fb = edge_foot(F, k + 1, tau0, tau1, ta, tb);
+            double fa = lf.foot(F, k);
+            double fb = lf.foot(F, k + 1);
             bk = remap_cell(F, v, fa, fb) + kbc * (foot_derivative(F, v, fb) - foot_derivative(F, v, fa));
           }
           bArr[(k - p0 + H) * PITCH + ln] = bk;
         }
       } else if (kb < ke) {
-        double fprev = edge_foot(F, kb, tau0, tau1, ta, tb);
+        double fprev = lf.foot(F, kb);
         T dprev = foot_derivative(F, v, fprev);
         for (int k = kb; k < ke; ++k) {
-          double fnext = edge_foot(F, k + 1, tau0, tau1, ta, tb);
+          double fnext = lf.foot(F, k + 1);
           T dnext = foot_derivative(F, v, fnext);
           T ic = remap_cell(F, v, fprev, fnext);
           T bk = ic + kbc * (dnext - dprev);
@@ -556,8 +591,8 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
             for (int t = 0; t < 6; ++t) ik += w[t] * cp[t * PITCH];
           }
         } else {
-          double fa = edge_foot(F, k, tau0, tau1, ta, tb);
-          double fb = edge_foot(F, k + 1, tau0, tau1, ta, tb);
+          double fa = lf.foot(F, k);
+          double fb = lf.foot(F, k + 1);
           ik = remap_cell(F, v, fa, fb);
         }
         R[(k - p0 + H) * PITCH + ln] = ik;
@@ -581,8 +616,8 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
             bk = vr(k) + acc;
           }
         } else {
-          double fa = edge_foot(F, k, tau0, tau1, ta, tb);
-          double fb = edge_foot(F, k + 1, tau0, tau1, ta, tb);
+          double fa = lf.foot(F, k);
+          double fb = lf.foot(F, k + 1);
           bk = vr(k) + kbc * (foot_derivative(F, vr, fb) - foot_derivative(F, vr, fa));
           if (F.src) bk += src_term(k, fa, fb);
         }
