@@ -1218,42 +1218,49 @@ __global__ void __launch_bounds__(NTH, 2)
     gdst = reinterpret_cast<T *>(vd);
   }
 
+  // Descriptor fields used in the loops live in registers: the descriptor is
+  // in shared memory, and the copies' memory clobbers and the generic-pointer
+  // stores would otherwise make the compiler reload it every iteration.
+  const long long s_pos = F.s_pos, s_line = F.s_line, M = F.M;
+  const bool xsweep = s_line == 1;
+
   // ---- stage rows p0-H .. p1+H-1 (periodic wrap) ----
-  if (F.s_line == 1) {
+  if (xsweep) {
     const int ln = lane & (LPG - 1);
     const long long gl = line0 + ln;
-    const bool okl = gl < F.M;
-    for (int row = warp * 2 + (lane >> 4); row < nrows; row += 2 * NW) {
-      int pos = p0 - H + row;
-      if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
-        pos %= L;
-        if (pos < 0) pos += L;
-      }
-      T *dst = S.C + row * PITCH + ln;
-      if (okl) {
-        const T *src = gsrc + (long long)pos * F.s_pos + gl;
-        if (sizeof(T) == 8) cp_async8(dst, src); else cp_async4(dst, src);
-      } else {
-        *dst = T(0);
-      }
-    }
-  } else {
-    for (int ln = warp; ln < LPG; ln += NW) {
-      const long long gl = line0 + ln;
-      const bool okl = gl < F.M;
-      const T *lbase = gsrc + gl * F.s_line;
-      for (int row = lane; row < nrows; row += 32) {
+    T *dcol = S.C + ln;
+    const int row0 = warp * 2 + (lane >> 4);
+    if (gl < M) {
+      const T *gcol = gsrc + gl;
+      for (int row = row0; row < nrows; row += 2 * NW) {
         int pos = p0 - H + row;
         if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
           pos %= L;
           if (pos < 0) pos += L;
         }
-        T *dst = S.C + row * PITCH + ln;
-        if (okl) {
-          if (sizeof(T) == 8) cp_async8(dst, lbase + pos); else cp_async4(dst, lbase + pos);
-        } else {
-          *dst = T(0);
+        const T *src = gcol + (long long)pos * s_pos;
+        if (sizeof(T) == 8) cp_async8(dcol + row * PITCH, src); else cp_async4(dcol + row * PITCH, src);
+      }
+    } else {
+      for (int row = row0; row < nrows; row += 2 * NW) dcol[row * PITCH] = T(0);
+    }
+  } else {
+    for (int ln = warp; ln < LPG; ln += NW) {
+      const long long gl = line0 + ln;
+      T *dcol = S.C + ln;
+      if (gl < M) {
+        const T *lbase = gsrc + gl * s_line;
+        for (int row = lane; row < nrows; row += 32) {
+          int pos = p0 - H + row;
+          if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
+            pos %= L;
+            if (pos < 0) pos += L;
+          }
+          if (sizeof(T) == 8) cp_async8(dcol + row * PITCH, lbase + pos);
+          else cp_async4(dcol + row * PITCH, lbase + pos);
         }
+      } else {
+        for (int row = lane; row < nrows; row += 32) dcol[row * PITCH] = T(0);
       }
     }
   }
@@ -1421,18 +1428,27 @@ __global__ void __launch_bounds__(NTH, 2)
   if (clustered) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
 
   // ---- cooperative store of rows H .. H+np-1 ----
-  if (F.s_line == 1) {
+  if (xsweep) {
     const int l = lane & (LPG - 1);
     const long long gl = line0 + l;
-    if (gl < F.M)
-      for (int row = warp * 2 + (lane >> 4); row < np; row += 2 * NW)
-        gdst[(long long)(p0 + row) * F.s_pos + gl] = S.C[(row + H) * PITCH + l];
+    if (gl < M) {
+      const int row0 = warp * 2 + (lane >> 4);
+      T *gp = gdst + (long long)(p0 + row0) * s_pos + gl;
+      const T *sp = S.C + (row0 + H) * PITCH + l;
+      const long long gstep = 2LL * NW * s_pos;
+      for (int row = row0; row < np; row += 2 * NW) {
+        *gp = *sp;
+        gp += gstep;
+        sp += 2 * NW * PITCH;
+      }
+    }
   } else {
     for (int l2 = warp; l2 < LPG; l2 += NW) {
       const long long gl2 = line0 + l2;
-      if (gl2 >= F.M) continue;
-      T *lbase = gdst + gl2 * F.s_line + p0;
-      for (int row = lane; row < np; row += 32) lbase[row] = S.C[(row + H) * PITCH + l2];
+      if (gl2 >= M) continue;
+      T *lbase = gdst + gl2 * s_line + p0;
+      const T *scol = S.C + H * PITCH + l2;
+      for (int row = lane; row < np; row += 32) lbase[row] = scol[row * PITCH];
     }
   }
 }
