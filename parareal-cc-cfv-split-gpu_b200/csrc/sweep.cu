@@ -1144,12 +1144,21 @@ constexpr int FLANES = 16;
 // Longest segment for a recurrence warm-up J: 16 * FCH >= np + 2J.
 __host__ __device__ constexpr int filter_seg_max(int J) { return FLANES * FCH - 2 * J; }
 
+// Rows of the staged tile: enough for the longest chunk walk, so the solve
+// loops need no bounds predicates (rows past the staged ones are only read
+// by lanes whose positions lie past the range; their values are masked).
+__host__ __device__ inline int filter_tile_rows(int lc_max, int H) {
+  return (lc_max > FLANES * FCH ? lc_max : FLANES * FCH) + 2 * H + 8;
+}
+
 template <typename T>
 struct FiltSmem {
-  T *C;      // [(lc_max + 2H) * PITCH]  input cells, then w, then x
-  T *om;     // [6 * LPG]
+  T *C;      // [filter_tile_rows * PITCH]  input cells, then w, then x
+  T *om;     // [8 * LPG]  weights of w's input (1/c) M b as an 8-tap stencil of C
+  T *pwt;    // [32]       (-mu)^(i+1), i = 0 .. FCH-1
   int *n0;   // [LPG]
   SweepField *fd;
+  int rows;
 };
 
 template <typename T>
@@ -1158,8 +1167,10 @@ __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max
   s.fd = reinterpret_cast<SweepField *>(raw);
   s.n0 = reinterpret_cast<int *>(raw + FD_BYTES);
   T *p = reinterpret_cast<T *>(raw + FD_BYTES + 64 * sizeof(int));
-  s.om = p; p += 6 * LPG;
+  s.om = p; p += 8 * LPG;
+  s.pwt = p; p += 32;
   s.C = p;
+  s.rows = filter_tile_rows(lc_max, H);
   return s;
 }
 
@@ -1282,13 +1293,31 @@ __global__ void __launch_bounds__(NTH, 2)
     const double pz = 12.0 * x3 - 18.0 * x2 - 24.0 * x + 15.0;
     const double pp1 = -8.0 * x3 + 6.0 * x2 + 18.0 * x - 1.0;
     const double pp2 = 2.0 * x3 - 3.0 * x;
-    T *om = S.om + 6 * l;
-    om[0] = T(A / 12.0 - kq * pm2);
-    om[1] = T((B - 8.0 * A) / 12.0 + kq * (pm2 - pm1));
-    om[2] = T(1.0 - Cc - 2.0 * B / 3.0 + kq * (pm1 - pz));
-    om[3] = T(Cc + 2.0 * A / 3.0 + kq * (pz - pp1));
-    om[4] = T((8.0 * B - A) / 12.0 + kq * (pp1 - pp2));
-    om[5] = T(-B / 12.0 + kq * pp2);
+    // b_k = sum_{j<6} o_j C_{k+n0-2+j}; the input of w is (1/c) M b with
+    // M b_k = (b_{k-1} + 10 b_k + b_{k+1}) / 12 = sum_{m=-3..4} W_m C_{k+n0+m}
+    double o[6];
+    o[0] = A / 12.0 - kq * pm2;
+    o[1] = (B - 8.0 * A) / 12.0 + kq * (pm2 - pm1);
+    o[2] = 1.0 - Cc - 2.0 * B / 3.0 + kq * (pm1 - pz);
+    o[3] = Cc + 2.0 * A / 3.0 + kq * (pz - pp1);
+    o[4] = (8.0 * B - A) / 12.0 + kq * (pp1 - pp2);
+    o[5] = -B / 12.0 + kq * pp2;
+    const double icw = F.sm_inv_den / 12.0;
+    T *om = S.om + 8 * l;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {  // tap m - 3
+      const double from_bm = m < 6 ? o[m] : 0.0;                  // b_{k-1}
+      const double from_bc = (m >= 1 && m < 7) ? o[m - 1] : 0.0;  // b_k
+      const double from_bp = m >= 2 ? o[m - 2] : 0.0;             // b_{k+1}
+      om[m] = T(icw * (from_bm + 10.0 * from_bc + from_bp));
+    }
+  } else if (threadIdx.x == LPG) {
+    const T mmu = T(-F.sm_fac);
+    T pk = mmu;
+    for (int i = 0; i < FCH; ++i) {
+      S.pwt[i] = pk;
+      pk *= mmu;
+    }
   }
   cp_async_wait_all_committed();
   __syncthreads();
@@ -1299,130 +1328,106 @@ __global__ void __launch_bounds__(NTH, 2)
   if (clustered) asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
 
   // ---- one line per half-warp, FCH positions per lane ----
-  const int c = lane & (FLANES - 1);
-  const int ln = warp * 2 + (lane >> 4);
-  const unsigned hmask = 0xffffffffu;  // the warp is converged at every shuffle
-  T *col = S.C + ln;  // this line's column: row r at col[r * PITCH]
-  const int rb = H - p0;  // row of position 0
-  const T mmu = -mu;
-  T pw = T(1);  // (-mu)^FCH
-#pragma unroll
-  for (int i = 0; i < FCH; ++i) pw *= mmu;
-
-  // forward: w over [qa, qb) = [p0 - J, p1 + J), M b from the staged cells
-  const int qb = p1 + J;
   if (np + 2 * J > FLANES * FCH) {  // the host keeps segments within filter_seg_max(J)
     if (threadIdx.x == 0) atomicOr(status, STATUS_HALO);
     return;
   }
-  const int k0 = p0 - J + c * FCH;
-  T v[FCH];
   {
-    const int n0 = S.n0[ln];
-    const T *omp = S.om + 6 * ln;
-    const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5];
-    // b needs rows k + n0 - 2 .. k + n0 + 3 for k = k0 - 1 .. min(k0 + FCH, qb)
-    const int klast = min(k0 + FCH, qb);
-    const int r0 = k0 - 1 + n0 - 2 + rb;
-    const int rlast = klast + n0 + 3 + rb;
-    bool ok = k0 < qb;
-    if (ok && (r0 < 0 || rlast >= nrows)) {
-      atomicOr(status, STATUS_HALO);
-      ok = false;
-    }
-    T w = T(0);
-    if (ok) {
-      const T *cp = col + r0 * PITCH;
+    const int c = lane & (FLANES - 1);
+    const int ln = warp * 2 + (lane >> 4);
+    const unsigned fm = 0xffffffffu;  // the warp is converged at every shuffle
+    const int rb = H - p0;            // row of position 0
+    const T mmu = -mu;
+    const T pw = S.pwt[FCH - 1];      // (-mu)^FCH
+
+    // forward: w_k = (1/c) M b_k - mu w_{k-1} over [p0 - J, qb), qb = p1 + J.
+    // Lanes past qb walk stage rows that are allocated but not staged: their
+    // values only flow further right and are masked by the backward load.
+    const int qb = p1 + J;
+    const int k0 = p0 - J + c * FCH;
+    const int r0 = k0 + S.n0[ln] - 3 + rb;  // row of tap -3 of position k0
+    const bool ok = r0 >= 0 && r0 + FCH + 7 <= S.rows;
+    if (!ok) atomicOr(status, STATUS_HALO);
+    T v[FCH];
+    {
+      const T *omp = S.om + 8 * ln;
+      const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5],
+              o6 = omp[6], o7 = omp[7];
+      const T *cp = S.C + (ok ? r0 : 0) * PITCH + ln;
       T w0 = cp[0], w1 = cp[PITCH], w2 = cp[2 * PITCH], w3 = cp[3 * PITCH], w4 = cp[4 * PITCH],
-        w5 = cp[5 * PITCH];
-      T bm = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
-      w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[6 * PITCH];
-      T bc = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
-      const int nin = klast - k0;  // positions of this chunk inside the range
+        w5 = cp[5 * PITCH], w6 = cp[6 * PITCH];
+      T w = T(0);
 #pragma unroll
       for (int i = 0; i < FCH; ++i) {
-        T mb = T(0);
-        if (i < nin) {
-          w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = cp[(7 + i) * PITCH];
-          const T bp = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5;
-          mb = (bp + T(10.0) * bc + bm) * T(1.0 / 12.0);
-          bm = bc;
-          bc = bp;
-        }
-        w = ic * mb + mmu * w;
+        const T w7 = cp[(7 + i) * PITCH];
+        const T mb = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5 + o6 * w6 + o7 * w7;
+        w = mb + mmu * w;
         v[i] = w;
+        w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6; w6 = w7;
       }
-    } else {
+      // carries: chunk map x -> pw x + e_c, inclusive scan over the line's lanes
+      T sa = pw, sb = v[FCH - 1];
 #pragma unroll
-      for (int i = 0; i < FCH; ++i) v[i] = T(0);
-    }
-    // carries: chunk map x -> pw x + e_c, inclusive scan over the line's lanes
-    T sa = pw, sb = v[FCH - 1];
-#pragma unroll
-    for (int d = 1; d < FLANES; d <<= 1) {
-      const T pa = __shfl_up_sync(hmask, sa, d, FLANES);
-      const T pb = __shfl_up_sync(hmask, sb, d, FLANES);
-      if (c >= d) {
-        sb = sa * pb + sb;
-        sa = sa * pa;
+      for (int d = 1; d < FLANES; d <<= 1) {
+        const T pa = __shfl_up_sync(fm, sa, d, FLANES);
+        const T pb = __shfl_up_sync(fm, sb, d, FLANES);
+        if (c >= d) {
+          sb = sa * pb + sb;
+          sa = sa * pa;
+        }
       }
-    }
-    T cin = __shfl_up_sync(hmask, sb, 1, FLANES);
-    if (c == 0) cin = T(0);
-    T pk = mmu;
+      T cin = __shfl_up_sync(fm, sb, 1, FLANES);
+      if (c == 0) cin = T(0);
 #pragma unroll
-    for (int i = 0; i < FCH; ++i) {
-      v[i] += cin * pk;
-      pk *= mmu;
+      for (int i = 0; i < FCH; ++i) v[i] += cin * S.pwt[i];
     }
-  }
-  // every stencil read of this line is done (the shuffles order the lanes)
-  __syncwarp(hmask);
+    // every stencil read of this line is done (the shuffles order the lanes);
+    // w of positions k0 .. k0+FCH-1 into this line's column
+    __syncwarp(fm);
+    {
+      T *wp = S.C + (k0 + rb) * PITCH + ln;
 #pragma unroll
-  for (int i = 0; i < FCH; ++i) {
-    const int k = k0 + i;
-    if (k >= p0 && k < qb) col[(k + rb) * PITCH] = v[i];
-  }
-  __syncwarp(hmask);
+      for (int i = 0; i < FCH; ++i) wp[i * PITCH] = v[i];
+    }
+    __syncwarp(fm);
 
-  // backward: x over [p0, qb), zero start at qb
-  const int k1 = p0 + c * FCH;
-  {
+    // backward: x over [p0, qb), zero start at qb
+    const int k1 = p0 + c * FCH;
+    {
+      const T *xp = S.C + (k1 + rb) * PITCH + ln;
+      const int nb = qb - k1;
 #pragma unroll
-    for (int i = 0; i < FCH; ++i) {
-      const int k = k1 + i;
-      v[i] = (k < qb) ? col[(k + rb) * PITCH] : T(0);
-    }
-    T x = T(0);
-#pragma unroll
-    for (int i = FCH - 1; i >= 0; --i) {
-      x = v[i] + mmu * x;
-      v[i] = x;
-    }
-    T sa = pw, sb = v[0];
-#pragma unroll
-    for (int d = 1; d < FLANES; d <<= 1) {
-      const T pa = __shfl_down_sync(hmask, sa, d, FLANES);
-      const T pb = __shfl_down_sync(hmask, sb, d, FLANES);
-      if (c + d < FLANES) {
-        sb = sa * pb + sb;
-        sa = sa * pa;
+      for (int i = 0; i < FCH; ++i) {
+        const T val = xp[i * PITCH];
+        v[i] = (i < nb) ? val : T(0);
       }
-    }
-    T cin = __shfl_down_sync(hmask, sb, 1, FLANES);
-    if (c == FLANES - 1) cin = T(0);
-    T pk = mmu;
+      T x = T(0);
 #pragma unroll
-    for (int i = FCH - 1; i >= 0; --i) {
-      v[i] += cin * pk;
-      pk *= mmu;
-    }
-  }
-  __syncwarp(hmask);
+      for (int i = FCH - 1; i >= 0; --i) {
+        x = v[i] + mmu * x;
+        v[i] = x;
+      }
+      T sa = pw, sb = v[0];
 #pragma unroll
-  for (int i = 0; i < FCH; ++i) {
-    const int k = k1 + i;
-    if (k < p1) col[(k + rb) * PITCH] = v[i];
+      for (int d = 1; d < FLANES; d <<= 1) {
+        const T pa = __shfl_down_sync(fm, sa, d, FLANES);
+        const T pb = __shfl_down_sync(fm, sb, d, FLANES);
+        if (c + d < FLANES) {
+          sb = sa * pb + sb;
+          sa = sa * pa;
+        }
+      }
+      T cin = __shfl_down_sync(fm, sb, 1, FLANES);
+      if (c == FLANES - 1) cin = T(0);
+#pragma unroll
+      for (int i = 0; i < FCH; ++i) v[i] += cin * S.pwt[FCH - 1 - i];
+    }
+    __syncwarp(fm);
+    {
+      T *xp = S.C + (k1 + rb) * PITCH + ln;
+#pragma unroll
+      for (int i = 0; i < FCH; ++i) xp[i * PITCH] = v[i];
+    }
   }
   __syncthreads();
   if (clustered) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
@@ -1464,7 +1469,8 @@ size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source) {
 
 size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64) {
   size_t el = fp64 ? 8 : 4;
-  return FD_BYTES + 64 * sizeof(int) + (6 * (size_t)LPG + (size_t)(lc_max + 2 * halo) * PITCH) * el;
+  return FD_BYTES + 64 * sizeof(int) +
+         (8 * (size_t)LPG + 32 + (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el;
 }
 
 int filter_segment_max(int J) { return filter_seg_max(J); }
