@@ -1174,8 +1174,10 @@ __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max
   return s;
 }
 
+// Three CTAs per SM (at most 85 registers a thread): the kernel is latency
+// bound, and the third CTA is worth more than the few registers it spills.
 template <typename T>
-__global__ void __launch_bounds__(NTH, 2)
+__global__ void __launch_bounds__(NTH, 3)
     sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
                         double toff, void *data_override, int lc_max, int H, unsigned *status,
                         int jstep, int nslice, const int *nlo, int cs, int clustered) {
