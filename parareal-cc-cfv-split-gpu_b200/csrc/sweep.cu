@@ -1174,10 +1174,12 @@ __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max
   return s;
 }
 
-// Three CTAs per SM (at most 85 registers a thread): the kernel is latency
-// bound, and the third CTA is worth more than the few registers it spills.
+// Four CTAs per SM (at most 64 registers a thread; shared memory allows no
+// more): the kernel is latency bound, and each added CTA was worth more than
+// the few registers it spills (2 -> 3 -> 4 CTAs: fine phase 1498 -> 1207 ->
+// 1105 us per launch on the 2048^2 x 63-slice bench).
 template <typename T>
-__global__ void __launch_bounds__(NTH, 3)
+__global__ void __launch_bounds__(NTH, 4)
     sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
                         double toff, void *data_override, int lc_max, int H, unsigned *status,
                         int jstep, int nslice, const int *nlo, int cs, int clustered) {
