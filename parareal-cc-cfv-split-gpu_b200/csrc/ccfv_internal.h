@@ -84,6 +84,11 @@ struct SweepField {
   double sm_inv_den;       // periodic, scan kernels: 1 / (1 + z0 + (a/gamma) z_{L-1});
                            // filter kernel: 1 / c
   const void *tab;         // T[3L]: alpha_k | g_k | z_k (solver factors)
+  // Filter kernel: per-line stencil of w's input, computed once per plan
+  // (the velocity fields it serves do not depend on time); null: computed
+  // per tile.  wt: T[groups*LPG][8] taps -3..4; nt: int[groups*LPG] shifts.
+  const void *wt;
+  const int *nt;
 };
 
 // Shared-memory slot of one descriptor at the head of every sweep kernel's
@@ -104,6 +109,11 @@ size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64);
 // Longest segment (cells per CTA along a line) of the filter kernel for a
 // recurrence warm-up of J cells.
 int filter_segment_max(int J);
+// Fills the per-line stencil table of the filter kernel for field `*d_field`
+// (device descriptor): wt = T[lines][8], nt = int[lines], lines = groups*LPG
+// (lines past M get zeros).
+cudaError_t launch_filter_weights(bool fp64, const SweepField *d_field, void *wt, int *nt,
+                                  int lines, cudaStream_t stream);
 
 // Launches one fused sweep over all fields of `d_fields` (device array,
 // sorted by group0; tiles group_base .. group_base+groups_total-1).  All fields share the cluster size `cs`, their

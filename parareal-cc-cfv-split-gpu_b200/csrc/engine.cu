@@ -424,8 +424,27 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
   }
   plan->nf = nf;
   plan->pp = nf > 0 && fields[0].B != nullptr;
+  // filter sub-steps: one per-line stencil table per kind, shared by the
+  // plan's fields (same grid and sub-step; the velocity fields of the filter
+  // kernel do not depend on time)
+  int lines[3] = {0, 0, 0};
+  for (int kind = 0; kind < 3 && nf > 0; ++kind) {
+    if (plan->geom[kind].variant != SWEEP_FILTER) continue;
+    lines[kind] = h[(size_t)kind * nf].groups * LPG;
+    CK(plan->wt[kind].alloc((fp64 ? 8 : 4) * 8 * (size_t)lines[kind]));
+    CK(plan->nt[kind].alloc(sizeof(int) * (size_t)lines[kind]));
+    for (int i = 0; i < nf; ++i) {
+      h[(size_t)kind * nf + i].wt = plan->wt[kind].p;
+      h[(size_t)kind * nf + i].nt = plan->nt[kind].as<int>();
+    }
+  }
   CK(plan->fields.alloc(sizeof(SweepField) * h.size()));
   CK(cudaMemcpy(plan->fields.p, h.data(), sizeof(SweepField) * h.size(), cudaMemcpyHostToDevice));
+  for (int kind = 0; kind < 3; ++kind)
+    if (lines[kind])
+      CK(launch_filter_weights(fp64, plan->fields.as<SweepField>() + (size_t)kind * nf,
+                               plan->wt[kind].p, plan->nt[kind].as<int>(), lines[kind], 0));
+  CK(cudaStreamSynchronize(0));
   return CCFV_OK;
 }
 

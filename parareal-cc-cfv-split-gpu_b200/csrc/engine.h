@@ -45,6 +45,7 @@ struct StepPlan {
   int groups_per_field[3] = {0, 0, 0};
   LaunchGeom geom[3];
   bool pp = false;        // out-of-place sequence (SweepField::pp)
+  DevBuf wt[3], nt[3];    // filter kernel: per-line stencil tables per sub-step kind
 };
 
 // One field of a plan: swept in place on A (B == nullptr), or an out-of-place

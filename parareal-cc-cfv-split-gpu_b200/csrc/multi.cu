@@ -146,7 +146,8 @@ using KKey = std::tuple<int, int, int, int, int>;  // kind, variant, cs, lc buck
 // segment length and halo, so they share a class across segment lengths; the
 // scan kernels also group by segment-length bucket.
 static void add_field(std::map<KKey, SweepClass> &classes, int kind, const ccfv_grid &g,
-                      const SweepField &f0, bool fp64) {
+                      const SweepField &f0, bool fp64, FilterTables *tabs,
+                      std::tuple<int, int, int, int> tkey) {
   const LaunchGeom G = step_geom(g, f0.dir, f0.Dt, f0.dsrc, fp64, /*inplace=*/false);
   const bool filt = G.variant == SWEEP_FILTER;
   const int bucket = filt ? 0 : (G.lc_max + 63) / 64;  // segment-length bucket bounds the tile
@@ -161,7 +162,20 @@ static void add_field(std::map<KKey, SweepClass> &classes, int kind, const ccfv_
   f.group0 = K.groups;
   f.cta0 = K.groups * G.cs;
   f.halo_f = G.halo;
-  if (filt) filter_field(g, f, fp64);
+  if (filt) {
+    filter_field(g, f, fp64);
+    FilterTable &T = (*tabs)[tkey];  // shared by every field of this key
+    if (!T.lines) {
+      T.lines = f.groups * LPG;
+      T.fp64 = fp64;
+      T.cls = KKey{kind, G.variant, G.cs, bucket, fp64 ? 1 : 0};
+      T.idx = K.h.size();
+      T.wt.alloc((fp64 ? 8 : 4) * 8 * (size_t)T.lines);
+      T.nt.alloc(sizeof(int) * (size_t)T.lines);
+    }
+    f.wt = T.wt.p;
+    f.nt = T.nt.as<int>();
+  }
   K.groups += f.groups;
   K.h.push_back(f);
 }
@@ -303,6 +317,7 @@ void MultiEngine::remove(int slot) {
 int MultiEngine::rebuild() {
   fine_.clear();
   coarse_.clear();
+  ftabs_.clear();
   const int n = (int)slots_.size();
   std::vector<BElem> he(n);
   norm_off_.assign(n, 0);
@@ -348,7 +363,7 @@ int MultiEngine::rebuild() {
           f.data2 = P->FS + (size_t)s * P->NN;
           f.in0 = P->U + (size_t)s * P->NN;
           f.par = pp_parity(P->J);
-          add_field(fine_, kind, g, f, true);
+          add_field(fine_, kind, g, f, true, &ftabs_, std::make_tuple(i, kind, 0, 1));
         }
       }
       {  // coarse: the work field W, slice from the launch (t0 + n DT + i dtc)
@@ -374,15 +389,18 @@ int MultiEngine::rebuild() {
         };
         const bool delta_src = g.source != CCFV_SRC_NONE && P->o.form == CCFV_FORM_DELTA;
         if (P->g64 && !delta_src) {
-          add_field(coarse_, kind, g, coarse_field(g, P->tab[2 + dir], 0), true);
+          add_field(coarse_, kind, g, coarse_field(g, P->tab[2 + dir], 0), true, &ftabs_,
+                    std::make_tuple(i, kind, 1, 1));
         } else {
           // the first sweep moves states: FP64, with the source; the
           // iterations move increments in the coarse precision (delta form:
           // with the linear part of G, without the source)
-          add_field(coarse_, kind, g, coarse_field(g, P->tab[4 + dir], 1), true);
+          add_field(coarse_, kind, g, coarse_field(g, P->tab[4 + dir], 1), true, &ftabs_,
+                    std::make_tuple(i, kind, 1, 1));
           ccfv_grid gh = g;
           if (P->o.form == CCFV_FORM_DELTA) gh.source = CCFV_SRC_NONE;
-          add_field(coarse_, kind, gh, coarse_field(gh, P->tab[2 + dir], 2), P->g64);
+          add_field(coarse_, kind, gh, coarse_field(gh, P->tab[2 + dir], 2), P->g64, &ftabs_,
+                    std::make_tuple(i, kind, 1, P->g64 ? 1 : 0));
         }
       }
     }
@@ -393,6 +411,14 @@ int MultiEngine::rebuild() {
       MCK(K.d.alloc(sizeof(SweepField) * K.h.size()));
       MCK(cudaMemcpyAsync(K.d.p, K.h.data(), sizeof(SweepField) * K.h.size(), cudaMemcpyHostToDevice, st_));
     }
+  for (auto &kv : ftabs_) {  // per-line stencil tables of the filter fields
+    FilterTable &T = kv.second;
+    if (!T.wt.p || !T.nt.p) return fail(CCFV_ERR_NOMEM, "stencil table allocation failed");
+    const int level = std::get<2>(kv.first);
+    SweepClass &K = (level == 0 ? fine_ : coarse_).at(T.cls);
+    MCK(launch_filter_weights(T.fp64, K.d.as<SweepField>() + T.idx, T.wt.p, T.nt.as<int>(),
+                              T.lines, st_));
+  }
   const int eb = 148;
   MCK(elems_.alloc(sizeof(BElem) * std::max(n, 1)));
   if (n) MCK(cudaMemcpyAsync(elems_.p, he.data(), sizeof(BElem) * n, cudaMemcpyHostToDevice, st_));

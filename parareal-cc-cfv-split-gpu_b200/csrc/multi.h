@@ -53,6 +53,17 @@ struct SweepClass {
   int groups = 0;
 };
 
+// Per-line stencil table of the filter kernel for one (problem, sub-step
+// kind, level, precision); `cls`/`idx` locate a descriptor that uses it.
+struct FilterTable {
+  DevBuf wt, nt;
+  int lines = 0;
+  bool fp64 = true;
+  std::tuple<int, int, int, int, int> cls;
+  size_t idx = 0;
+};
+using FilterTables = std::map<std::tuple<int, int, int, int>, FilterTable>;
+
 class MultiEngine {
  public:
   MultiEngine(int device, cudaStream_t st) : device_(device), st_(st) {
@@ -95,6 +106,7 @@ class MultiEngine {
   std::vector<std::unique_ptr<Problem>> slots_;
   bool dirty_ = true;
   std::map<std::tuple<int, int, int, int, int>, SweepClass> fine_, coarse_;
+  FilterTables ftabs_;
   DevBuf elems_, nlo_d_, partial_, counters_, status_, norms_d_;
   std::vector<int> nlo_;
   std::vector<size_t> norm_off_;

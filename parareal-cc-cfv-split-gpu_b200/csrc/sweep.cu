@@ -1174,6 +1174,62 @@ __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max
   return s;
 }
 
+// Stencil of line gl's w input: w_k = sum_{m=-3..4} om[m+3] C_{k+n0+m} - mu
+// w_{k-1}, i.e. (1/c) M b with b the remap + foot-derivative stencil of the
+// shared foot -sigma = n0 + xi and M b_k = (b_{k-1} + 10 b_k + b_{k+1}) / 12.
+template <typename T>
+__device__ __forceinline__ void filter_line_stencil(const SweepField &F, long long gl,
+                                                    double toff, T *om, int *n0) {
+  const double tau0 = F.t_min + F.ht * (double)gl;
+  const double tau1 = F.t_min + F.ht * (double)(gl + 1);
+  const double f0 = edge_foot(F, 0, tau0, tau1, toff + F.ta_rel, toff + F.tb_rel);
+  const double u = (f0 - F.s_min) / F.h;
+  const double fl = floor(u);
+  *n0 = (int)fl;
+  const double x = u - fl, x2 = x * x, x3 = x2 * x;
+  const double A = x - 2.0 * x2 + x3, B = x3 - x2, Cc = 3.0 * x2 - 2.0 * x3;
+  const double kq = F.kb * F.inv12h;
+  const double pm2 = 2.0 * x3 - 6.0 * x2 + 3.0 * x + 1.0;
+  const double pm1 = -8.0 * x3 + 18.0 * x2 + 6.0 * x - 15.0;
+  const double pz = 12.0 * x3 - 18.0 * x2 - 24.0 * x + 15.0;
+  const double pp1 = -8.0 * x3 + 6.0 * x2 + 18.0 * x - 1.0;
+  const double pp2 = 2.0 * x3 - 3.0 * x;
+  double o[6];  // b_k = sum_{j<6} o_j C_{k+n0-2+j}
+  o[0] = A / 12.0 - kq * pm2;
+  o[1] = (B - 8.0 * A) / 12.0 + kq * (pm2 - pm1);
+  o[2] = 1.0 - Cc - 2.0 * B / 3.0 + kq * (pm1 - pz);
+  o[3] = Cc + 2.0 * A / 3.0 + kq * (pz - pp1);
+  o[4] = (8.0 * B - A) / 12.0 + kq * (pp1 - pp2);
+  o[5] = -B / 12.0 + kq * pp2;
+  const double icw = F.sm_inv_den / 12.0;
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {  // tap m - 3
+    const double from_bm = m < 6 ? o[m] : 0.0;                  // b_{k-1}
+    const double from_bc = (m >= 1 && m < 7) ? o[m - 1] : 0.0;  // b_k
+    const double from_bp = m >= 2 ? o[m - 2] : 0.0;             // b_{k+1}
+    om[m] = T(icw * (from_bm + 10.0 * from_bc + from_bp));
+  }
+}
+
+// The per-line stencil table of one field (one thread per line).
+template <typename T>
+__global__ void filter_weights_kernel(const SweepField *__restrict__ f, T *__restrict__ wt,
+                                      int *__restrict__ nt, int lines) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= lines) return;
+  const SweepField F = *f;
+  if (l < F.M) {
+    T om[8];
+    int n0 = 0;
+    filter_line_stencil<T>(F, l, 0.0, om, &n0);
+    for (int m = 0; m < 8; ++m) wt[(size_t)l * 8 + m] = om[m];
+    nt[l] = n0;
+  } else {
+    for (int m = 0; m < 8; ++m) wt[(size_t)l * 8 + m] = T(0);
+    nt[l] = 0;
+  }
+}
+
 // Four CTAs per SM (at most 64 registers a thread; shared memory allows no
 // more): the kernel is latency bound, and each added CTA was worth more than
 // the few registers it spills (2 -> 3 -> 4 CTAs: fine phase 1498 -> 1207 ->
@@ -1279,43 +1335,20 @@ __global__ void __launch_bounds__(NTH, 4)
       }
     }
   }
-  cp_async_commit();
-  if (threadIdx.x < LPG) {  // per-line stencil b_k = sum_t om_t C_{k+n0+t}
-    const int l = threadIdx.x;
-    const long long gl = line0 + l;
-    const double tau0 = F.t_min + F.ht * (double)gl;
-    const double tau1 = F.t_min + F.ht * (double)(gl + 1);
-    const double f0 = edge_foot(F, 0, tau0, tau1, toff + F.ta_rel, toff + F.tb_rel);
-    const double u = (f0 - F.s_min) / F.h;
-    const double fl = floor(u);
-    S.n0[l] = (int)fl;
-    const double x = u - fl, x2 = x * x, x3 = x2 * x;
-    const double A = x - 2.0 * x2 + x3, B = x3 - x2, Cc = 3.0 * x2 - 2.0 * x3;
-    const double kq = F.kb * F.inv12h;
-    const double pm2 = 2.0 * x3 - 6.0 * x2 + 3.0 * x + 1.0;
-    const double pm1 = -8.0 * x3 + 18.0 * x2 + 6.0 * x - 15.0;
-    const double pz = 12.0 * x3 - 18.0 * x2 - 24.0 * x + 15.0;
-    const double pp1 = -8.0 * x3 + 6.0 * x2 + 18.0 * x - 1.0;
-    const double pp2 = 2.0 * x3 - 3.0 * x;
-    // b_k = sum_{j<6} o_j C_{k+n0-2+j}; the input of w is (1/c) M b with
-    // M b_k = (b_{k-1} + 10 b_k + b_{k+1}) / 12 = sum_{m=-3..4} W_m C_{k+n0+m}
-    double o[6];
-    o[0] = A / 12.0 - kq * pm2;
-    o[1] = (B - 8.0 * A) / 12.0 + kq * (pm2 - pm1);
-    o[2] = 1.0 - Cc - 2.0 * B / 3.0 + kq * (pm1 - pz);
-    o[3] = Cc + 2.0 * A / 3.0 + kq * (pz - pp1);
-    o[4] = (8.0 * B - A) / 12.0 + kq * (pp1 - pp2);
-    o[5] = -B / 12.0 + kq * pp2;
-    const double icw = F.sm_inv_den / 12.0;
-    T *om = S.om + 8 * l;
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {  // tap m - 3
-      const double from_bm = m < 6 ? o[m] : 0.0;                  // b_{k-1}
-      const double from_bc = (m >= 1 && m < 7) ? o[m - 1] : 0.0;  // b_k
-      const double from_bp = m >= 2 ? o[m - 2] : 0.0;             // b_{k+1}
-      om[m] = T(icw * (from_bm + 10.0 * from_bc + from_bp));
+  if (F.wt) {  // per-line stencil from the plan's table, copied with the cells
+    if (threadIdx.x < 8 * LPG) {
+      const T *src = reinterpret_cast<const T *>(F.wt) + line0 * 8 + threadIdx.x;
+      if (sizeof(T) == 8) cp_async8(S.om + threadIdx.x, src); else cp_async4(S.om + threadIdx.x, src);
+    } else if (threadIdx.x < 9 * LPG) {
+      const int l = threadIdx.x - 8 * LPG;
+      cp_async4(S.n0 + l, F.nt + line0 + l);
     }
-  } else if (threadIdx.x == LPG) {
+  }
+  cp_async_commit();
+  if (!F.wt && threadIdx.x < LPG) {
+    filter_line_stencil<T>(F, line0 + threadIdx.x, toff, S.om + 8 * threadIdx.x,
+                           S.n0 + threadIdx.x);
+  } else if (threadIdx.x == 9 * LPG) {
     const T mmu = T(-F.sm_fac);
     T pk = mmu;
     for (int i = 0; i < FCH; ++i) {
@@ -1478,6 +1511,19 @@ size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64) {
 }
 
 int filter_segment_max(int J) { return filter_seg_max(J); }
+
+cudaError_t launch_filter_weights(bool fp64, const SweepField *d_field, void *wt, int *nt,
+                                  int lines, cudaStream_t stream) {
+  const int bt = 128, grid = (lines + bt - 1) / bt;
+  count_launch();
+  if (fp64)
+    filter_weights_kernel<double><<<grid, bt, 0, stream>>>(d_field, static_cast<double *>(wt), nt,
+                                                           lines);
+  else
+    filter_weights_kernel<float><<<grid, bt, 0, stream>>>(d_field, static_cast<float *>(wt), nt,
+                                                          lines);
+  return cudaGetLastError();
+}
 
 size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64) {
   size_t el = fp64 ? 8 : 4;
