@@ -1277,17 +1277,26 @@ __device__ __forceinline__ void filter_tile(FiltSmem<T> &S, const SweepField &F,
   const bool xsweep = s_line == 1;
 
   // ---- stage rows p0-H .. p1+H-1 (periodic wrap) ----
-  if (P == FP_X) {  // FP64 x-sweep: line pairs as 16-byte copies
+  if (P == FP_X) {  // FP64 x-sweep: line pairs as 16-byte copies (M even: a pair is
+                    // inside the field or wholly past its last line)
     const int pr = threadIdx.x & 7, rs = threadIdx.x >> 3;
-    const T *gpair = gsrc + line0 + 2 * pr;
+    const long long gl = line0 + 2 * pr;
     T *dpair = S.C + 2 * pr;
-    for (int row = rs; row < nrows; row += NTH / 8) {
-      int pos = p0 - H + row;
-      if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
-        pos %= L;
-        if (pos < 0) pos += L;
+    if (gl < M) {
+      const T *gpair = gsrc + gl;
+      for (int row = rs; row < nrows; row += NTH / 8) {
+        int pos = p0 - H + row;
+        if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
+          pos %= L;
+          if (pos < 0) pos += L;
+        }
+        cp_async16(dpair + row * P, gpair + (long long)pos * s_pos);
       }
-      cp_async16(dpair + row * P, gpair + (long long)pos * s_pos);
+    } else {
+      for (int row = rs; row < nrows; row += NTH / 8) {
+        dpair[row * P] = T(0);
+        dpair[row * P + 1] = T(0);
+      }
     }
   } else if (xsweep) {
     const int ln = lane & (LPG - 1);
@@ -1465,13 +1474,16 @@ __device__ __forceinline__ void filter_tile(FiltSmem<T> &S, const SweepField &F,
   // ---- cooperative store of rows H .. H+np-1 ----
   if (P == FP_X) {  // FP64 x-sweep: line pairs as 16-byte stores
     const int pr = threadIdx.x & 7, rs = threadIdx.x >> 3;
-    T *gp = gdst + (long long)(p0 + rs) * s_pos + line0 + 2 * pr;
-    const T *sp = S.C + (rs + H) * P + 2 * pr;
-    const long long gstep = (long long)(NTH / 8) * s_pos;
-    for (int row = rs; row < np; row += NTH / 8) {
-      *reinterpret_cast<double2 *>(gp) = *reinterpret_cast<const double2 *>(sp);
-      gp += gstep;
-      sp += (NTH / 8) * P;
+    const long long gl = line0 + 2 * pr;
+    if (gl < M) {
+      T *gp = gdst + (long long)(p0 + rs) * s_pos + gl;
+      const T *sp = S.C + (rs + H) * P + 2 * pr;
+      const long long gstep = (long long)(NTH / 8) * s_pos;
+      for (int row = rs; row < np; row += NTH / 8) {
+        *reinterpret_cast<double2 *>(gp) = *reinterpret_cast<const double2 *>(sp);
+        gp += gstep;
+        sp += (NTH / 8) * P;
+      }
     }
   } else if (xsweep) {
     const int l = lane & (LPG - 1);
