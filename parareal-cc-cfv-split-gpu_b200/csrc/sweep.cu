@@ -780,10 +780,6 @@ __device__ __forceinline__ void cp_async4(void *sdst, const void *gsrc) {
   unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gsrc) : "memory");
 }
-__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
-  unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
@@ -1144,12 +1140,6 @@ __global__ void __launch_bounds__(NTH, 2)
 // staging and before the cooperative store.
 
 constexpr int FCH = 17;  // positions per lane (odd: conflict-free shared-memory columns)
-// Pitch of the staged tile: FP_Y (odd) for transposed staging, FP_X for FP64
-// x-sweeps moved as 16-byte line pairs (rows 16-byte aligned).  The
-// half-warp's column walk (rows FCH apart per lane) is free of bank conflicts
-// for both.
-constexpr int FP_Y = LPG + 1;
-constexpr int FP_X = LPG + 2;
 constexpr int FLANES = 16;
 // Longest segment for a recurrence warm-up J: 16 * FCH >= np + 2J.
 __host__ __device__ constexpr int filter_seg_max(int J) { return FLANES * FCH - 2 * J; }
@@ -1179,7 +1169,7 @@ __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max
   T *p = reinterpret_cast<T *>(raw + FD_BYTES + 64 * sizeof(int));
   s.om = p; p += 8 * LPG;
   s.pwt = p; p += 32;
-  s.C = reinterpret_cast<T *>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+  s.C = p;
   s.rows = filter_tile_rows(lc_max, H);
   return s;
 }
@@ -1240,15 +1230,44 @@ __global__ void filter_weights_kernel(const SweepField *__restrict__ f, T *__res
   }
 }
 
-// The tile's work after its descriptor is in shared memory: staging,
-// solve and store with the staged cells at pitch P (FP_X: FP64 x-sweeps
-// moved as 16-byte line pairs; FP_Y otherwise).
-template <typename T, int P>
-__device__ __forceinline__ void filter_tile(FiltSmem<T> &S, const SweepField &F, int cta,
-                                            int cs, int clustered, double toff, int jstep,
-                                            unsigned *status) {
+// Four CTAs per SM (at most 64 registers a thread; shared memory allows no
+// more): the kernel is latency bound, and each added CTA was worth more than
+// the few registers it spills (2 -> 3 -> 4 CTAs: fine phase 1498 -> 1207 ->
+// 1105 us per launch on the 2048^2 x 63-slice bench).
+template <typename T>
+__global__ void __launch_bounds__(NTH, 4)
+    sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
+                        double toff, void *data_override, int lc_max, int H, unsigned *status,
+                        int jstep, int nslice, const int *nlo, int cs, int clustered) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // CTA -> (field, tile of LPG lines, segment).  The launch's clusters are the
+  // cs segments of one tile; fields carry their first CTA and halo, so fields
+  // of different segment lengths share one launch (lc_max and H size the
+  // shared memory only)
+  const int cta = (int)blockIdx.x + group_base;
+  FiltSmem<T> S = carve_filt<T>(smem_raw, lc_max, H);
+  {
+    int lo = 0, hi = nfields - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(&fields[mid].cta0) <= cta) lo = mid; else hi = mid - 1;
+    }
+    constexpr int NW8 = (int)(sizeof(SweepField) / 8);
+    if (threadIdx.x < NW8)
+      reinterpret_cast<long long *>(S.fd)[threadIdx.x] =
+          __ldg(reinterpret_cast<const long long *>(&fields[lo]) + threadIdx.x);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && data_override) {
+    S.fd->data = data_override;
+    if (S.fd->pp) S.fd->in0 = data_override;
+  }
+  __syncthreads();
+  const SweepField &F = *S.fd;
+  if (!field_active(F, jstep, nslice, nlo)) return;
+  toff = field_time(F, toff, jstep, nslice);
   const int L = F.L;
-  const int H = F.halo_f;
+  H = F.halo_f;
   const int q = cta - F.cta0;
   const int rank = q % cs;
   const long long line0 = (long long)(q / cs) * LPG;
@@ -1277,28 +1296,7 @@ __device__ __forceinline__ void filter_tile(FiltSmem<T> &S, const SweepField &F,
   const bool xsweep = s_line == 1;
 
   // ---- stage rows p0-H .. p1+H-1 (periodic wrap) ----
-  if (P == FP_X) {  // FP64 x-sweep: line pairs as 16-byte copies (M even: a pair is
-                    // inside the field or wholly past its last line)
-    const int pr = threadIdx.x & 7, rs = threadIdx.x >> 3;
-    const long long gl = line0 + 2 * pr;
-    T *dpair = S.C + 2 * pr;
-    if (gl < M) {
-      const T *gpair = gsrc + gl;
-      for (int row = rs; row < nrows; row += NTH / 8) {
-        int pos = p0 - H + row;
-        if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
-          pos %= L;
-          if (pos < 0) pos += L;
-        }
-        cp_async16(dpair + row * P, gpair + (long long)pos * s_pos);
-      }
-    } else {
-      for (int row = rs; row < nrows; row += NTH / 8) {
-        dpair[row * P] = T(0);
-        dpair[row * P + 1] = T(0);
-      }
-    }
-  } else if (xsweep) {
+  if (xsweep) {
     const int ln = lane & (LPG - 1);
     const long long gl = line0 + ln;
     T *dcol = S.C + ln;
@@ -1312,10 +1310,10 @@ __device__ __forceinline__ void filter_tile(FiltSmem<T> &S, const SweepField &F,
           if (pos < 0) pos += L;
         }
         const T *src = gcol + (long long)pos * s_pos;
-        if (sizeof(T) == 8) cp_async8(dcol + row * P, src); else cp_async4(dcol + row * P, src);
+        if (sizeof(T) == 8) cp_async8(dcol + row * PITCH, src); else cp_async4(dcol + row * PITCH, src);
       }
     } else {
-      for (int row = row0; row < nrows; row += 2 * NW) dcol[row * P] = T(0);
+      for (int row = row0; row < nrows; row += 2 * NW) dcol[row * PITCH] = T(0);
     }
   } else {
     for (int ln = warp; ln < LPG; ln += NW) {
@@ -1329,11 +1327,11 @@ __device__ __forceinline__ void filter_tile(FiltSmem<T> &S, const SweepField &F,
             pos %= L;
             if (pos < 0) pos += L;
           }
-          if (sizeof(T) == 8) cp_async8(dcol + row * P, lbase + pos);
-          else cp_async4(dcol + row * P, lbase + pos);
+          if (sizeof(T) == 8) cp_async8(dcol + row * PITCH, lbase + pos);
+          else cp_async4(dcol + row * PITCH, lbase + pos);
         }
       } else {
-        for (int row = lane; row < nrows; row += 32) dcol[row * P] = T(0);
+        for (int row = lane; row < nrows; row += 32) dcol[row * PITCH] = T(0);
       }
     }
   }
@@ -1392,13 +1390,13 @@ __device__ __forceinline__ void filter_tile(FiltSmem<T> &S, const SweepField &F,
       const T *omp = S.om + 8 * ln;
       const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5],
               o6 = omp[6], o7 = omp[7];
-      const T *cp = S.C + (ok ? r0 : 0) * P + ln;
-      T w0 = cp[0], w1 = cp[P], w2 = cp[2 * P], w3 = cp[3 * P], w4 = cp[4 * P],
-        w5 = cp[5 * P], w6 = cp[6 * P];
+      const T *cp = S.C + (ok ? r0 : 0) * PITCH + ln;
+      T w0 = cp[0], w1 = cp[PITCH], w2 = cp[2 * PITCH], w3 = cp[3 * PITCH], w4 = cp[4 * PITCH],
+        w5 = cp[5 * PITCH], w6 = cp[6 * PITCH];
       T w = T(0);
 #pragma unroll
       for (int i = 0; i < FCH; ++i) {
-        const T w7 = cp[(7 + i) * P];
+        const T w7 = cp[(7 + i) * PITCH];
         const T mb = o0 * w0 + o1 * w1 + o2 * w2 + o3 * w3 + o4 * w4 + o5 * w5 + o6 * w6 + o7 * w7;
         w = mb + mmu * w;
         v[i] = w;
@@ -1424,20 +1422,20 @@ __device__ __forceinline__ void filter_tile(FiltSmem<T> &S, const SweepField &F,
     // w of positions k0 .. k0+FCH-1 into this line's column
     __syncwarp(fm);
     {
-      T *wp = S.C + (k0 + rb) * P + ln;
+      T *wp = S.C + (k0 + rb) * PITCH + ln;
 #pragma unroll
-      for (int i = 0; i < FCH; ++i) wp[i * P] = v[i];
+      for (int i = 0; i < FCH; ++i) wp[i * PITCH] = v[i];
     }
     __syncwarp(fm);
 
     // backward: x over [p0, qb), zero start at qb
     const int k1 = p0 + c * FCH;
     {
-      const T *xp = S.C + (k1 + rb) * P + ln;
+      const T *xp = S.C + (k1 + rb) * PITCH + ln;
       const int nb = qb - k1;
 #pragma unroll
       for (int i = 0; i < FCH; ++i) {
-        const T val = xp[i * P];
+        const T val = xp[i * PITCH];
         v[i] = (i < nb) ? val : T(0);
       }
       T x = T(0);
@@ -1463,40 +1461,27 @@ __device__ __forceinline__ void filter_tile(FiltSmem<T> &S, const SweepField &F,
     }
     __syncwarp(fm);
     {
-      T *xp = S.C + (k1 + rb) * P + ln;
+      T *xp = S.C + (k1 + rb) * PITCH + ln;
 #pragma unroll
-      for (int i = 0; i < FCH; ++i) xp[i * P] = v[i];
+      for (int i = 0; i < FCH; ++i) xp[i * PITCH] = v[i];
     }
   }
   __syncthreads();
   if (clustered) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
 
   // ---- cooperative store of rows H .. H+np-1 ----
-  if (P == FP_X) {  // FP64 x-sweep: line pairs as 16-byte stores
-    const int pr = threadIdx.x & 7, rs = threadIdx.x >> 3;
-    const long long gl = line0 + 2 * pr;
-    if (gl < M) {
-      T *gp = gdst + (long long)(p0 + rs) * s_pos + gl;
-      const T *sp = S.C + (rs + H) * P + 2 * pr;
-      const long long gstep = (long long)(NTH / 8) * s_pos;
-      for (int row = rs; row < np; row += NTH / 8) {
-        *reinterpret_cast<double2 *>(gp) = *reinterpret_cast<const double2 *>(sp);
-        gp += gstep;
-        sp += (NTH / 8) * P;
-      }
-    }
-  } else if (xsweep) {
+  if (xsweep) {
     const int l = lane & (LPG - 1);
     const long long gl = line0 + l;
     if (gl < M) {
       const int row0 = warp * 2 + (lane >> 4);
       T *gp = gdst + (long long)(p0 + row0) * s_pos + gl;
-      const T *sp = S.C + (row0 + H) * P + l;
+      const T *sp = S.C + (row0 + H) * PITCH + l;
       const long long gstep = 2LL * NW * s_pos;
       for (int row = row0; row < np; row += 2 * NW) {
         *gp = *sp;
         gp += gstep;
-        sp += 2 * NW * P;
+        sp += 2 * NW * PITCH;
       }
     }
   } else {
@@ -1504,57 +1489,10 @@ __device__ __forceinline__ void filter_tile(FiltSmem<T> &S, const SweepField &F,
       const long long gl2 = line0 + l2;
       if (gl2 >= M) continue;
       T *lbase = gdst + gl2 * s_line + p0;
-      const T *scol = S.C + H * P + l2;
-      for (int row = lane; row < np; row += 32) lbase[row] = scol[row * P];
+      const T *scol = S.C + H * PITCH + l2;
+      for (int row = lane; row < np; row += 32) lbase[row] = scol[row * PITCH];
     }
   }
-}
-
-// Four CTAs per SM (at most 64 registers a thread; shared memory allows no
-// more): the kernel is latency bound, and each added CTA was worth more than
-// the few registers it spills (2 -> 3 -> 4 CTAs: fine phase 1498 -> 1207 ->
-// 1105 us per launch on the 2048^2 x 63-slice bench).
-template <typename T>
-__global__ void __launch_bounds__(NTH, 4)
-    sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
-                        double toff, void *data_override, int lc_max, int H, unsigned *status,
-                        int jstep, int nslice, const int *nlo, int cs, int clustered) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  // CTA -> (field, tile of LPG lines, segment).  The launch's clusters are the
-  // cs segments of one tile; fields carry their first CTA and halo, so fields
-  // of different segment lengths share one launch (lc_max and H size the
-  // shared memory only)
-  const int cta = (int)blockIdx.x + group_base;
-  FiltSmem<T> S = carve_filt<T>(smem_raw, lc_max, H);
-  {
-    int lo = 0, hi = nfields - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (__ldg(&fields[mid].cta0) <= cta) lo = mid; else hi = mid - 1;
-    }
-    constexpr int NW8 = (int)(sizeof(SweepField) / 8);
-    if (threadIdx.x < NW8)
-      reinterpret_cast<long long *>(S.fd)[threadIdx.x] =
-          __ldg(reinterpret_cast<const long long *>(&fields[lo]) + threadIdx.x);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0 && data_override) {
-    S.fd->data = data_override;
-    if (S.fd->pp) S.fd->in0 = data_override;
-  }
-  __syncthreads();
-  const SweepField &F = *S.fd;
-  if (!field_active(F, jstep, nslice, nlo)) return;
-  toff = field_time(F, toff, jstep, nslice);
-  // FP64 x-sweeps with an even line stride, 16-byte aligned buffers and whole
-  // line pairs move cells as 16-byte line pairs (pitch FP_X)
-  const void *vs;
-  void *vd;
-  field_io(F, jstep, &vs, &vd);
-  const bool vec = sizeof(T) == 8 && F.s_line == 1 && (F.s_pos & 1) == 0 && (F.M & 1) == 0 &&
-                   ((reinterpret_cast<uintptr_t>(vs) | reinterpret_cast<uintptr_t>(vd)) & 15) == 0;
-  if (vec) filter_tile<T, FP_X>(S, F, cta, cs, clustered, toff, jstep, status);
-  else filter_tile<T, FP_Y>(S, F, cta, cs, clustered, toff, jstep, status);
 }
 
 }  // namespace
@@ -1568,8 +1506,8 @@ size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source) {
 
 size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64) {
   size_t el = fp64 ? 8 : 4;
-  return FD_BYTES + 64 * sizeof(int) + 16 +
-         (8 * (size_t)LPG + 32 + (size_t)filter_tile_rows(lc_max, halo) * FP_X) * el;
+  return FD_BYTES + 64 * sizeof(int) +
+         (8 * (size_t)LPG + 32 + (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el;
 }
 
 int filter_segment_max(int J) { return filter_seg_max(J); }
