@@ -65,9 +65,23 @@ def parse():
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--seed", type=int, default=20261206)
-    ap.add_argument("--plain-sample", type=int, default=24,
-                    help="instances solved one at a time (FP64 coarse) for the plain rate")
+    ap.add_argument("--plain-sample", type=int, default=0,
+                    help="instances solved one at a time (FP64 coarse) for the plain rate "
+                         "(0: all; the solve times are heavy-tailed, so a sample is noisy)")
+    ap.add_argument("--coarse-theta", default="auto",
+                    help="batch/serve: diffusion weight of the coarse steps ('auto': the "
+                         "damping rule, 'cn': Crank-Nicolson as the reference, or a value "
+                         "in [0.5, 1]); the plain rate always uses Crank-Nicolson")
     return ap.parse_args()
+
+
+def coarse_theta_arg(a):
+    import ccfv
+    if a.coarse_theta == "auto":
+        return ccfv.COARSE_THETA_AUTO
+    if a.coarse_theta == "cn":
+        return 0.5
+    return float(a.coarse_theta)
 
 
 def workload(a):
@@ -463,7 +477,7 @@ def batch_problems(a, rng, n, nmin=64, nmax=1024, mixed_velocity=False):
                            scheme=ccfv.SCHEME_CONSISTENT)
         probs.append(dict(grid=g, gauss=par, t0=0.0, t1=T, nt_fine=nt, n_slices=S,
                           coarse_ratio=ratio, tol=tol, kmax=S, coarse_precision=ccfv.FP32,
-                          form=ccfv.FORM_DELTA, N=N))
+                          form=ccfv.FORM_DELTA, N=N, coarse_theta=coarse_theta_arg(a)))
     return probs
 
 
@@ -483,14 +497,23 @@ def _fields(probs, device, host=False):
         s.close()
 
 
-def plain_rate(probs, device):
-    """Plain single-instance FP64 form: each problem alone, FP64 coarse."""
+def plain_sample(probs, n):
+    """Every problem (n <= 0) or n of them, evenly strided."""
+    if n <= 0 or n >= len(probs):
+        return list(probs)
+    return probs[:: max(1, len(probs) // n)][:n]
+
+
+def plain_rate(probs, device, theta=0.5):
+    """Plain single-instance FP64 form: each problem alone, FP64 coarse
+    (Crank-Nicolson coarse steps unless `theta` says otherwise)."""
     import torch
     import ccfv
     cells, ms = 0.0, 0.0
     for p in probs:
         s = ccfv.Solver(p["grid"], device)
         kw = {k: p[k] for k in ("t0", "t1", "nt_fine", "n_slices", "coarse_ratio", "tol", "kmax")}
+        kw["coarse_theta"] = theta
         s.parareal(p["C0"], p["C_T"], coarse_precision=ccfv.FP64, form=ccfv.FORM_DELTA, **kw)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
@@ -528,8 +551,10 @@ def run_batch(a, ws, rank, local):
     ck = clocks.stop()
     ms = reduce_max(ev0.elapsed_time(ev1), ws)
     value = ws * cells * a.steps / (ms * 1e-3)
-    sample = probs[:: max(1, len(probs) // a.plain_sample)][: a.plain_sample]
+    sample = plain_sample(probs, a.plain_sample)
     plain = plain_rate(sample, local) if rank == 0 else None
+    th = coarse_theta_arg(a)
+    plain_th = plain_rate(sample, local, th) if rank == 0 and th != 0.5 else plain
     if rank == 0:
         its = [x["iterations"] for x in st]
         conv = sum(1 for x in st if x["converged"])
@@ -542,10 +567,16 @@ def run_batch(a, ws, rank, local):
                                 "64..1024, constant velocity U[-2,2]^2, nu log-uniform "
                                 "1e-4..1e-1, 1-8 Gaussians, T=1, fine dt at CFL 0.8, 16-64 "
                                 "slices, coarse dt = 8 x fine, FP32 coarse / FP64 fine, "
-                                "tol 1e-10 (cap = slices)", "seed": a.seed},
+                                f"coarse diffusion weight {a.coarse_theta}, "
+                                "tol 1e-10 (cap = slices)", "seed": a.seed,
+                    "plain": "each instance alone, FP64 Crank-Nicolson coarse steps "
+                             f"({len(sample)} instances)"},
             iterations_mean=float(np.mean(its)), converged=conv, instances=len(st),
+            fine_ms=st[0]["fine_ms"], coarse_ms=st[0]["coarse_ms"],
             plain_fp64_single_instance_cell_updates_per_s=plain,
             batched_vs_plain=(value / ws / plain) if plain else None,
+            plain_fp64_same_coarse_theta_cell_updates_per_s=plain_th,
+            batched_vs_plain_same_coarse_theta=(value / ws / plain_th) if plain_th else None,
             clocks=ck, gpu_launches=launches)))
 
 
@@ -585,7 +616,7 @@ def run_serve(a, ws, rank, local):
         its.append(st["iterations"])
     span = time.perf_counter() - t_start
     srv.close()
-    sample = probs[:: max(1, len(probs) // a.plain_sample)][: a.plain_sample]
+    sample = plain_sample(probs, a.plain_sample)
     for p in sample:
         p["C0"] = torch.from_numpy(p["C0"]).cuda(local)
         p["C_T"] = torch.empty_like(p["C0"])
@@ -599,8 +630,11 @@ def run_serve(a, ws, rank, local):
             config={"workload": f"{a.requests} requests, Poisson arrivals at 80% of measured "
                                 "capacity, N log-uniform 128..1024, velocity from {constant, "
                                 "rotation, swirl}, nu log-uniform 1e-4..1e-2, T U[0.25,2], "
-                                "tol in {1e-8,1e-10}, HBM budget 96 GB, FP32 coarse",
-                    "seed": a.seed},
+                                "tol in {1e-8,1e-10}, HBM budget 96 GB, FP32 coarse, "
+                                f"coarse diffusion weight {a.coarse_theta}",
+                    "seed": a.seed,
+                    "plain": "each request alone, FP64 Crank-Nicolson coarse steps "
+                             f"({len(sample)} requests)"},
             latency_ms_p50=float(np.percentile(lat, 50)),
             latency_ms_p99=float(np.percentile(lat, 99)),
             capacity_cell_updates_per_s=cap, arrival_rate_per_s=rate,

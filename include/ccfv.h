@@ -153,7 +153,23 @@ typedef struct ccfv_parareal_opts {
                           at t1): stats.err_* get ||U_k(t1) - ref|| after
                           every iteration, the reference's diagnostic
                           (T2S4_Parareal.cu:1333-1346); NULL = off          */
+  double coarse_theta; /* implicit weight of the coarse propagator's
+                          diffusion sub-steps: 0 or 0.5 = Crank-Nicolson as
+                          in the fine steps (reference); a value in (0.5, 1]
+                          (1 = backward Euler); or CCFV_COARSE_THETA_AUTO.
+                          With K dtc/h^2 >> 1 Crank-Nicolson keeps the stiff
+                          modes at amplification near -1 per coarse step,
+                          and Parareal amplifies their rounding from slice
+                          to slice (binomially in the iteration count), so
+                          it stalls; a larger theta damps them.  The
+                          converged result is the fine solution whatever
+                          G is.                                             */
 } ccfv_parareal_opts;
+
+/* coarse_theta: the smallest theta >= 0.5 whose coarse sub-steps damp the
+ * grid-scale mode by at least 1/5 (0.5 when Crank-Nicolson already does,
+ * i.e. K dtc/h^2 below ~0.58; ~0.8 for stiff diffusion). */
+#define CCFV_COARSE_THETA_AUTO (-1.0)
 
 #define CCFV_MAX_ITERS 128
 

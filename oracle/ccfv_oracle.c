@@ -148,6 +148,7 @@ typedef struct line_par {
   double eps_remap; /* x: 1e-15 (T2S4:323-324), y: 1e-16 (T2S4:414-415) */
   int deriv_of_remap; /* derivative taken of the remapped field (3rd sweep) */
   double src_w;       /* RHS weight of (remapped f(t_a) + f(t_b))           */
+  double theta;       /* implicit diffusion weight (0.5: Crank-Nicolson)    */
 } line_par;
 
 /* PPM antiderivative in cell units (d_intC_ppm4th, T2S4_Parareal.cu:63-65). */
@@ -356,7 +357,9 @@ static void sweep_line(const line_par *p, const double *c, const double *foot,
    * b = remap(C) + w (remap(f(t_a)) + f(t_b)) + 0.5 K Dt/h (D_{k+1} - D_k);
    * f(t_a) is remapped by the same PPM integral as C (T2S4:846-853,
    * 893-900, 944-951).  The reference's w is 0.25 dt for the x half-steps
-   * and 0.5 dt for the y step, i.e. 0.5 Dt of the sub-step. */
+   * and 0.5 dt for the y step, i.e. 0.5 Dt of the sub-step.  A theta-weighted
+   * diffusion (theta = 0.5 above) takes (1 - theta) K Dt/h here and theta in
+   * the LHS. */
   const double rinv = p->Dt / p->h;
   double *F0b = u; /* remapped f(t_a); u is free until the cyclic solve */
   if (s0) {
@@ -365,7 +368,7 @@ static void sweep_line(const line_par *p, const double *c, const double *foot,
   }
   for (int k = 0; k < L; k++) {
     const double fs = s0 ? p->src_w * (F0b[k] + s1[k]) : 0.0;
-    b[k] = IntC[k] + fs + 0.5 * p->K * rinv * (D[k + 1] - D[k]);
+    b[k] = IntC[k] + fs + (1.0 - p->theta) * p->K * rinv * (D[k + 1] - D[k]);
   }
   /* compact mass matrix (x_b_rhs_compact_on_gpu T2S4:616-634) */
   if (p->bc == OR_BC_COMPAT) {
@@ -380,8 +383,8 @@ static void sweep_line(const line_par *p, const double *c, const double *foot,
   }
   /* constant LHS (x_A_LHS_on_gpu T2S4:550-561 / y_A_LHS_on_gpu T2S4:583-594) */
   const double r2 = p->Dt / (p->h * p->h);
-  const double coA = 1.0 / 12 - 0.5 * p->K * r2;
-  const double coB = 10.0 / 12 + p->K * r2;
+  const double coA = 1.0 / 12 - p->theta * p->K * r2;
+  const double coB = 10.0 / 12 + 2.0 * p->theta * p->K * r2;
   const double coC = coA;
   if (p->bc == OR_BC_COMPAT) {
     for (int k = 0; k < L; k++) diag[k] = coB;
@@ -410,6 +413,7 @@ static void sweep(const or_grid *g, int dir, const double *in, double *outp, con
   line_par p;
   p.K = g->K;
   p.Dt = Dt;
+  p.theta = g->theta > 0 ? g->theta : 0.5;
   p.bc = g->bc;
   p.deriv_of_remap = deriv_of_remap;
   /* the reference's 0.5 Dt adds the source twice over a full split step
@@ -590,6 +594,23 @@ int or_parareal_ref(const or_grid *g, const double *C0, double T_min, double T_m
  * identical).  DELTA form: U+[n+1] = F(U[n]) + G(U+[n] - U[n]), equal in
  * exact arithmetic because every operator of the scheme is linear in C. */
 
+/* Automatic coarse diffusion weight: the grid-scale mode of a theta-weighted
+ * sub-step with nu = K Dt/h^2 is multiplied by
+ * (2/3 - 32/9 (1-theta) nu) / (2/3 + 4 theta nu) (mass matrix 8/12, LHS
+ * second difference 4, RHS difference of the fourth-order edge derivatives
+ * 16/3); theta is the smallest value >= 1/2 that makes its magnitude at most
+ * 1/5 at the largest nu of a coarse step (x sub-steps dtc/2, y dtc). */
+static double auto_theta(const or_grid *g, double dtc) {
+  const double hx = (g->x_max - g->x_min) / g->nx, hy = (g->y_max - g->y_min) / g->ny;
+  double nu = 0.5 * dtc / (hx * hx);
+  if (dtc / (hy * hy) > nu) nu = dtc / (hy * hy);
+  nu *= g->K;
+  if (!(nu > 0)) return 0.5;
+  const double rho = 0.2;
+  double th = (32.0 / 9.0 * nu - 2.0 / 3.0 * (1.0 + rho)) / (nu * (32.0 / 9.0 + 4.0 * rho));
+  return th < 0.5 ? 0.5 : (th > 1.0 ? 1.0 : th);
+}
+
 static double l2(const double *a, size_t n) {
   double s = 0.0;
   for (size_t i = 0; i < n; ++i) s += a[i] * a[i];
@@ -604,6 +625,10 @@ int or_parareal(const or_grid *g, const or_parareal_opts *o, const double *C0, d
   const int J = o->nt_fine / S;
   const int m = o->coarse_steps < 1 ? 1 : o->coarse_steps;
   const double DT = (o->t1 - o->t0) / S;
+  /* every coarse step, the first sweep included, uses the coarse weight */
+  or_grid gc = *g;
+  gc.theta = o->coarse_theta > 0 ? o->coarse_theta
+             : o->coarse_theta == -1.0 ? auto_theta(g, DT / m) : 0.5;
   double *U = (double *)malloc(sizeof(double) * NN * (S + 1));
   double *F = (double *)malloc(sizeof(double) * NN * (S + 1));
   double *Gold = (double *)malloc(sizeof(double) * NN * (S + 1));
@@ -612,7 +637,7 @@ int or_parareal(const or_grid *g, const or_parareal_opts *o, const double *C0, d
   memcpy(U, C0, sizeof(double) * NN);
   for (int n = 0; n < S; ++n) {
     memcpy(U + (n + 1) * NN, U + n * NN, sizeof(double) * NN);
-    or_coarse(g, U + (n + 1) * NN, o->t0 + n * DT, DT, m);
+    or_coarse(&gc, U + (n + 1) * NN, o->t0 + n * DT, DT, m);
     memcpy(Gold + (n + 1) * NN, U + (n + 1) * NN, sizeof(double) * NN);
   }
   int k;
@@ -629,7 +654,7 @@ int or_parareal(const or_grid *g, const or_parareal_opts *o, const double *C0, d
       if (o->form == OR_FORM_STANDARD) {
         /* U+[n] is already in U[n] (updated in place in slice order) */
         memcpy(w, U + n * NN, sizeof(double) * NN);
-        or_coarse(g, w, tn, DT, m);
+        or_coarse(&gc, w, tn, DT, m);
         double *Fn = F + (n + 1) * NN, *Go = Gold + (n + 1) * NN;
         for (size_t i = 0; i < NN; ++i) {
           double nv = w[i] + (Fn[i] - Go[i]);
@@ -640,7 +665,7 @@ int or_parareal(const or_grid *g, const or_parareal_opts *o, const double *C0, d
       } else {
         /* e = U+[n] - U[n] goes through the linear part of G (without the
          * source term), so G(0) = 0 */
-        or_grid gh = *g;
+        or_grid gh = gc;
         gh.src = OR_SRC_NONE;
         memcpy(w, e, sizeof(double) * NN);
         or_coarse(&gh, w, tn, DT, m);

@@ -39,6 +39,8 @@ typedef struct or_grid {
   int scheme;        /* OR_SCHEME_REFERENCE or OR_SCHEME_CONSISTENT         */
   int src;           /* OR_SRC_NONE or OR_SRC_GAUSSIAN                      */
   double sp[5];      /* GAUSSIAN: (amplitude, xc, yc, width, omega)         */
+  double theta;      /* implicit weight of the diffusion sub-steps (<=0: 0.5,
+                        the reference's Crank-Nicolson; 1: backward Euler)   */
 } or_grid;
 
 typedef struct or_parareal_opts {
@@ -49,6 +51,9 @@ typedef struct or_parareal_opts {
   double tol;        /* stop when max relative slice update < tol (0: off)  */
   int kmax;
   int form;          /* OR_FORM_STANDARD (reference) or OR_FORM_DELTA       */
+  double coarse_theta;  /* diffusion weight of every coarse step: 0 -> 0.5;
+                           -1: the smallest theta >= 0.5 whose sub-steps
+                           damp the grid-scale mode by 1/5 or more          */
 } or_parareal_opts;
 
 /* One full split step x(dt/2) y(dt) x(dt/2), in place (GpuOneStep). */

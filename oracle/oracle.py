@@ -21,6 +21,7 @@ REF_PATH = HERE / "_ref" / "libt2s4ref.so"
 BC_COMPAT, BC_PERIODIC = 0, 1
 VEL_REF_ROT4, VEL_CONST, VEL_ROTATION, VEL_SWIRL = 0, 1, 2, 3
 FORM_STANDARD, FORM_DELTA = 0, 1
+COARSE_THETA_AUTO = -1.0
 SCHEME_REFERENCE, SCHEME_CONSISTENT = 0, 1
 SRC_NONE, SRC_GAUSSIAN = 0, 1
 
@@ -37,6 +38,7 @@ class OrGrid(C.Structure):
         ("scheme", C.c_int),
         ("src", C.c_int),
         ("sp", C.c_double * 5),
+        ("theta", C.c_double),
     ]
 
 
@@ -45,6 +47,7 @@ class OrPararealOpts(C.Structure):
         ("t0", C.c_double), ("t1", C.c_double),
         ("nt_fine", C.c_int), ("n_slices", C.c_int), ("coarse_steps", C.c_int),
         ("tol", C.c_double), ("kmax", C.c_int), ("form", C.c_int),
+        ("coarse_theta", C.c_double),
     ]
 
 
@@ -86,7 +89,7 @@ def lib():
 
 def grid(nx, ny=None, *, bc=BC_COMPAT, vel=VEL_REF_ROT4, vp=(0, 0, 0, 0), K=0.0,
          domain=None, quirks=1, threads=1, scheme=SCHEME_REFERENCE, src=SRC_NONE,
-         sp=(0, 0, 0, 1, 0)) -> OrGrid:
+         sp=(0, 0, 0, 1, 0), theta=0.5) -> OrGrid:
     ny = nx if ny is None else ny
     if domain is None:
         domain = (-1.0, 1.0, -1.0, 1.0) if bc == BC_COMPAT else (0.0, 1.0, 0.0, 1.0)
@@ -102,6 +105,7 @@ def grid(nx, ny=None, *, bc=BC_COMPAT, vel=VEL_REF_ROT4, vp=(0, 0, 0, 0), K=0.0,
     g.src = src
     for i in range(5):
         g.sp[i] = float(sp[i]) if i < len(sp) else 0.0
+    g.theta = float(theta)
     return g
 
 
@@ -146,8 +150,9 @@ def parareal_ref(g, C0, T_min, T_max, Nt, n_slices=40, kmax=8, Uref=None):
 
 
 def parareal(g, C0, *, t0, t1, nt_fine, n_slices, coarse_steps=1, tol=0.0, kmax=8,
-             form=FORM_STANDARD):
-    o = OrPararealOpts(t0, t1, nt_fine, n_slices, coarse_steps, tol, kmax, form)
+             form=FORM_STANDARD, coarse_theta=0.5):
+    o = OrPararealOpts(t0, t1, nt_fine, n_slices, coarse_steps, tol, kmax, form,
+                       float(coarse_theta))
     c0 = np.ascontiguousarray(C0, dtype=np.float64).reshape(-1)
     UT = np.empty_like(c0)
     upd = np.zeros(max(kmax, 1))

@@ -32,6 +32,7 @@ SRC_NONE, SRC_GAUSSIAN = 0, 1
 FP64, FP32 = 0, 1
 MEM_DEVICE, MEM_HOST = 0, 1
 FORM_STANDARD, FORM_DELTA = 0, 1
+COARSE_THETA_AUTO = -1.0  # ccfv_parareal_opts::coarse_theta: damping rule
 MAX_ITERS = 128
 
 
@@ -61,6 +62,7 @@ class PararealOpts(C.Structure):
         ("nt_fine", C.c_int), ("n_slices", C.c_int), ("coarse_ratio", C.c_int),
         ("tol", C.c_double), ("kmax", C.c_int), ("coarse_precision", C.c_int),
         ("form", C.c_int), ("mem", C.c_int), ("d_ref", C.c_void_p),
+        ("coarse_theta", C.c_double),
     ]
 
 
@@ -316,15 +318,18 @@ class Solver:
 
     # -- Parareal --------------------------------------------------------
     def parareal(self, C0, C_T=None, *, t0, t1, nt_fine, n_slices, coarse_ratio=0, tol=0.0,
-                 kmax=8, coarse_precision=FP64, form=FORM_STANDARD, ref=None, stream=None):
+                 kmax=8, coarse_precision=FP64, form=FORM_STANDARD, ref=None, coarse_theta=0.5,
+                 stream=None):
         """Parareal solve.  C0 / C_T are CUDA tensors (device) or numpy
         arrays (host); `ref` an optional CUDA tensor the iterates at t1 are
-        compared with.  Returns (C_T, stats dict)."""
+        compared with; `coarse_theta` the implicit weight of the coarse
+        propagator's diffusion (0.5 Crank-Nicolson as the reference, 1
+        backward Euler).  Returns (C_T, stats dict)."""
         host = isinstance(C0, np.ndarray)
         o = PararealOpts(t0, t1, int(nt_fine), int(n_slices), int(coarse_ratio), float(tol),
                          int(kmax), int(coarse_precision), int(form),
                          MEM_HOST if host else MEM_DEVICE,
-                         None if ref is None else _dptr(ref).value)
+                         None if ref is None else _dptr(ref).value, float(coarse_theta))
         st = Stats()
         if host:
             c0 = np.ascontiguousarray(C0, dtype=np.float64)
@@ -346,7 +351,8 @@ def _problem(p):
     o = PararealOpts(p["t0"], p["t1"], int(p["nt_fine"]), int(p["n_slices"]),
                      int(p.get("coarse_ratio", 0)), float(p.get("tol", 0.0)),
                      int(p.get("kmax", 8)), int(p.get("coarse_precision", FP64)),
-                     int(p.get("form", FORM_STANDARD)), MEM_HOST if host else MEM_DEVICE, None)
+                     int(p.get("form", FORM_STANDARD)), MEM_HOST if host else MEM_DEVICE, None,
+                     float(p.get("coarse_theta", 0.5)))
     pr = Problem()
     pr.grid = p["grid"]
     pr.opts = o
@@ -428,7 +434,7 @@ def batch_solve(problems, device=0, stream=None):
                          int(p.get("coarse_ratio", 0)), float(p.get("tol", 0.0)),
                          int(p.get("kmax", 8)), int(p.get("coarse_precision", FP64)),
                          int(p.get("form", FORM_STANDARD)), MEM_HOST if host else MEM_DEVICE,
-                         None)
+                         None, float(p.get("coarse_theta", 0.5)))
         arr[i].grid = p["grid"]
         arr[i].opts = o
         if host:

@@ -78,7 +78,9 @@ struct SweepField {
   double Dt;               // sub-step length
   double ta_rel, tb_rel;   // foot-tracing interval relative to the launch time
   double eps_remap;        // compat remap clamp (x: 1e-15, y: 1e-16)
-  double kb;               // 0.5*K*(Dt/h): RHS diffusion coefficient
+  double kb;               // (1-theta)*K*(Dt/h): RHS diffusion coefficient
+  double theta;            // implicit weight of the diffusion (0.5: Crank-Nicolson);
+                           // host bookkeeping: the kernels read kb and the tables
   double inv12h;           // 1/(12 h)
   double sm_fac;           // periodic, scan kernels: a / gamma; filter kernel: mu
   double sm_inv_den;       // periodic, scan kernels: 1 / (1 + z0 + (a/gamma) z_{L-1});
@@ -90,6 +92,20 @@ struct SweepField {
   const void *wt;
   const int *nt;
 };
+
+// Whether a field takes part in a batched launch (`nlo[inst]`: the first
+// active slice of every instance, -1 before the first coarse sweep; null: a
+// single-instance launch, always active).  The batched engine evaluates the
+// same rule on the host to skip launches in which no field is active.
+__host__ __device__ inline bool field_active(const SweepField &f, int jstep, int nslice,
+                                             const int *nlo) {
+  if (f.jmax > 0 && jstep >= f.jmax) return false;
+  if (!nlo) return true;
+  const int lo = nlo[f.inst];
+  if (f.slice >= 0) return f.slice >= lo;
+  if ((f.phase == 1 && lo >= 0) || (f.phase == 2 && lo < 0)) return false;
+  return nslice < f.smax && nslice >= lo + f.gskip;
+}
 
 // Shared-memory slot of one descriptor at the head of every sweep kernel's
 // dynamic shared memory (the data behind it stays 64-byte aligned).

@@ -123,16 +123,18 @@ static double spacing(const ccfv_grid &g, int dir) {
   return dir == 0 ? (g.x_max - g.x_min) / g.nx : (g.y_max - g.y_min) / g.ny;
 }
 
-const SolverTable *get_table(ccfv_ctx *ctx, int dir, double Dt, bool fp64, int *status) {
-  auto key = std::make_tuple(dir, Dt, fp64 ? 1 : 0);
+const SolverTable *get_table(ccfv_ctx *ctx, int dir, double Dt, bool fp64, int *status,
+                             double theta) {
+  auto key = std::make_tuple(dir, Dt, fp64 ? 1 : 0, theta);
   auto it = ctx->tables.find(key);
   if (it != ctx->tables.end()) return it->second.get();
   const ccfv_grid &g = ctx->grid;
   const int L = dir == 0 ? g.nx : g.ny;
   const double h = spacing(g, dir);
   const double r2 = Dt / (h * h);
-  const double coA = 1.0 / 12 - 0.5 * g.K * r2;
-  const double coB = 10.0 / 12 + g.K * r2;
+  // x_A_LHS / y_A_LHS (T2S4:550-594) at theta = 1/2
+  const double coA = 1.0 / 12 - theta * g.K * r2;
+  const double coB = 10.0 / 12 + 2.0 * theta * g.K * r2;
   auto tab = std::make_unique<SolverTable>();
   size_t bytes = table_len(L) * (fp64 ? 8 : 4);
   if (tab->buf.alloc(bytes) != cudaSuccess) {
@@ -158,6 +160,29 @@ const SolverTable *get_table(ccfv_ctx *ctx, int dir, double Dt, bool fp64, int *
   return res;
 }
 
+// Automatic coarse diffusion weight.  For the grid-scale (checkerboard) mode
+// a theta-weighted sub-step of diffusion number nu = K Dt/h^2 multiplies the
+// field by
+//   a(theta, nu) = (2/3 - (32/9)(1 - theta) nu) / (2/3 + 4 theta nu):
+// the compact mass matrix (1,10,1)/12 gives 2/3, the LHS second difference
+// 4 theta nu, and the RHS difference of fourth-order edge derivatives
+// (C_{i-1} - 15 C_i + 15 C_{i+1} - C_{i+2}) / 12h gives (16/3) nu under the
+// mass matrix.  Crank-Nicolson (theta = 1/2) tends to -8/9 as nu grows; the
+// rule takes the smallest theta >= 1/2 with |a| <= rho = 1/5 at the largest
+// nu of the coarse step's sub-steps (x: dtc/2, y: dtc).  Measured against the
+// Parareal iteration count on stiff cases (nu from 2 to 26), the optimum
+// theta sits at |a| of 0.2 - 0.25.
+double coarse_theta(const ccfv_parareal_opts &o, const ccfv_grid &g, double dtc) {
+  if (o.coarse_theta > 0) return o.coarse_theta;
+  if (o.coarse_theta != CCFV_COARSE_THETA_AUTO) return 0.5;
+  const double hx = spacing(g, 0), hy = spacing(g, 1);
+  const double nu = g.K * std::max(0.5 * dtc / (hx * hx), dtc / (hy * hy));
+  const double rho = 0.2;
+  if (!(nu > 0)) return 0.5;
+  const double th = (32.0 / 9.0 * nu - 2.0 / 3.0 * (1.0 + rho)) / (nu * (32.0 / 9.0 + 4.0 * rho));
+  return std::min(1.0, std::max(0.5, th));
+}
+
 // Largest |velocity component along the sweep| over the domain (bounds the
 // characteristic displacement, hence the staged halo).
 static double wmax(const ccfv_grid &g, int dir) {
@@ -181,7 +206,7 @@ static int shift_cells(const ccfv_grid &g, int dir, double Dt) {
 }
 
 SweepField make_field(const ccfv_grid &g, int dir, double Dt, double ta_rel, double tb_rel,
-                      void *data, const SolverTable *tab, int dsrc) {
+                      void *data, const SolverTable *tab, int dsrc, double theta) {
   SweepField f;
   std::memset(&f, 0, sizeof(f));
   const double dx = (g.x_max - g.x_min) / g.nx, dy = (g.y_max - g.y_min) / g.ny;
@@ -202,7 +227,8 @@ SweepField make_field(const ccfv_grid &g, int dir, double Dt, double ta_rel, dou
   f.Dt = Dt;
   f.ta_rel = ta_rel;
   f.tb_rel = tb_rel;
-  f.kb = 0.5 * g.K * (Dt / f.h);
+  f.kb = (1.0 - theta) * g.K * (Dt / f.h);  // explicit diffusion weight (theta = 1: none)
+  f.theta = theta;
   f.src = g.source;
   for (int i = 0; i < 5; ++i) f.sp[i] = g.source_params[i];
   f.src_w = g.source ? (g.scheme == CCFV_SCHEME_REFERENCE ? 0.5 : 0.25) * Dt : 0.0;
@@ -224,10 +250,10 @@ SweepField make_field(const ccfv_grid &g, int dir, double Dt, double ta_rel, dou
 // with |mu|^J below the rounding of the precision.  Returns false when the
 // warm-up would exceed FILTER_JMAX (strong diffusion: exact-scan kernels).
 bool filter_params(const ccfv_grid &g, int dir, double Dt, bool fp64, double *mu, double *ic,
-                   int *J) {
+                   int *J, double theta) {
   const double h = spacing(g, dir);
   const double r2 = Dt / (h * h);
-  const double a = 1.0 / 12 - 0.5 * g.K * r2, b = 10.0 / 12 + g.K * r2;
+  const double a = 1.0 / 12 - theta * g.K * r2, b = 10.0 / 12 + 2.0 * theta * g.K * r2;
   const double r = a / b;  // |r| < 1/2 (diagonal dominance)
   const double m = 2.0 * r / (1.0 + std::sqrt(std::max(0.0, 1.0 - 4.0 * r * r)));
   const double c = b / (1.0 + m * m);
@@ -253,7 +279,8 @@ int filter_lc(int L, bool fp64) {
   return it == g_filter_lc.end() ? LC_MAX : it->second;
 }
 
-LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64, bool inplace) {
+LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64, bool inplace,
+                     double theta) {
   LaunchGeom G;
   const int L = dir == 0 ? g.nx : g.ny;
   G.cs = (L + LC_MAX - 1) / LC_MAX;
@@ -265,7 +292,7 @@ LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64
   G.variant = g.source ? SWEEP_GENERAL_SRC : SWEEP_GENERAL;
   if (!g.source && uniform && g.bc == CCFV_BC_PERIODIC && dsrc == 0) {
     int J = 0;
-    if (filter_params(g, dir, Dt, fp64, nullptr, nullptr, &J) && L > 2 * J) {
+    if (filter_params(g, dir, Dt, fp64, nullptr, nullptr, &J, theta) && L > 2 * J) {
       G.variant = SWEEP_FILTER;
       G.halo = J + sh + 6;
       // segment length from the tuner; the segments of a line form one
@@ -355,7 +382,7 @@ int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen) 
 void filter_field(const ccfv_grid &g, SweepField &f, bool fp64) {
   double mu = 0, ic = 0;
   int J = 0;
-  filter_params(g, f.dir, f.Dt, fp64, &mu, &ic, &J);
+  filter_params(g, f.dir, f.Dt, fp64, &mu, &ic, &J, f.theta);
   f.sm_fac = mu;
   f.sm_inv_den = ic;
   f.jf = J;
@@ -370,17 +397,18 @@ static void sweep_kind(int kind, double dt, int *dir, double *Dt, double *ta, do
 }
 
 int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
-                    const std::vector<std::pair<void *, double>> &fields, bool homogeneous) {
+                    const std::vector<std::pair<void *, double>> &fields, bool homogeneous,
+                    double theta) {
   std::vector<PlanField> pf(fields.size());
   for (size_t i = 0; i < fields.size(); ++i) {
     pf[i].A = fields[i].first;
     pf[i].t0 = fields[i].second;
   }
-  return build_step_plan(ctx, plan, dt, fp64, pf, homogeneous);
+  return build_step_plan(ctx, plan, dt, fp64, pf, homogeneous, theta);
 }
 
 int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
-                    const std::vector<PlanField> &fields, bool homogeneous) {
+                    const std::vector<PlanField> &fields, bool homogeneous, double theta) {
   ccfv_grid g = ctx->grid;
   if (homogeneous) g.source = CCFV_SRC_NONE;
   const int nf = (int)fields.size();
@@ -391,10 +419,10 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
     sweep_kind(kind, dt, &dir, &Dt, &ta, &tb);
     const int dsrc = (kind == 2 && g.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
     int st = CCFV_OK;
-    const SolverTable *tab = get_table(ctx, dir, Dt, fp64, &st);
+    const SolverTable *tab = get_table(ctx, dir, Dt, fp64, &st, theta);
     if (!tab) return st;
     const bool plan_pp = !fields.empty() && fields[0].B != nullptr;
-    LaunchGeom G = step_geom(g, dir, Dt, dsrc, fp64, !plan_pp);
+    LaunchGeom G = step_geom(g, dir, Dt, dsrc, fp64, !plan_pp, theta);
     if (ctx->force_general && G.variant != SWEEP_GENERAL_SRC) G.variant = SWEEP_GENERAL;
     if (G.cs > MAX_CLUSTER && !(G.variant == SWEEP_FILTER && plan_pp))
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
@@ -404,7 +432,7 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
     for (int i = 0; i < nf; ++i) {
       const PlanField &pfi = fields[i];
-      SweepField f = make_field(g, dir, Dt, ta + pfi.t0, tb + pfi.t0, pfi.A, tab, dsrc);
+      SweepField f = make_field(g, dir, Dt, ta + pfi.t0, tb + pfi.t0, pfi.A, tab, dsrc, theta);
       f.kind = kind;
       if (pfi.B) {
         f.pp = 1;
@@ -470,8 +498,8 @@ int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int
 
 // Plan of one field for the single-field calls: an out-of-place sequence
 // between the caller's field (passed per launch) and a context scratch field.
-static StepPlan *single_plan(ccfv_ctx *ctx, double dt, bool fp64, int *status) {
-  auto key = std::make_tuple(dt, fp64 ? 1 : 0, 0);
+static StepPlan *single_plan(ccfv_ctx *ctx, double dt, bool fp64, int *status, double theta) {
+  auto key = std::make_tuple(dt, fp64 ? 1 : 0, 0, theta);
   auto it = ctx->step_plans.find(key);
   if (it != ctx->step_plans.end()) return it->second.get();
   const size_t el = fp64 ? sizeof(double) : sizeof(float);
@@ -487,7 +515,7 @@ static StepPlan *single_plan(ccfv_ctx *ctx, double dt, bool fp64, int *status) {
   auto plan = std::make_unique<StepPlan>();
   std::vector<PlanField> f(1);
   f[0].B = scratch.p;  // A and in0: the caller's field (launch override)
-  int st = build_step_plan(ctx, plan.get(), dt, fp64, f);
+  int st = build_step_plan(ctx, plan.get(), dt, fp64, f, false, theta);
   if (st != CCFV_OK) {
     *status = st;
     return nullptr;
@@ -500,9 +528,10 @@ static StepPlan *single_plan(ccfv_ctx *ctx, double dt, bool fp64, int *status) {
 // nsteps split steps on one field: 3 nsteps sweeps alternating between the
 // field and the scratch field; an odd count ends in the scratch field and is
 // copied back.
-int steps(ccfv_ctx *ctx, void *d_C, bool fp64, double t0, double dt, int nsteps, cudaStream_t st) {
+int steps(ccfv_ctx *ctx, void *d_C, bool fp64, double t0, double dt, int nsteps, cudaStream_t st,
+          double theta) {
   int status = CCFV_OK;
-  StepPlan *plan = single_plan(ctx, dt, fp64, &status);
+  StepPlan *plan = single_plan(ctx, dt, fp64, &status, theta);
   if (!plan) return status;
   for (int n = 0; n < nsteps; ++n) {
     int rc = run_step_plan(ctx, *plan, fp64, 0, 1, t0 + n * dt, d_C, st, n);
@@ -684,15 +713,18 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
   // Coarse sweeps of the iterations: m steps out of place over W / W2,
   // starting from W; the result is in W2 when 3m is odd.  The delta form
   // propagates increments: the linear part of G (no source).
+  // Every coarse step (first sweep included) uses the run's coarse diffusion
+  // weight, so the standard form's cached G(U_k) is the iterations' G.
+  const double th = coarse_theta(*o, g, dtc);
   StepPlan cplan, hplan;
   {
     std::vector<PlanField> f(1);
     f[0].A = W;
     f[0].B = W2;
     f[0].in0 = W;
-    int rc = build_step_plan(ctx, &cplan, dtc, g64, f);
+    int rc = build_step_plan(ctx, &cplan, dtc, g64, f, false, th);
     if (!rc && o->form == CCFV_FORM_DELTA && g.source != CCFV_SRC_NONE)
-      rc = build_step_plan(ctx, &hplan, dtc, g64, f, true);
+      rc = build_step_plan(ctx, &hplan, dtc, g64, f, true, th);
     if (rc) return rc;
   }
   const StepPlan *dplan =
@@ -718,7 +750,7 @@ static int parareal_impl(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const doubl
   for (int n = 0; n < S; ++n) {
     double *un1 = U + (size_t)(n + 1) * NN;
     CK(cudaMemcpyAsync(un1, U + (size_t)n * NN, fb, cudaMemcpyDeviceToDevice, st));
-    int rc = steps(ctx, un1, true, o->t0 + n * DT, dtc, m, st);
+    int rc = steps(ctx, un1, true, o->t0 + n * DT, dtc, m, st, th);
     if (rc) return rc;
     if (Gold) CK(cudaMemcpyAsync(Gold + (size_t)(n + 1) * NN, un1, fb, cudaMemcpyDeviceToDevice, st));
   }
@@ -834,6 +866,9 @@ int parareal(ccfv_ctx *ctx, const ccfv_parareal_opts *o, const double *C0, doubl
     return set_error(ctx, CCFV_ERR_INVALID, "unknown Parareal form");
   if (o->coarse_precision == CCFV_FP32 && o->form != CCFV_FORM_DELTA)
     return set_error(ctx, CCFV_ERR_INVALID, "an FP32 coarse propagator needs the DELTA form");
+  if (!coarse_theta_ok(o->coarse_theta))
+    return set_error(ctx, CCFV_ERR_INVALID,
+                     "coarse_theta must be 0 (Crank-Nicolson), in [0.5, 1] or CCFV_COARSE_THETA_AUTO");
   if (stats) std::memset(stats, 0, sizeof(*stats));
   int rc = o->coarse_precision == CCFV_FP32 ? parareal_impl<float>(ctx, o, C0, C_T, stats, st)
                                             : parareal_impl<double>(ctx, o, C0, C_T, stats, st);

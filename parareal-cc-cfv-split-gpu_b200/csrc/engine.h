@@ -68,8 +68,9 @@ struct ccfv_ctx {
   ccfv_grid grid;
   int device = 0;
   ccfv::DevBuf status;  // unsigned status word + partial-sum scratch
-  std::map<std::tuple<int, double, int>, std::unique_ptr<ccfv::SolverTable>> tables;
-  std::map<std::tuple<double, int, int>, std::unique_ptr<ccfv::StepPlan>> step_plans;
+  // keyed by (dir, sub-step, FP64, diffusion theta) / (dt, FP64, 0, theta)
+  std::map<std::tuple<int, double, int, double>, std::unique_ptr<ccfv::SolverTable>> tables;
+  std::map<std::tuple<double, int, int, double>, std::unique_ptr<ccfv::StepPlan>> step_plans;
   // Parareal slice states and scratch
   ccfv::DevBuf U, F, Gold, W, C64, C32, norms, partial, counter, io, aux;
   ccfv::DevBuf FS, W2;  // ping-pong partners of the fine slices and the coarse work field
@@ -86,13 +87,24 @@ struct ccfv_ctx {
 namespace ccfv {
 
 int set_error(ccfv_ctx *ctx, int code, const std::string &msg);
-const SolverTable *get_table(ccfv_ctx *ctx, int dir, double Dt, bool fp64, int *status);
+// `theta` is the implicit weight of the diffusion sub-step: 0.5 is the
+// reference's Crank-Nicolson; 1 is backward Euler (L-stable), which the
+// coarse propagator may use (ccfv_parareal_opts::coarse_theta).
+const SolverTable *get_table(ccfv_ctx *ctx, int dir, double Dt, bool fp64, int *status,
+                             double theta = 0.5);
 SweepField make_field(const ccfv_grid &g, int dir, double Dt, double ta_rel, double tb_rel,
-                      void *data, const SolverTable *tab, int dsrc);
+                      void *data, const SolverTable *tab, int dsrc, double theta = 0.5);
 // inplace: the sweep overwrites its input (the filter kernel's segments of a
 // line then form one cluster, at most MAX_CLUSTER CTAs).
 LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64,
-                     bool inplace = true);
+                     bool inplace = true, double theta = 0.5);
+// Diffusion weight of a Parareal run's coarse propagator of step dtc
+// (ccfv_parareal_opts::coarse_theta; 0 selects 0.5).
+double coarse_theta(const ccfv_parareal_opts &o, const ccfv_grid &g, double dtc);
+// Whether coarse_theta holds an accepted value.
+inline bool coarse_theta_ok(double th) {
+  return th == 0.0 || th == CCFV_COARSE_THETA_AUTO || (th >= 0.5 && th <= 1.0);
+}
 void filter_field(const ccfv_grid &g, SweepField &f, bool fp64);
 int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen);
 int batch_solve(int n, const ccfv_problem *probs, ccfv_stats *stats, int device,
@@ -101,13 +113,15 @@ int batch_solve(int n, const ccfv_problem *probs, ccfv_stats *stats, int device,
 // which the delta form of Parareal applies to slice increments).
 int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
                     const std::vector<std::pair<void *, double>> &fields,
-                    bool homogeneous = false);
+                    bool homogeneous = false, double theta = 0.5);
 int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
-                    const std::vector<PlanField> &fields, bool homogeneous = false);
+                    const std::vector<PlanField> &fields, bool homogeneous = false,
+                    double theta = 0.5);
 // jstep: the step's index in an out-of-place sequence (selects the buffers).
 int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int count,
                   double toff, void *data_override, cudaStream_t st, int jstep = 0);
-int steps(ccfv_ctx *ctx, void *d_C, bool fp64, double t0, double dt, int nsteps, cudaStream_t st);
+int steps(ccfv_ctx *ctx, void *d_C, bool fp64, double t0, double dt, int nsteps, cudaStream_t st,
+          double theta = 0.5);
 int coarse_fp32(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, cudaStream_t st);
 int fine_slices(ccfv_ctx *ctx, double *d_fields, int n, double t0, double slice_dt, double DT,
                 int J, cudaStream_t st);

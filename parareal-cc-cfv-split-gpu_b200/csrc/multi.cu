@@ -9,7 +9,8 @@
 // launch classes (kernel variant, precision, cluster size, segment length);
 // instances that have converged, slices that are already exact and instances
 // with fewer steps or slices drop out on the device (per-instance `nlo`
-// array, SweepField::jmax/smax) without any host work per launch.
+// array, SweepField::jmax/smax), and the host, which holds the same `nlo`,
+// skips every launch in which no field or instance would take part.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -147,8 +148,8 @@ using KKey = std::tuple<int, int, int, int, int>;  // kind, variant, cs, lc buck
 // scan kernels also group by segment-length bucket.
 static void add_field(std::map<KKey, SweepClass> &classes, int kind, const ccfv_grid &g,
                       const SweepField &f0, bool fp64, FilterTables *tabs,
-                      std::tuple<int, int, int, int> tkey) {
-  const LaunchGeom G = step_geom(g, f0.dir, f0.Dt, f0.dsrc, fp64, /*inplace=*/false);
+                      std::tuple<int, int, int> tkey, std::vector<FilterTable *> *pending) {
+  const LaunchGeom G = step_geom(g, f0.dir, f0.Dt, f0.dsrc, fp64, /*inplace=*/false, f0.theta);
   const bool filt = G.variant == SWEEP_FILTER;
   const int bucket = filt ? 0 : (G.lc_max + 63) / 64;  // segment-length bucket bounds the tile
   SweepClass &K = classes[KKey{kind, G.variant, G.cs, bucket, fp64 ? 1 : 0}];
@@ -168,10 +169,15 @@ static void add_field(std::map<KKey, SweepClass> &classes, int kind, const ccfv_
     if (!T.lines) {
       T.lines = f.groups * LPG;
       T.fp64 = fp64;
-      T.cls = KKey{kind, G.variant, G.cs, bucket, fp64 ? 1 : 0};
-      T.idx = K.h.size();
       T.wt.alloc((fp64 ? 8 : 4) * 8 * (size_t)T.lines);
       T.nt.alloc(sizeof(int) * (size_t)T.lines);
+    }
+    if (!T.ready && (pending->empty() || pending->back() != &T) &&
+        std::find(pending->begin(), pending->end(), &T) == pending->end()) {
+      T.cls = KKey{kind, G.variant, G.cs, bucket, fp64 ? 1 : 0};
+      T.idx = K.h.size();
+      T.level = std::get<1>(tkey);
+      pending->push_back(&T);
     }
     f.wt = T.wt.p;
     f.nt = T.nt.as<int>();
@@ -198,7 +204,8 @@ int problem_setup(Problem &P, const ccfv_problem &p, std::string *err) {
   const ccfv_parareal_opts &o = P.o;
   if (o.n_slices < 1 || o.nt_fine < o.n_slices || o.nt_fine % o.n_slices || o.kmax < 1 ||
       o.kmax > CCFV_MAX_ITERS || (o.coarse_precision == CCFV_FP32 && o.form != CCFV_FORM_DELTA) ||
-      (o.form != CCFV_FORM_STANDARD && o.form != CCFV_FORM_DELTA)) {
+      (o.form != CCFV_FORM_STANDARD && o.form != CCFV_FORM_DELTA) ||
+      !coarse_theta_ok(o.coarse_theta)) {
     if (err) *err = "invalid Parareal options";
     return CCFV_ERR_INVALID;
   }
@@ -214,6 +221,7 @@ int problem_setup(Problem &P, const ccfv_problem &p, std::string *err) {
   P.dtc = P.DT / (double)P.m;
   P.NN = (long long)P.g.nx * P.g.ny;
   P.g64 = o.coarse_precision != CCFV_FP32;
+  P.theta = coarse_theta(o, P.g, P.dtc);
   P.bytes = problem_bytes(P.g, o);
   return CCFV_OK;
 }
@@ -248,10 +256,12 @@ int MultiEngine::add(const ccfv_problem &pr, int *slot) {
   P->ctx = std::make_unique<ccfv_ctx>();
   P->ctx->grid = P->g;
   P->ctx->device = device_;
+  const double th = P->theta;  // fine tables: the reference's 0.5
   for (int t = 0; t < 6; ++t) {
     const int dir = t & 1;
     const double Dt = (t < 2 ? P->dt : P->dtc) * (dir == 0 ? 0.5 : 1.0);
-    P->tab[t] = get_table(P->ctx.get(), dir, Dt, (t < 2 || t >= 4) ? true : P->g64, &rc);
+    P->tab[t] = get_table(P->ctx.get(), dir, Dt, (t < 2 || t >= 4) ? true : P->g64, &rc,
+                          t < 2 ? 0.5 : th);
     if (!P->tab[t]) return fail(rc, P->ctx->last_error);
   }
   for (int kind = 0; kind < 3; ++kind)
@@ -259,7 +269,8 @@ int MultiEngine::add(const ccfv_problem &pr, int *slot) {
       const int dir = kind == 1 ? 1 : 0;
       const double Dt = (level == 0 ? P->dt : P->dtc) * (dir == 0 ? 0.5 : 1.0);
       const int dsrc = (kind == 2 && P->g.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
-      const LaunchGeom G = step_geom(P->g, dir, Dt, dsrc, level == 0 || P->g64, false);
+      const LaunchGeom G = step_geom(P->g, dir, Dt, dsrc, level == 0 || P->g64, false,
+                                     level == 0 ? 0.5 : th);
       if (G.variant != SWEEP_FILTER && G.cs > MAX_CLUSTER)
         return fail(CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
       if (std::max({sweep_smem_bytes(G.lc_max, G.halo, true, P->g.source != 0),
@@ -317,7 +328,7 @@ void MultiEngine::remove(int slot) {
 int MultiEngine::rebuild() {
   fine_.clear();
   coarse_.clear();
-  ftabs_.clear();
+  std::vector<FilterTable *> pending;  // stencil tables not computed yet
   const int n = (int)slots_.size();
   std::vector<BElem> he(n);
   norm_off_.assign(n, 0);
@@ -363,14 +374,15 @@ int MultiEngine::rebuild() {
           f.data2 = P->FS + (size_t)s * P->NN;
           f.in0 = P->U + (size_t)s * P->NN;
           f.par = pp_parity(P->J);
-          add_field(fine_, kind, g, f, true, &ftabs_, std::make_tuple(i, kind, 0, 1));
+          add_field(fine_, kind, g, f, true, &P->ftab, std::make_tuple(kind, 0, 1), &pending);
         }
       }
       {  // coarse: the work field W, slice from the launch (t0 + n DT + i dtc)
         const double Dt = kind == 1 ? P->dtc : 0.5 * P->dtc;
         const double ta = kind == 2 ? 0.5 * P->dtc : 0.0, tb = kind == 0 ? 0.5 * P->dtc : P->dtc;
         auto coarse_field = [&](const ccfv_grid &gg, const SolverTable *tab, int phase) {
-          SweepField f = make_field(gg, dir, Dt, ta + P->o.t0, tb + P->o.t0, P->W, tab, dsrc);
+          SweepField f = make_field(gg, dir, Dt, ta + P->o.t0, tb + P->o.t0, P->W, tab, dsrc,
+                                    P->theta);
           f.inst = i;
           f.slice = -1;
           f.jmax = P->m;
@@ -389,35 +401,39 @@ int MultiEngine::rebuild() {
         };
         const bool delta_src = g.source != CCFV_SRC_NONE && P->o.form == CCFV_FORM_DELTA;
         if (P->g64 && !delta_src) {
-          add_field(coarse_, kind, g, coarse_field(g, P->tab[2 + dir], 0), true, &ftabs_,
-                    std::make_tuple(i, kind, 1, 1));
+          add_field(coarse_, kind, g, coarse_field(g, P->tab[2 + dir], 0), true, &P->ftab,
+                    std::make_tuple(kind, 1, 1), &pending);
         } else {
           // the first sweep moves states: FP64, with the source; the
           // iterations move increments in the coarse precision (delta form:
           // with the linear part of G, without the source)
-          add_field(coarse_, kind, g, coarse_field(g, P->tab[4 + dir], 1), true, &ftabs_,
-                    std::make_tuple(i, kind, 1, 1));
+          add_field(coarse_, kind, g, coarse_field(g, P->tab[4 + dir], 1), true, &P->ftab,
+                    std::make_tuple(kind, 1, 1), &pending);
           ccfv_grid gh = g;
           if (P->o.form == CCFV_FORM_DELTA) gh.source = CCFV_SRC_NONE;
-          add_field(coarse_, kind, gh, coarse_field(gh, P->tab[2 + dir], 2), P->g64, &ftabs_,
-                    std::make_tuple(i, kind, 1, P->g64 ? 1 : 0));
+          add_field(coarse_, kind, gh, coarse_field(gh, P->tab[2 + dir], 2), P->g64, &P->ftab,
+                    std::make_tuple(kind, 1, P->g64 ? 1 : 0), &pending);
         }
       }
     }
   }
+  hclass_.clear();
   for (auto *cls : {&fine_, &coarse_})
     for (auto &kv : *cls) {
       SweepClass &K = kv.second;
-      MCK(K.d.alloc(sizeof(SweepField) * K.h.size()));
-      MCK(cudaMemcpyAsync(K.d.p, K.h.data(), sizeof(SweepField) * K.h.size(), cudaMemcpyHostToDevice, st_));
+      K.off = hclass_.size();
+      hclass_.insert(hclass_.end(), K.h.begin(), K.h.end());
     }
-  for (auto &kv : ftabs_) {  // per-line stencil tables of the filter fields
-    FilterTable &T = kv.second;
-    if (!T.wt.p || !T.nt.p) return fail(CCFV_ERR_NOMEM, "stencil table allocation failed");
-    const int level = std::get<2>(kv.first);
-    SweepClass &K = (level == 0 ? fine_ : coarse_).at(T.cls);
-    MCK(launch_filter_weights(T.fp64, K.d.as<SweepField>() + T.idx, T.wt.p, T.nt.as<int>(),
-                              T.lines, st_));
+  MCK(classbuf_.alloc(sizeof(SweepField) * std::max<size_t>(hclass_.size(), 1)));
+  if (!hclass_.empty())
+    MCK(cudaMemcpyAsync(classbuf_.p, hclass_.data(), sizeof(SweepField) * hclass_.size(),
+                        cudaMemcpyHostToDevice, st_));
+  for (FilterTable *T : pending) {  // stencil tables first needed by this rebuild
+    if (!T->wt.p || !T->nt.p) return fail(CCFV_ERR_NOMEM, "stencil table allocation failed");
+    const SweepClass &K = (T->level == 0 ? fine_ : coarse_).at(T->cls);
+    MCK(launch_filter_weights(T->fp64, classbuf_.as<SweepField>() + K.off + T->idx, T->wt.p,
+                              T->nt.as<int>(), T->lines, st_));
+    T->ready = true;
   }
   const int eb = 148;
   MCK(elems_.alloc(sizeof(BElem) * std::max(n, 1)));
@@ -444,9 +460,20 @@ int MultiEngine::push_nlo() {
   return CCFV_OK;
 }
 
+// Host mirror of batch_elem_kernel's per-instance guard.
+bool MultiEngine::elem_active(int op, int n) const {
+  for (size_t i = 0; i < slots_.size(); ++i) {
+    const Problem *P = slots_[i].get();
+    if (!P || P->state == Problem::DONE) continue;  // zeroed element: S = 0
+    if (op == OP_LOAD_W_STD && P->o.form != CCFV_FORM_STANDARD) continue;
+    if (n < P->S && n >= nlo_[i]) return true;
+  }
+  return false;
+}
+
 int MultiEngine::elem(int op, int slice) {
   const int n = (int)slots_.size();
-  if (!n) return CCFV_OK;
+  if (!n || !elem_active(op, slice)) return CCFV_OK;
   count_launch();
   batch_elem_kernel<<<dim3(148, n), BT, 0, st_>>>(op, elems_.as<BElem>(), slice, nlo_d_.as<int>(),
                                                    partial_.as<double>(), counters_.as<unsigned>());
@@ -464,10 +491,14 @@ int MultiEngine::sweeps(std::map<KKey, SweepClass> &classes, int kind, int jstep
   for (auto &kv : classes) {
     SweepClass &K = kv.second;
     if (K.kind != kind) continue;
+    bool any = false;  // the kernel's own guard, evaluated here on the host copy of nlo
+    for (const SweepField &f : K.h)
+      if ((any = field_active(f, jstep, nslice, nlo_.data()))) break;
+    if (!any) continue;
     cudaError_t e =
-        K.fp64 ? launch_sweep_batch<double>(K.variant, K.d.as<SweepField>(), (int)K.h.size(), 0, K.groups,
+        K.fp64 ? launch_sweep_batch<double>(K.variant, classbuf_.as<SweepField>() + K.off, (int)K.h.size(), 0, K.groups,
                                             K.cs, K.lc_max, K.halo, bs, status, st_)
-               : launch_sweep_batch<float>(K.variant, K.d.as<SweepField>(), (int)K.h.size(), 0, K.groups,
+               : launch_sweep_batch<float>(K.variant, classbuf_.as<SweepField>() + K.off, (int)K.h.size(), 0, K.groups,
                                            K.cs, K.lc_max, K.halo, bs, status, st_);
     MCK(e);
   }
@@ -486,8 +517,10 @@ int MultiEngine::iterate(std::vector<int> *finished) {
   if (dirty_)
     if (int rc = rebuild()) return rc;
   const int n = (int)slots_.size();
-  cudaEvent_t e0, e1;
+  cudaEvent_t e0, ef, ef2, e1;
   MCK(cudaEventCreate(&e0));
+  MCK(cudaEventCreate(&ef));
+  MCK(cudaEventCreate(&ef2));
   MCK(cudaEventCreate(&e1));
   MCK(cudaEventRecord(e0, st_));
   // first coarse sweep U[s+1] = G(U[s]) of newly admitted problems
@@ -538,9 +571,11 @@ int MultiEngine::iterate(std::vector<int> *finished) {
   if (running) {
     if (int rc = push_nlo()) return rc;
     // F[s+1] = F(U[s]): the fine sequences read U[s] in their first sweep
+    MCK(cudaEventRecord(ef, st_));
     for (int j = 0; j < Jmax; ++j)
       for (int kind = 0; kind < 3; ++kind)
         if (int rc = sweeps(fine_, kind, j, 0)) return rc;
+    MCK(cudaEventRecord(ef2, st_));
     for (int s = 0; s < Smax; ++s) {
       int rc = any_std ? elem(OP_LOAD_W_STD, s) : CCFV_OK;
       if (!rc) rc = coarse_slice(s, mmax);
@@ -555,7 +590,14 @@ int MultiEngine::iterate(std::vector<int> *finished) {
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
   ms_ += ms;
+  if (running) {
+    float fms = 0;
+    cudaEventElapsedTime(&fms, ef, ef2);
+    fine_ms_ += fms;
+  }
   cudaEventDestroy(e0);
+  cudaEventDestroy(ef);
+  cudaEventDestroy(ef2);
   cudaEventDestroy(e1);
   unsigned flag = 0;
   MCK(cudaMemcpy(&flag, status_.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
@@ -615,7 +657,12 @@ int batch_solve(int n, const ccfv_problem *probs, ccfv_stats *stats, int device,
   }
   if (cudaStreamSynchronize(st) != cudaSuccess) return bail(CCFV_ERR_CUDA);
   if (stats)
-    for (int i = 0; i < n; ++i) fill_stats(*E.get(slot[i]), &stats[i], E.device_ms());
+    for (int i = 0; i < n; ++i) {
+      fill_stats(*E.get(slot[i]), &stats[i], E.device_ms());
+      // phases are shared by the whole batch: engine-wide device times
+      stats[i].fine_ms = E.fine_ms();
+      stats[i].coarse_ms = E.device_ms() - E.fine_ms();
+    }
   return CCFV_OK;
 }
 

@@ -12,6 +12,21 @@
 
 namespace ccfv {
 
+// Per-line stencil table of the filter kernel for one (sub-step kind, level,
+// precision) of a problem; `cls`/`idx` locate a descriptor that uses it in
+// the launch classes of the rebuild that first needs it (the weights are
+// computed once, then kept while the problem lives).
+struct FilterTable {
+  DevBuf wt, nt;
+  int lines = 0;
+  bool fp64 = true;
+  bool ready = false;
+  int level = 0;  // 0: fine class, 1: coarse class
+  std::tuple<int, int, int, int, int> cls;
+  size_t idx = 0;
+};
+using FilterTables = std::map<std::tuple<int, int, int>, FilterTable>;  // kind, level, fp64
+
 // One live problem.  Its slice states stay resident on the device from
 // admission until it finishes.
 struct Problem {
@@ -21,6 +36,7 @@ struct Problem {
   double *C_T = nullptr;
   int S = 0, J = 0, m = 0;
   double DT = 0, dt = 0, dtc = 0;
+  double theta = 0.5;        // diffusion weight of the coarse steps
   long long NN = 0;
   bool g64 = true;
   void *mem = nullptr;       // cudaMallocAsync arena: U, F, FS, Gold, W, W2
@@ -32,6 +48,7 @@ struct Problem {
   // fine x, fine y, coarse x, coarse y (coarse precision), coarse x, y in
   // FP64 (the first coarse sweep, which always runs in FP64)
   const SolverTable *tab[6] = {};
+  FilterTables ftab;         // stencil tables of its filter-kernel fields
   enum { NEW, RUNNING, DONE } state = NEW;
   int k = 0;                 // iterations done
   int converged = 0;
@@ -46,23 +63,14 @@ size_t problem_bytes(const ccfv_grid &g, const ccfv_parareal_opts &o);
 // Validates options and fills the derived sizes; no device work.
 int problem_setup(Problem &P, const ccfv_problem &p, std::string *err);
 
+// A launch class: its descriptors sit at `off` in the engine's descriptor
+// buffer (one grow-only allocation and one upload for all classes).
 struct SweepClass {
   int kind = 0, variant = 0, cs = 1, lc_max = 0, halo = 0, fp64 = 1;
   std::vector<SweepField> h;
-  DevBuf d;
+  size_t off = 0;
   int groups = 0;
 };
-
-// Per-line stencil table of the filter kernel for one (problem, sub-step
-// kind, level, precision); `cls`/`idx` locate a descriptor that uses it.
-struct FilterTable {
-  DevBuf wt, nt;
-  int lines = 0;
-  bool fp64 = true;
-  std::tuple<int, int, int, int, int> cls;
-  size_t idx = 0;
-};
-using FilterTables = std::map<std::tuple<int, int, int, int>, FilterTable>;
 
 class MultiEngine {
  public:
@@ -88,11 +96,15 @@ class MultiEngine {
   int live() const;
   const std::string &error() const { return err_; }
   double device_ms() const { return ms_; }
+  // device time of the F phases (the rest of device_ms is coarse sweeps,
+  // corrections and norms)
+  double fine_ms() const { return fine_ms_; }
 
  private:
   int rebuild();
   int push_nlo();
   int elem(int op, int slice);
+  bool elem_active(int op, int slice) const;
   int sweeps(std::map<std::tuple<int, int, int, int, int>, SweepClass> &cls, int kind, int jstep,
              int nslice);
   int coarse_slice(int s, int mmax);
@@ -106,13 +118,14 @@ class MultiEngine {
   std::vector<std::unique_ptr<Problem>> slots_;
   bool dirty_ = true;
   std::map<std::tuple<int, int, int, int, int>, SweepClass> fine_, coarse_;
-  FilterTables ftabs_;
+  DevBuf classbuf_;  // SweepField descriptors of every class
+  std::vector<SweepField> hclass_;
   DevBuf elems_, nlo_d_, partial_, counters_, status_, norms_d_;
   std::vector<int> nlo_;
   std::vector<size_t> norm_off_;
   std::vector<double> hnorms_;
   std::string err_;
-  double ms_ = 0;
+  double ms_ = 0, fine_ms_ = 0;
 };
 
 }  // namespace ccfv

@@ -112,16 +112,8 @@ struct LineFeet {
   }
 };
 
-// Whether a field takes part in a batched launch, and its launch time offset.
-__device__ __forceinline__ bool field_active(const SweepField &f, int jstep, int nslice,
-                                             const int *nlo) {
-  if (f.jmax > 0 && jstep >= f.jmax) return false;
-  if (!nlo) return true;
-  const int lo = nlo[f.inst];
-  if (f.slice >= 0) return f.slice >= lo;
-  if ((f.phase == 1 && lo >= 0) || (f.phase == 2 && lo < 0)) return false;
-  return nslice < f.smax && nslice >= lo + f.gskip;
-}
+// A field's launch time offset (field_active, ccfv_internal.h, says whether
+// it takes part in a batched launch).
 __device__ __forceinline__ double field_time(const SweepField &f, double toff, int jstep,
                                              int nslice) {
   return toff + jstep * f.t_step + (f.slice < 0 ? nslice * f.t_slice : 0.0);

@@ -5,8 +5,9 @@
 //   T_min, T_max, N, Nt, T_span, K
 // plus optional keys of this solver
 //   slices (40), kmax (8), tol (0), coarse_ratio (0 = one coarse step per
-//   slice), coarse (fp64|fp32), form (standard|delta), scheme
-//   (reference|consistent), bc (compat|periodic), dump (1|0), device (0)
+//   slice), coarse (fp64|fp32), form (standard|delta), coarse_theta (0.5 =
+//   Crank-Nicolson G, 1 = backward Euler G), scheme (reference|consistent),
+//   bc (compat|periodic), dump (1|0), device (0)
 // and runs what the reference's main() runs: the initial condition, the
 // serial fine solve with gnuplot dumps every T_span steps
 // (data_T2S4_%06d.txt, T2S4:93-114), then Parareal with the per-iteration
@@ -156,6 +157,7 @@ int main(int argc, char **argv) {
                : CCFV_FORM_STANDARD;
   o.mem = CCFV_MEM_DEVICE;
   o.d_ref = d_ref;
+  o.coarse_theta = num("coarse_theta", 0.5);  // 0.5: Crank-Nicolson G (reference), 1: backward Euler
   ccfv_stats st;
   CHECK(ccfv_parareal(ctx, &o, d_C0, d_UT, &st, nullptr));
   for (int k = 0; k < st.iterations && k < CCFV_MAX_ITERS; ++k)

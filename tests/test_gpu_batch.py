@@ -40,6 +40,13 @@ def _problems(ccfv):
         C0 = periodic_field(N, int(rng.integers(1000)))
         probs.append(dict(grid=g, C0=C0, t0=0.0, t1=0.25, nt_fine=nt, n_slices=S,
                           coarse_ratio=ratio, tol=tol, kmax=3, coarse_precision=prec, form=form))
+    # stiff diffusion (K dtc/h^2 of 5 - 13) with damped coarse steps: the
+    # automatic weight in FP32 (delta form) and a fixed 0.8 in FP64 (standard)
+    for N, K, prec, form, th in ((64, 5e-2, 1, 1, ccfv.COARSE_THETA_AUTO), (90, 2e-2, 0, 0, 0.8)):
+        g = ccfv.make_grid(N, bc=1, velocity=1, vel_params=(0.6, -0.4), K=K, scheme=1)
+        probs.append(dict(grid=g, C0=periodic_field(N, int(rng.integers(1000))), t0=0.0, t1=0.25,
+                          nt_fine=64, n_slices=8, coarse_ratio=2, tol=0.0, kmax=3,
+                          coarse_precision=prec, form=form, coarse_theta=th))
     return probs
 
 
@@ -52,7 +59,7 @@ def test_batch_matches_individual_solves(ccfv):
         out, st = s.parareal(dev(p["C0"]), t0=p["t0"], t1=p["t1"], nt_fine=p["nt_fine"],
                              n_slices=p["n_slices"], coarse_ratio=p["coarse_ratio"],
                              tol=p["tol"], kmax=p["kmax"], coarse_precision=p["coarse_precision"],
-                             form=p["form"])
+                             form=p["form"], coarse_theta=p.get("coarse_theta", 0.5))
         alone.append((out.cpu().numpy(), st))
     batch = []
     for p in probs:

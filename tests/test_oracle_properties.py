@@ -138,3 +138,43 @@ def test_parareal_with_source_converges_to_serial_fine(oracle, form):
                                   coarse_steps=2, tol=0.0, kmax=S, form=form)
     assert it == S
     assert rel_l2(UT, fine) < 1e-13
+
+
+@pytest.mark.parametrize("theta", [0.5, 0.8, 1.0])
+def test_theta_step_damps_grid_scale_mode_as_derived(oracle, theta):
+    """Zero velocity: one split step multiplies the checkerboard mode by
+    a(nu/2)^2 a(nu), a(nu) = (2/3 - 32/9 (1-theta) nu) / (2/3 + 4 theta nu),
+    the amplification the automatic coarse weight is derived from."""
+    N, K, dt = 32, 0.05, 0.02
+    g = oracle.grid(N, bc=oracle.BC_PERIODIC, vel=oracle.VEL_CONST, vp=(0.0, 0.0), K=K,
+                    threads=4, scheme=1, theta=theta)
+    i = np.arange(N)
+    C0 = np.where((i[:, None] + i[None, :]) % 2 == 0, 1.0, -1.0)
+    out = oracle.step(g, C0, 0.0, dt)
+    nu = K * dt * N * N
+
+    def a(n):
+        return (2 / 3 - 32 / 9 * (1 - theta) * n) / (2 / 3 + 4 * theta * n)
+
+    np.testing.assert_allclose(out, a(nu / 2) ** 2 * a(nu) * C0, rtol=1e-10, atol=1e-14)
+
+
+def test_auto_coarse_theta_restores_convergence(oracle):
+    """Stiff diffusion (K dtc/h^2 = 6.4, one coarse step per slice, 64
+    slices): Crank-Nicolson coarse steps stall Parareal; the automatic weight
+    converges in a few iterations to the serial fine solve, its fixed point
+    whatever G is."""
+    N, S, K, V = 64, 64, 0.1, (1.0, 0.5)
+    g = oracle.grid(N, bc=oracle.BC_PERIODIC, vel=oracle.VEL_CONST, vp=V, K=K, threads=8,
+                    scheme=1)
+    C0 = oracle.gaussians(g, [0.4, 0.7], [0.6, 0.3], [2 * 0.06 ** 2, 2 * 0.04 ** 2], [1.0, 0.5],
+                          img=1)
+    nt = 512  # dt = 1/512 (CFL 0.125), 8 fine steps per slice
+    fine = oracle.run(g, C0, 0.0, 1.0 / nt, nt)
+    kw = dict(t0=0.0, t1=1.0, nt_fine=nt, n_slices=S, coarse_steps=1, tol=1e-10, kmax=12,
+              form=oracle.FORM_DELTA)
+    _, it_cn, upd_cn = oracle.parareal(g, C0, **kw)
+    assert upd_cn[-1] > 1e-6, upd_cn
+    UT, it, upd = oracle.parareal(g, C0, coarse_theta=oracle.COARSE_THETA_AUTO, **kw)
+    assert it <= 12 and upd[-1] < 1e-10, upd
+    assert rel_l2(UT, fine) < 1e-9
