@@ -146,44 +146,61 @@ using KKey = std::tuple<int, int, int, int, int>;  // kind, variant, cs, lc buck
 // cluster size (segments per line).  Filter-kernel fields carry their own
 // segment length and halo, so they share a class across segment lengths; the
 // scan kernels also group by segment-length bucket.
-static void add_field(std::map<KKey, SweepClass> &classes, int kind, const ccfv_grid &g,
-                      const SweepField &f0, bool fp64, FilterTables *tabs,
-                      std::tuple<int, int, int> tkey, std::vector<FilterTable *> *pending) {
-  const LaunchGeom G = step_geom(g, f0.dir, f0.Dt, f0.dsrc, fp64, /*inplace=*/false, f0.theta);
-  const bool filt = G.variant == SWEEP_FILTER;
-  const int bucket = filt ? 0 : (G.lc_max + 63) / 64;  // segment-length bucket bounds the tile
-  SweepClass &K = classes[KKey{kind, G.variant, G.cs, bucket, fp64 ? 1 : 0}];
-  K.kind = kind;
-  K.variant = G.variant;
-  K.cs = G.cs;
-  K.fp64 = fp64 ? 1 : 0;
-  K.lc_max = std::max(K.lc_max, G.lc_max);
-  K.halo = std::max(K.halo, G.halo);
-  SweepField f = f0;
-  f.group0 = K.groups;
-  f.cta0 = K.groups * G.cs;
-  f.halo_f = G.halo;
+static void prepare_field(std::vector<PreparedField> &out, int kind, const ccfv_grid &g,
+                          const SweepField &f0, bool fp64, FilterTables *tabs,
+                          std::tuple<int, int, int> tkey) {
+  PreparedField pf;
+  pf.G = step_geom(g, f0.dir, f0.Dt, f0.dsrc, fp64, /*inplace=*/false, f0.theta);
+  const bool filt = pf.G.variant == SWEEP_FILTER;
+  const int bucket = filt ? 0 : (pf.G.lc_max + 63) / 64;  // segment-length bucket bounds the tile
+  pf.key = KKey{kind, pf.G.variant, pf.G.cs, bucket, fp64 ? 1 : 0};
+  pf.level = std::get<1>(tkey);
+  pf.f = f0;
+  pf.f.halo_f = pf.G.halo;
   if (filt) {
-    filter_field(g, f, fp64);
+    filter_field(g, pf.f, fp64);
     FilterTable &T = (*tabs)[tkey];  // shared by every field of this key
     if (!T.lines) {
-      T.lines = f.groups * LPG;
+      T.lines = pf.f.groups * LPG;
       T.fp64 = fp64;
+      T.level = pf.level;
       T.wt.alloc((fp64 ? 8 : 4) * 8 * (size_t)T.lines);
       T.nt.alloc(sizeof(int) * (size_t)T.lines);
     }
-    if (!T.ready && (pending->empty() || pending->back() != &T) &&
-        std::find(pending->begin(), pending->end(), &T) == pending->end()) {
-      T.cls = KKey{kind, G.variant, G.cs, bucket, fp64 ? 1 : 0};
-      T.idx = K.h.size();
-      T.level = std::get<1>(tkey);
-      pending->push_back(&T);
-    }
-    f.wt = T.wt.p;
-    f.nt = T.nt.as<int>();
+    pf.f.wt = T.wt.p;
+    pf.f.nt = T.nt.as<int>();
+    pf.T = &T;
   }
+  out.push_back(pf);
+}
+
+static void place_field(std::map<KKey, SweepClass> &classes, const PreparedField &pf,
+                        std::vector<FilterTable *> *pending) {
+  SweepClass &K = classes[pf.key];
+  K.kind = std::get<0>(pf.key);
+  K.variant = pf.G.variant;
+  K.cs = pf.G.cs;
+  K.fp64 = std::get<4>(pf.key);
+  K.lc_max = std::max(K.lc_max, pf.G.lc_max);
+  K.halo = std::max(K.halo, pf.G.halo);
+  FilterTable *T = pf.T;
+  if (T && !T->ready && (pending->empty() || pending->back() != T) &&
+      std::find(pending->begin(), pending->end(), T) == pending->end()) {
+    T->cls = pf.key;
+    T->idx = K.h.size();
+    pending->push_back(T);
+  }
+  K.jmax_all = (K.jmax_all < 0 || pf.f.jmax == 0 || K.jmax_all == 0)
+                   ? (K.jmax_all < 0 ? pf.f.jmax : 0)
+                   : std::max(K.jmax_all, pf.f.jmax);
+  const int sm = pf.f.slice >= 0 ? 0 : pf.f.smax;  // fixed-slice fields: no slice bound
+  K.smax_all = (K.smax_all < 0 || sm == 0 || K.smax_all == 0) ? (K.smax_all < 0 ? sm : 0)
+                                                              : std::max(K.smax_all, sm);
+  K.h.push_back(pf.f);
+  SweepField &f = K.h.back();
+  f.group0 = K.groups;
+  f.cta0 = K.groups * pf.G.cs;
   K.groups += f.groups;
-  K.h.push_back(f);
 }
 
 size_t problem_bytes(const ccfv_grid &g, const ccfv_parareal_opts &o) {
@@ -354,7 +371,7 @@ int MultiEngine::rebuild() {
     // coarse sequences start in W and end in W2 when 3m is odd
     he[i] = BElem{P->U, P->F, P->Gold, P->W, ((3 * P->m) & 1) ? P->W2 : P->W, P->NN, P->S,
                   P->o.form, P->g64 ? 1 : 0, 0, norms_d_.as<double>() + norm_off_[i]};
-    for (int kind = 0; kind < 3; ++kind) {
+    for (int kind = 0; kind < 3 && !P->prepared; ++kind) {
       const int dir = kind == 1 ? 1 : 0;
       const int dsrc = (kind == 2 && g.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
       {  // fine: field s = F[s+1], time t0 + s DT (+ j dt per launch step)
@@ -374,7 +391,7 @@ int MultiEngine::rebuild() {
           f.data2 = P->FS + (size_t)s * P->NN;
           f.in0 = P->U + (size_t)s * P->NN;
           f.par = pp_parity(P->J);
-          add_field(fine_, kind, g, f, true, &P->ftab, std::make_tuple(kind, 0, 1), &pending);
+          prepare_field(P->prep, kind, g, f, true, &P->ftab, std::make_tuple(kind, 0, 1));
         }
       }
       {  // coarse: the work field W, slice from the launch (t0 + n DT + i dtc)
@@ -401,21 +418,23 @@ int MultiEngine::rebuild() {
         };
         const bool delta_src = g.source != CCFV_SRC_NONE && P->o.form == CCFV_FORM_DELTA;
         if (P->g64 && !delta_src) {
-          add_field(coarse_, kind, g, coarse_field(g, P->tab[2 + dir], 0), true, &P->ftab,
-                    std::make_tuple(kind, 1, 1), &pending);
+          prepare_field(P->prep, kind, g, coarse_field(g, P->tab[2 + dir], 0), true, &P->ftab,
+                        std::make_tuple(kind, 1, 1));
         } else {
           // the first sweep moves states: FP64, with the source; the
           // iterations move increments in the coarse precision (delta form:
           // with the linear part of G, without the source)
-          add_field(coarse_, kind, g, coarse_field(g, P->tab[4 + dir], 1), true, &P->ftab,
-                    std::make_tuple(kind, 1, 1), &pending);
+          prepare_field(P->prep, kind, g, coarse_field(g, P->tab[4 + dir], 1), true, &P->ftab,
+                        std::make_tuple(kind, 1, 1));
           ccfv_grid gh = g;
           if (P->o.form == CCFV_FORM_DELTA) gh.source = CCFV_SRC_NONE;
-          add_field(coarse_, kind, gh, coarse_field(gh, P->tab[2 + dir], 2), P->g64, &P->ftab,
-                    std::make_tuple(kind, 1, P->g64 ? 1 : 0), &pending);
+          prepare_field(P->prep, kind, gh, coarse_field(gh, P->tab[2 + dir], 2), P->g64,
+                        &P->ftab, std::make_tuple(kind, 1, P->g64 ? 1 : 0));
         }
       }
     }
+    P->prepared = true;
+    for (const PreparedField &pf : P->prep) place_field(pf.level == 0 ? fine_ : coarse_, pf, &pending);
   }
   hclass_.clear();
   for (auto *cls : {&fine_, &coarse_})
@@ -491,6 +510,8 @@ int MultiEngine::sweeps(std::map<KKey, SweepClass> &classes, int kind, int jstep
   for (auto &kv : classes) {
     SweepClass &K = kv.second;
     if (K.kind != kind) continue;
+    if ((K.jmax_all > 0 && jstep >= K.jmax_all) || (K.smax_all > 0 && nslice >= K.smax_all))
+      continue;
     bool any = false;  // the kernel's own guard, evaluated here on the host copy of nlo
     for (const SweepField &f : K.h)
       if ((any = field_active(f, jstep, nslice, nlo_.data()))) break;

@@ -27,6 +27,16 @@ struct FilterTable {
 };
 using FilterTables = std::map<std::tuple<int, int, int>, FilterTable>;  // kind, level, fp64
 
+// A sweep descriptor of a problem, prepared once (launch geometry, filter
+// constants, stencil table); a rebuild only places it into its launch class.
+struct PreparedField {
+  std::tuple<int, int, int, int, int> key;  // launch class
+  int level = 0;                            // 0: fine, 1: coarse
+  LaunchGeom G;
+  FilterTable *T = nullptr;                 // filter kernel: its stencil table
+  SweepField f;
+};
+
 // One live problem.  Its slice states stay resident on the device from
 // admission until it finishes.
 struct Problem {
@@ -49,6 +59,8 @@ struct Problem {
   // FP64 (the first coarse sweep, which always runs in FP64)
   const SolverTable *tab[6] = {};
   FilterTables ftab;         // stencil tables of its filter-kernel fields
+  std::vector<PreparedField> prep;  // its sweep descriptors (built at the first rebuild)
+  bool prepared = false;
   enum { NEW, RUNNING, DONE } state = NEW;
   int k = 0;                 // iterations done
   int converged = 0;
@@ -70,6 +82,9 @@ struct SweepClass {
   std::vector<SweepField> h;
   size_t off = 0;
   int groups = 0;
+  // bounds over the fields (0: some field has no bound): a launch with
+  // jstep >= jmax_all or nslice >= smax_all has no active field
+  int jmax_all = -1, smax_all = -1;
 };
 
 class MultiEngine {
