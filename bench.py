@@ -558,6 +558,13 @@ def run_batch(a, ws, rank, local):
     if rank == 0:
         its = [x["iterations"] for x in st]
         conv = sum(1 for x in st if x["converged"])
+        # the batch's shared F phases: 48 algorithmic bytes per executed fine
+        # cell-update (3 FP64 sweeps, read + write)
+        fine_cu = float(sum(x["fine_cell_updates"] for x in st))
+        peak, peak_kind = measured_peak()
+        f_gbs = 48.0 * fine_cu / (st[0]["fine_ms"] * 1e-3) / 1e9 if st[0]["fine_ms"] else None
+        fine_phase = {"executed_fine_cell_updates": fine_cu, "achieved_gbs": f_gbs, "peak_gbs": peak,
+                      "frac": (f_gbs / peak) if f_gbs else None, "peak_source": peak_kind}
         print(json.dumps(dict(
             metric="parareal_cell_updates_per_s", value=value, unit="cell-updates/s",
             mode="batch", n_gpus=ws, steps=a.steps, warmup=a.warmup,
@@ -572,7 +579,7 @@ def run_batch(a, ws, rank, local):
                     "plain": "each instance alone, FP64 Crank-Nicolson coarse steps "
                              f"({len(sample)} instances)"},
             iterations_mean=float(np.mean(its)), converged=conv, instances=len(st),
-            fine_ms=st[0]["fine_ms"], coarse_ms=st[0]["coarse_ms"],
+            fine_ms=st[0]["fine_ms"], coarse_ms=st[0]["coarse_ms"], fine_phase=fine_phase,
             plain_fp64_single_instance_cell_updates_per_s=plain,
             batched_vs_plain=(value / ws / plain) if plain else None,
             plain_fp64_same_coarse_theta_cell_updates_per_s=plain_th,
