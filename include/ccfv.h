@@ -323,11 +323,13 @@ int ccfv_autotune(ccfv_ctx *ctx, double dt, int precision, int *segment, void *s
  * reference): variant[s] for s = x(dt/2), y(dt), x(dt/2)
  * is CCFV_SWEEP_GENERAL (per-cell feet), CCFV_SWEEP_UNIFORM (shared-foot
  * stencil with exact chunked scans), CCFV_SWEEP_FILTER (shared-foot stencil
- * with the factored cyclic solve) or CCFV_SWEEP_SOURCE (per-cell, with the
- * source term); segment[s] = cells per CTA along a line (either may be NULL).
+ * with the factored cyclic solve), CCFV_SWEEP_SOURCE (per-cell, with the
+ * source term) or CCFV_SWEEP_FILTER_EXACT (the factored solve with the
+ * periodic closure taken exactly across a line's segments: strong
+ * diffusion); segment[s] = cells per CTA along a line (either may be NULL).
  * No device work. */
 enum { CCFV_SWEEP_GENERAL = 0, CCFV_SWEEP_UNIFORM = 1, CCFV_SWEEP_FILTER = 2,
-       CCFV_SWEEP_SOURCE = 3 };
+       CCFV_SWEEP_SOURCE = 3, CCFV_SWEEP_FILTER_EXACT = 4 };
 int ccfv_sweep_plan(ccfv_ctx *ctx, double dt, int precision, int variant[3], int segment[3]);
 
 /* ---- library info ---------------------------------------------------- */

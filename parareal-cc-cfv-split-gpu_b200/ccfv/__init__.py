@@ -285,7 +285,7 @@ class Solver:
                                       _stream_ptr(stream)))
         return seg.value
 
-    SWEEP_NAMES = ("general", "uniform", "filter", "source")
+    SWEEP_NAMES = ("general", "uniform", "filter", "source", "filter_exact")
 
     def sweep_plan(self, dt, precision=FP64):
         """Kernel variant and segment length of the three sub-steps of a step
@@ -295,7 +295,8 @@ class Solver:
         return [(self.SWEEP_NAMES[v[i]], sg[i]) for i in range(3)]
 
     SWEEP_KERNELS = {"general": "sweep_kernel", "uniform": "sweep_fast_kernel",
-                     "filter": "sweep_filter_kernel", "source": "sweep_kernel"}
+                     "filter": "sweep_filter_kernel", "source": "sweep_kernel",
+                     "filter_exact": "sweep_filter_kernel"}
 
     def variant_names(self, dt, precision=FP64):
         """Names of the sweep kernels a step of dt launches (x, y, x)."""

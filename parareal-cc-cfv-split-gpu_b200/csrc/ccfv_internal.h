@@ -114,14 +114,18 @@ constexpr size_t FD_BYTES = (sizeof(SweepField) + 63) & ~size_t(63);
 // Kernel variants: the per-cell kernel (any velocity / boundary / scheme) and
 // the fused stencil kernel (uniform displacement, periodic, derivative of the
 // sweep input).
-// SWEEP_GENERAL_SRC is the per-cell kernel with the source tile staged.
-enum { SWEEP_GENERAL = 0, SWEEP_FAST = 1, SWEEP_FILTER = 2, SWEEP_GENERAL_SRC = 3 };
+// SWEEP_GENERAL_SRC is the per-cell kernel with the source tile staged;
+// SWEEP_FILTER_EXACT the filter kernel's cluster form (any diffusion number,
+// out of place).
+enum { SWEEP_GENERAL = 0, SWEEP_FAST = 1, SWEEP_FILTER = 2, SWEEP_GENERAL_SRC = 3,
+       SWEEP_FILTER_EXACT = 4 };
+inline bool filter_variant(int v) { return v == SWEEP_FILTER || v == SWEEP_FILTER_EXACT; }
 constexpr int FILTER_JMAX = 64;  // longest recurrence warm-up of the filter kernel
 
 // Shared-memory bytes of the sweep kernels for a launch.
 size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source = false);
 size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64);
-size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64);
+size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact = false);
 // Longest segment (cells per CTA along a line) of the filter kernel for a
 // recurrence warm-up of J cells.
 int filter_segment_max(int J);
@@ -151,6 +155,7 @@ struct BatchStep {
   int jstep = 0, nslice = 0;
   const int *nlo = nullptr;
   bool inplace = true;
+  const int *g0idx = nullptr;  // the fields' group0 values (device), or null
 };
 template <typename T>
 cudaError_t launch_sweep_batch(int variant, const SweepField *d_fields, int nfields,

@@ -292,7 +292,18 @@ LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64
   G.variant = g.source ? SWEEP_GENERAL_SRC : SWEEP_GENERAL;
   if (!g.source && uniform && g.bc == CCFV_BC_PERIODIC && dsrc == 0) {
     int J = 0;
-    if (filter_params(g, dir, Dt, fp64, nullptr, nullptr, &J, theta) && L > 2 * J) {
+    const bool warm = filter_params(g, dir, Dt, fp64, nullptr, nullptr, &J, theta) && L > 2 * J;
+    const int seg_exact = filter_segment_max(0);  // cells per CTA without warm-up
+    if (!warm && !inplace && (L + seg_exact - 1) / seg_exact <= MAX_CLUSTER) {
+      // strong diffusion, out of place: the filter kernel's cluster form
+      // (exact periodic closure across the segments, no warm-up)
+      const int lc = std::min(seg_exact, std::max({32, (L + MAX_CLUSTER - 1) / MAX_CLUSTER,
+                                                   std::min(L, filter_lc(L, fp64))}));
+      G.variant = SWEEP_FILTER_EXACT;
+      G.cs = (L + lc - 1) / lc;
+      G.lc_max = (L + G.cs - 1) / G.cs;
+      G.halo = sh + 6;
+    } else if (warm) {
       G.variant = SWEEP_FILTER;
       G.halo = J + sh + 6;
       // segment length from the tuner; the segments of a line form one
@@ -428,7 +439,7 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
     if (std::max({sweep_smem_bytes(G.lc_max, G.halo, fp64, g.source != 0),
                   sweep_fast_smem_bytes(G.lc_max, G.halo, fp64),
-                  sweep_filter_smem_bytes(G.lc_max, G.halo, fp64)}) > 227 * 1024)
+                  sweep_filter_smem_bytes(G.lc_max, G.halo, fp64, true)}) > 227 * 1024)
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
     for (int i = 0; i < nf; ++i) {
       const PlanField &pfi = fields[i];
@@ -440,7 +451,7 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
         f.in0 = pfi.in0;
         f.par = pfi.par;
       }
-      if (G.variant == SWEEP_FILTER) filter_field(g, f, fp64);
+      if (filter_variant(G.variant)) filter_field(g, f, fp64);
       f.src_tb = kind == 2 ? 1 : 0;
       f.group0 = i * f.groups;
       f.cta0 = f.group0 * G.cs;
@@ -457,7 +468,7 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
   // kernel do not depend on time)
   int lines[3] = {0, 0, 0};
   for (int kind = 0; kind < 3 && nf > 0; ++kind) {
-    if (plan->geom[kind].variant != SWEEP_FILTER) continue;
+    if (!filter_variant(plan->geom[kind].variant)) continue;
     lines[kind] = h[(size_t)kind * nf].groups * LPG;
     CK(plan->wt[kind].alloc((fp64 ? 8 : 4) * 8 * (size_t)lines[kind]));
     CK(plan->nt[kind].alloc(sizeof(int) * (size_t)lines[kind]));

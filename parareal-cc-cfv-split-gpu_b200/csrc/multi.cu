@@ -12,6 +12,7 @@
 // array, SweepField::jmax/smax), and the host, which holds the same `nlo`,
 // skips every launch in which no field or instance would take part.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -151,7 +152,7 @@ static void prepare_field(std::vector<PreparedField> &out, int kind, const ccfv_
                           std::tuple<int, int, int> tkey) {
   PreparedField pf;
   pf.G = step_geom(g, f0.dir, f0.Dt, f0.dsrc, fp64, /*inplace=*/false, f0.theta);
-  const bool filt = pf.G.variant == SWEEP_FILTER;
+  const bool filt = filter_variant(pf.G.variant);
   const int bucket = filt ? 0 : (pf.G.lc_max + 63) / 64;  // segment-length bucket bounds the tile
   pf.key = KKey{kind, pf.G.variant, pf.G.cs, bucket, fp64 ? 1 : 0};
   pf.level = std::get<1>(tkey);
@@ -186,21 +187,34 @@ static void place_field(std::map<KKey, SweepClass> &classes, const PreparedField
   FilterTable *T = pf.T;
   if (T && !T->ready && (pending->empty() || pending->back() != T) &&
       std::find(pending->begin(), pending->end(), T) == pending->end()) {
-    T->cls = pf.key;
-    T->idx = K.h.size();
+    T->cls = pf.key;  // T->idx is set once the class is sorted
     pending->push_back(T);
   }
-  K.jmax_all = (K.jmax_all < 0 || pf.f.jmax == 0 || K.jmax_all == 0)
-                   ? (K.jmax_all < 0 ? pf.f.jmax : 0)
-                   : std::max(K.jmax_all, pf.f.jmax);
   const int sm = pf.f.slice >= 0 ? 0 : pf.f.smax;  // fixed-slice fields: no slice bound
   K.smax_all = (K.smax_all < 0 || sm == 0 || K.smax_all == 0) ? (K.smax_all < 0 ? sm : 0)
                                                               : std::max(K.smax_all, sm);
   K.h.push_back(pf.f);
-  SweepField &f = K.h.back();
-  f.group0 = K.groups;
-  f.cta0 = K.groups * pf.G.cs;
-  K.groups += f.groups;
+}
+
+static int step_bound(const SweepField &f) { return f.jmax > 0 ? f.jmax : INT_MAX; }
+
+// Sorts a class by step bound (descending, stable: problem and slice order
+// kept within a bound) and numbers its tiles.
+static void finish_class(SweepClass &K) {
+  std::stable_sort(K.h.begin(), K.h.end(), [](const SweepField &a, const SweepField &b) {
+    return step_bound(a) > step_bound(b);
+  });
+  K.groups = 0;
+  K.bound.resize(K.h.size());
+  K.gpre.assign(K.h.size() + 1, 0);
+  for (size_t i = 0; i < K.h.size(); ++i) {
+    SweepField &f = K.h[i];
+    f.group0 = K.groups;
+    f.cta0 = K.groups * K.cs;
+    K.groups += f.groups;
+    K.bound[i] = step_bound(f);
+    K.gpre[i + 1] = K.groups;
+  }
 }
 
 size_t problem_bytes(const ccfv_grid &g, const ccfv_parareal_opts &o) {
@@ -292,7 +306,7 @@ int MultiEngine::add(const ccfv_problem &pr, int *slot) {
         return fail(CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
       if (std::max({sweep_smem_bytes(G.lc_max, G.halo, true, P->g.source != 0),
                     sweep_fast_smem_bytes(G.lc_max, G.halo, true),
-                    sweep_filter_smem_bytes(G.lc_max, G.halo, true)}) > 227 * 1024)
+                    sweep_filter_smem_bytes(G.lc_max, G.halo, true, true)}) > 227 * 1024)
         return fail(CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
     }
   MCK(cudaMallocAsync(&P->mem, P->bytes, st_));
@@ -437,16 +451,31 @@ int MultiEngine::rebuild() {
     for (const PreparedField &pf : P->prep) place_field(pf.level == 0 ? fine_ : coarse_, pf, &pending);
   }
   hclass_.clear();
+  hidx_.clear();
   for (auto *cls : {&fine_, &coarse_})
     for (auto &kv : *cls) {
       SweepClass &K = kv.second;
+      finish_class(K);
       K.off = hclass_.size();
+      K.ioff = hidx_.size();
       hclass_.insert(hclass_.end(), K.h.begin(), K.h.end());
+      for (const SweepField &f : K.h) hidx_.push_back(f.group0);
     }
+  for (FilterTable *T : pending) {  // a descriptor of each new table, after the sort
+    const SweepClass &K = (T->level == 0 ? fine_ : coarse_).at(T->cls);
+    size_t i = 0;
+    while (i < K.h.size() && K.h[i].wt != T->wt.p) ++i;
+    if (i == K.h.size()) return fail(CCFV_ERR_CUDA, "stencil table without a field");
+    T->idx = i;
+  }
   MCK(classbuf_.alloc(sizeof(SweepField) * std::max<size_t>(hclass_.size(), 1)));
-  if (!hclass_.empty())
+  MCK(idxbuf_.alloc(sizeof(int) * std::max<size_t>(hidx_.size(), 1)));
+  if (!hclass_.empty()) {
     MCK(cudaMemcpyAsync(classbuf_.p, hclass_.data(), sizeof(SweepField) * hclass_.size(),
                         cudaMemcpyHostToDevice, st_));
+    MCK(cudaMemcpyAsync(idxbuf_.p, hidx_.data(), sizeof(int) * hidx_.size(),
+                        cudaMemcpyHostToDevice, st_));
+  }
   for (FilterTable *T : pending) {  // stencil tables first needed by this rebuild
     if (!T->wt.p || !T->nt.p) return fail(CCFV_ERR_NOMEM, "stencil table allocation failed");
     const SweepClass &K = (T->level == 0 ? fine_ : coarse_).at(T->cls);
@@ -510,17 +539,21 @@ int MultiEngine::sweeps(std::map<KKey, SweepClass> &classes, int kind, int jstep
   for (auto &kv : classes) {
     SweepClass &K = kv.second;
     if (K.kind != kind) continue;
-    if ((K.jmax_all > 0 && jstep >= K.jmax_all) || (K.smax_all > 0 && nslice >= K.smax_all))
-      continue;
+    if (K.smax_all > 0 && nslice >= K.smax_all) continue;
+    // fields with a step bound above jstep: a prefix of the sorted class
+    const int np = (int)(std::partition_point(K.bound.begin(), K.bound.end(),
+                                              [&](int b) { return b > jstep; }) -
+                         K.bound.begin());
     bool any = false;  // the kernel's own guard, evaluated here on the host copy of nlo
-    for (const SweepField &f : K.h)
-      if ((any = field_active(f, jstep, nslice, nlo_.data()))) break;
+    for (int i = 0; i < np && !any; ++i) any = field_active(K.h[i], jstep, nslice, nlo_.data());
     if (!any) continue;
+    bs.g0idx = idxbuf_.as<int>() + K.ioff;
+    const SweepField *fd = classbuf_.as<SweepField>() + K.off;
     cudaError_t e =
-        K.fp64 ? launch_sweep_batch<double>(K.variant, classbuf_.as<SweepField>() + K.off, (int)K.h.size(), 0, K.groups,
-                                            K.cs, K.lc_max, K.halo, bs, status, st_)
-               : launch_sweep_batch<float>(K.variant, classbuf_.as<SweepField>() + K.off, (int)K.h.size(), 0, K.groups,
-                                           K.cs, K.lc_max, K.halo, bs, status, st_);
+        K.fp64 ? launch_sweep_batch<double>(K.variant, fd, np, 0, K.gpre[np], K.cs, K.lc_max,
+                                            K.halo, bs, status, st_)
+               : launch_sweep_batch<float>(K.variant, fd, np, 0, K.gpre[np], K.cs, K.lc_max,
+                                           K.halo, bs, status, st_);
     MCK(e);
   }
   return CCFV_OK;

@@ -76,15 +76,21 @@ size_t problem_bytes(const ccfv_grid &g, const ccfv_parareal_opts &o);
 int problem_setup(Problem &P, const ccfv_problem &p, std::string *err);
 
 // A launch class: its descriptors sit at `off` in the engine's descriptor
-// buffer (one grow-only allocation and one upload for all classes).
+// buffer and their group0 values at `ioff` in its index buffer (one
+// grow-only allocation and one upload each for all classes).  Fields are
+// sorted by their step bound (SweepField::jmax, 0 = none) in descending
+// order, so the fields active at step j form a prefix: a launch covers only
+// that prefix's tiles.
 struct SweepClass {
   int kind = 0, variant = 0, cs = 1, lc_max = 0, halo = 0, fp64 = 1;
   std::vector<SweepField> h;
-  size_t off = 0;
+  size_t off = 0, ioff = 0;
   int groups = 0;
-  // bounds over the fields (0: some field has no bound): a launch with
-  // jstep >= jmax_all or nslice >= smax_all has no active field
-  int jmax_all = -1, smax_all = -1;
+  std::vector<int> bound;  // step bound per field (jmax, 0 -> INT_MAX), descending
+  std::vector<int> gpre;   // gpre[i]: tiles of fields [0, i)
+  // slice bound over the fields (0: some field has none): a launch with
+  // nslice >= smax_all has no active field
+  int smax_all = -1;
 };
 
 class MultiEngine {
@@ -133,8 +139,9 @@ class MultiEngine {
   std::vector<std::unique_ptr<Problem>> slots_;
   bool dirty_ = true;
   std::map<std::tuple<int, int, int, int, int>, SweepClass> fine_, coarse_;
-  DevBuf classbuf_;  // SweepField descriptors of every class
+  DevBuf classbuf_, idxbuf_;  // SweepField descriptors and group0 indices of every class
   std::vector<SweepField> hclass_;
+  std::vector<int> hidx_;
   DevBuf elems_, nlo_d_, partial_, counters_, status_, norms_d_;
   std::vector<int> nlo_;
   std::vector<size_t> norm_off_;

@@ -112,6 +112,27 @@ struct LineFeet {
   }
 };
 
+// Field of tile `tile` (fields sorted by group0): binary search on the
+// launch's compact group0 index when it has one (batched launches of
+// thousands of fields: a few cache lines instead of one descriptor line per
+// probe), else on the descriptors.
+__device__ __forceinline__ int find_field(const SweepField *__restrict__ fields,
+                                          const int *__restrict__ g0idx, int nfields, int tile) {
+  int lo = 0, hi = nfields - 1;
+  if (g0idx) {
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(g0idx + mid) <= tile) lo = mid; else hi = mid - 1;
+    }
+  } else {
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(&fields[mid].group0) <= tile) lo = mid; else hi = mid - 1;
+    }
+  }
+  return lo;
+}
+
 // A field's launch time offset (field_active, ccfv_internal.h, says whether
 // it takes part in a batched launch).
 __device__ __forceinline__ double field_time(const SweepField &f, double toff, int jstep,
@@ -358,7 +379,7 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
                                                     int nfields, int group_base, double toff,
                                                     void *data_override, int lc_max, int H,
                                                     unsigned *status, int jstep, int nslice,
-                                                    const int *nlo) {
+                                                    const int *nlo, const int *g0idx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cg::cluster_group cluster = cg::this_cluster();
   const int cs = (int)cluster.num_blocks();
@@ -368,12 +389,7 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
 
   // ---- descriptor of this tile's field (binary search on group0) ----
   if (threadIdx.x == 0) {
-    int lo = 0, hi = nfields - 1;
-    while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if (fields[mid].group0 <= tile) lo = mid; else hi = mid - 1;
-    }
-    *S.fd = fields[lo];
+    *S.fd = fields[find_field(fields, g0idx, nfields, tile)];
     if (data_override) {
       S.fd->data = data_override;
       if (S.fd->pp) S.fd->in0 = data_override;
@@ -824,7 +840,7 @@ template <typename T>
 __global__ void __launch_bounds__(NTH, 2)
     sweep_fast_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
                       double toff, void *data_override, int lc_max, int H, unsigned *status,
-                      int jstep, int nslice, const int *nlo) {
+                      int jstep, int nslice, const int *nlo, const int *g0idx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cg::cluster_group cluster = cg::this_cluster();
   const int cs = (int)cluster.num_blocks();
@@ -833,11 +849,7 @@ __global__ void __launch_bounds__(NTH, 2)
   FastSmem<T> S = carve_fast<T>(smem_raw, lc_max, H);
   {
     // every thread finds the field; the descriptor is copied cooperatively
-    int lo = 0, hi = nfields - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (__ldg(&fields[mid].group0) <= tile) lo = mid; else hi = mid - 1;
-    }
+    const int lo = find_field(fields, g0idx, nfields, tile);
     constexpr int NW8 = (int)(sizeof(SweepField) / 8);
     if (threadIdx.x < NW8)
       reinterpret_cast<long long *>(S.fd)[threadIdx.x] =
@@ -1143,17 +1155,23 @@ __host__ __device__ inline int filter_tile_rows(int lc_max, int H) {
   return (lc_max > FLANES * FCH ? lc_max : FLANES * FCH) + 2 * H + 8;
 }
 
+// Exact (cluster) form: powers (-mu)^e for e = 0 .. FPW - 1 (a segment of at
+// most FLANES * FCH cells needs exponents up to FLANES * FCH).
+constexpr int FPW = FLANES * FCH + 8;
+
 template <typename T>
 struct FiltSmem {
   T *C;      // [filter_tile_rows * PITCH]  input cells, then w, then x
   T *om;     // [8 * LPG]  weights of w's input (1/c) M b as an 8-tap stencil of C
   T *pwt;    // [32]       (-mu)^(i+1), i = 0 .. FCH-1
+  T *pwa;    // exact form: [FPW] (-mu)^e
+  T *ex;     // exact form: [2 * LPG] this segment's forward end / backward start per line
   int *n0;   // [LPG]
   SweepField *fd;
   int rows;
 };
 
-template <typename T>
+template <typename T, bool EXACT>
 __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max, int H) {
   FiltSmem<T> s;
   s.fd = reinterpret_cast<SweepField *>(raw);
@@ -1161,9 +1179,26 @@ __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max
   T *p = reinterpret_cast<T *>(raw + FD_BYTES + 64 * sizeof(int));
   s.om = p; p += 8 * LPG;
   s.pwt = p; p += 32;
+  s.pwa = nullptr;
+  s.ex = nullptr;
+  if (EXACT) {
+    s.pwa = p; p += FPW;
+    s.ex = p; p += 2 * LPG;
+  }
   s.C = p;
   s.rows = filter_tile_rows(lc_max, H);
   return s;
+}
+
+// x^n (n >= 0) by binary powering, in FP64.
+__device__ __forceinline__ double powi(double x, int n) {
+  double r = 1.0;
+  while (n > 0) {
+    if (n & 1) r *= x;
+    x *= x;
+    n >>= 1;
+  }
+  return r;
 }
 
 // Stencil of line gl's w input: w_k = sum_{m=-3..4} om[m+3] C_{k+n0+m} - mu
@@ -1226,24 +1261,33 @@ __global__ void filter_weights_kernel(const SweepField *__restrict__ f, T *__res
 // more): the kernel is latency bound, and each added CTA was worth more than
 // the few registers it spills (2 -> 3 -> 4 CTAs: fine phase 1498 -> 1207 ->
 // 1105 us per launch on the 2048^2 x 63-slice bench).
-template <typename T>
+//
+// EXACT (out of place, any diffusion number): a line's cs segments form one
+// thread-block cluster and no recurrence is warmed up.  Each segment runs
+// both filters from a zero start over its own cells only; a segment maps its
+// incoming carry linearly, w_end = (-mu)^np w_in + E (forward) and
+// x_start = (-mu)^np x_in + X (backward), so after the segments publish E (X)
+// in shared memory the periodic closure over the cluster gives every carry
+// exactly: w_{L-1} = E_total / (1 - (-mu)^L), then carries segment by
+// segment; each cell adds carry * (-mu)^distance from a power table.  The
+// field, its activity and the segment length are uniform over a cluster, so
+// every CTA of a cluster reaches every cluster barrier.
+template <typename T, bool EXACT>
 __global__ void __launch_bounds__(NTH, 4)
     sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
                         double toff, void *data_override, int lc_max, int H, unsigned *status,
-                        int jstep, int nslice, const int *nlo, int cs, int clustered) {
+                        int jstep, int nslice, const int *nlo, int cs, int clustered,
+                        const int *g0idx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // CTA -> (field, tile of LPG lines, segment).  The launch's clusters are the
   // cs segments of one tile; fields carry their first CTA and halo, so fields
   // of different segment lengths share one launch (lc_max and H size the
   // shared memory only)
   const int cta = (int)blockIdx.x + group_base;
-  FiltSmem<T> S = carve_filt<T>(smem_raw, lc_max, H);
+  FiltSmem<T> S = carve_filt<T, EXACT>(smem_raw, lc_max, H);
   {
-    int lo = 0, hi = nfields - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (__ldg(&fields[mid].cta0) <= cta) lo = mid; else hi = mid - 1;
-    }
+    // a field's CTAs start at cta0 = group0 * cs (cs is uniform over a launch)
+    const int lo = find_field(fields, g0idx, nfields, cta / cs);
     constexpr int NW8 = (int)(sizeof(SweepField) / 8);
     if (threadIdx.x < NW8)
       reinterpret_cast<long long *>(S.fd)[threadIdx.x] =
@@ -1268,7 +1312,7 @@ __global__ void __launch_bounds__(NTH, 4)
   const int p1 = min(L, p0 + Lc);
   const int np = p1 - p0;
   const int nrows = np + 2 * H;
-  const int J = F.jf;
+  const int J = EXACT ? 0 : F.jf;
   const T mu = T(F.sm_fac), ic = T(F.sm_inv_den);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const T *gsrc;
@@ -1348,6 +1392,8 @@ __global__ void __launch_bounds__(NTH, 4)
       pk *= mmu;
     }
   }
+  if (EXACT)
+    for (int e = threadIdx.x; e < FPW; e += NTH) S.pwa[e] = T(powi(-F.sm_fac, e));
   cp_async_wait_all_committed();
   __syncthreads();
   // In place, the segments of a line are read (halo) by the neighbouring CTAs
@@ -1357,7 +1403,10 @@ __global__ void __launch_bounds__(NTH, 4)
   if (clustered) asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
 
   // ---- one line per half-warp, FCH positions per lane ----
-  if (np + 2 * J > FLANES * FCH) {  // the host keeps segments within filter_seg_max(J)
+  // (exact form: Lc bounds every segment of the cluster, so all its CTAs
+  // leave here together, before any cluster barrier)
+  if (EXACT ? Lc > FLANES * FCH : np + 2 * J > FLANES * FCH) {
+    // the host keeps segments within filter_seg_max(J) (exact: FLANES * FCH)
     if (threadIdx.x == 0) atomicOr(status, STATUS_HALO);
     return;
   }
@@ -1410,25 +1459,60 @@ __global__ void __launch_bounds__(NTH, 4)
 #pragma unroll
       for (int i = 0; i < FCH; ++i) v[i] += cin * S.pwt[i];
     }
-    // every stencil read of this line is done (the shuffles order the lanes);
-    // w of positions k0 .. k0+FCH-1 into this line's column
-    __syncwarp(fm);
-    {
-      T *wp = S.C + (k0 + rb) * PITCH + ln;
-#pragma unroll
-      for (int i = 0; i < FCH; ++i) wp[i * PITCH] = v[i];
-    }
-    __syncwarp(fm);
-
-    // backward: x over [p0, qb), zero start at qb
     const int k1 = p0 + c * FCH;
-    {
-      const T *xp = S.C + (k1 + rb) * PITCH + ln;
-      const int nb = qb - k1;
+    const int nb = qb - k1;  // positions of this lane inside the backward range
+    if (EXACT) {
+      // forward end of the segment from a zero carry (position p1 - 1)
+      const int cend = (np - 1) / FCH, iend = (np - 1) - cend * FCH;
+      T e = T(0);
+#pragma unroll
+      for (int i = 0; i < FCH; ++i) e = (c == cend && i == iend) ? v[i] : e;
+      e = __shfl_sync(fm, e, cend, FLANES);
+      if (c == 0) S.ex[ln] = e;
+      cg::this_cluster().sync();
+      T cr = T(0);
+      if (c == 0) {  // carry into this segment: periodic closure over the cluster
+        cg::cluster_group cl = cg::this_cluster();
+        T at = T(1), et = T(0);
+        for (int r = 0; r < cs; ++r) {
+          const int a0 = min(L, r * Lc), a1 = min(L, a0 + Lc);
+          const T ar = S.pwa[a1 - a0];
+          et = ar * et + cl.map_shared_rank(S.ex, r)[ln];
+          at = ar * at;
+        }
+        cr = et / (T(1) - at);
+        for (int r = 0; r < rank; ++r) {
+          const int a0 = min(L, r * Lc), a1 = min(L, a0 + Lc);
+          cr = S.pwa[a1 - a0] * cr + cl.map_shared_rank(S.ex, r)[ln];
+        }
+      }
+      cr = __shfl_sync(fm, cr, 0, FLANES);
 #pragma unroll
       for (int i = 0; i < FCH; ++i) {
-        const T val = xp[i * PITCH];
-        v[i] = (i < nb) ? val : T(0);
+        const T cv = cr * S.pwa[c * FCH + i + 1];
+        v[i] = (i < nb) ? v[i] + cv : T(0);  // backward input; zero past p1
+      }
+    } else {
+      // every stencil read of this line is done (the shuffles order the
+      // lanes); w of positions k0 .. k0+FCH-1 into this line's column
+      __syncwarp(fm);
+      {
+        T *wp = S.C + (k0 + rb) * PITCH + ln;
+#pragma unroll
+        for (int i = 0; i < FCH; ++i) wp[i * PITCH] = v[i];
+      }
+      __syncwarp(fm);
+    }
+
+    // backward: x over [p0, qb), zero start at qb
+    {
+      if (!EXACT) {
+        const T *xp = S.C + (k1 + rb) * PITCH + ln;
+#pragma unroll
+        for (int i = 0; i < FCH; ++i) {
+          const T val = xp[i * PITCH];
+          v[i] = (i < nb) ? val : T(0);
+        }
       }
       T x = T(0);
 #pragma unroll
@@ -1450,6 +1534,36 @@ __global__ void __launch_bounds__(NTH, 4)
       if (c == FLANES - 1) cin = T(0);
 #pragma unroll
       for (int i = 0; i < FCH; ++i) v[i] += cin * S.pwt[FCH - 1 - i];
+    }
+    if (EXACT) {
+      // backward start of the segment from a zero carry (position p0)
+      const T xs = __shfl_sync(fm, v[0], 0, FLANES);
+      if (c == 0) S.ex[LPG + ln] = xs;
+      cg::this_cluster().sync();
+      T d = T(0);
+      if (c == 0) {  // carry from the right: periodic closure, last segment first
+        cg::cluster_group cl = cg::this_cluster();
+        T at = T(1), xt = T(0);
+        for (int r = cs - 1; r >= 0; --r) {
+          const int a0 = min(L, r * Lc), a1 = min(L, a0 + Lc);
+          const T ar = S.pwa[a1 - a0];
+          xt = ar * xt + cl.map_shared_rank(S.ex, r)[LPG + ln];
+          at = ar * at;
+        }
+        d = xt / (T(1) - at);
+        for (int r = cs - 1; r > rank; --r) {
+          const int a0 = min(L, r * Lc), a1 = min(L, a0 + Lc);
+          d = S.pwa[a1 - a0] * d + cl.map_shared_rank(S.ex, r)[LPG + ln];
+        }
+      }
+      // this CTA's reads of the cluster's shared memory are done; it waits
+      // for the others' before it exits
+      // (non-aligned forms: the warp has just left the c == 0 branch)
+      asm volatile("barrier.cluster.arrive;\n" ::: "memory");
+      d = __shfl_sync(fm, d, 0, FLANES);
+#pragma unroll
+      for (int i = 0; i < FCH; ++i)
+        if (i < nb) v[i] += d * S.pwa[nb - i];
     }
     __syncwarp(fm);
     {
@@ -1485,6 +1599,7 @@ __global__ void __launch_bounds__(NTH, 4)
       for (int row = lane; row < np; row += 32) lbase[row] = scol[row * PITCH];
     }
   }
+  if (EXACT) asm volatile("barrier.cluster.wait;\n" ::: "memory");
 }
 
 }  // namespace
@@ -1496,10 +1611,11 @@ size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source) {
   return FD_BYTES + n * el;
 }
 
-size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64) {
+size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact) {
   size_t el = fp64 ? 8 : 4;
   return FD_BYTES + 64 * sizeof(int) +
-         (8 * (size_t)LPG + 32 + (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el;
+         (8 * (size_t)LPG + 32 + (exact ? (size_t)FPW + 2 * LPG : 0) +
+          (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el;
 }
 
 int filter_segment_max(int J) { return filter_seg_max(J); }
@@ -1528,17 +1644,20 @@ template <typename T>
 static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfields,
                                int group_base, int groups_total, int cs, int lc_max, int halo,
                                double toff, void *data, unsigned *d_status, int jstep,
-                               int nslice, const int *nlo, bool inplace, cudaStream_t stream) {
+                               int nslice, const int *nlo, bool inplace, cudaStream_t stream,
+                               const int *g0idx) {
   const bool fast = (variant == SWEEP_FAST);
-  const bool filt = (variant == SWEEP_FILTER);
+  const bool exact = (variant == SWEEP_FILTER_EXACT);
+  const bool filt = (variant == SWEEP_FILTER) || exact;
   const bool src = (variant == SWEEP_GENERAL_SRC);
-  const size_t smem = filt ? sweep_filter_smem_bytes(lc_max, halo, sizeof(T) == 8)
+  const size_t smem = filt ? sweep_filter_smem_bytes(lc_max, halo, sizeof(T) == 8, exact)
                       : fast ? sweep_fast_smem_bytes(lc_max, halo, sizeof(T) == 8)
                              : sweep_smem_bytes(lc_max, halo, sizeof(T) == 8, src);
   static bool configured = false;
   if (!configured) {
     for (const void *fn : {(const void *)sweep_kernel<T>, (const void *)sweep_fast_kernel<T>,
-                           (const void *)sweep_filter_kernel<T>}) {
+                           (const void *)sweep_filter_kernel<T, false>,
+                           (const void *)sweep_filter_kernel<T, true>}) {
       cudaError_t err =
           cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
       if (err != cudaSuccess) return err;
@@ -1548,11 +1667,12 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
     configured = true;
   }
   if (groups_total <= 0) return cudaSuccess;
-  if (filt && (cs == 1 || !inplace)) {  // whole lines per CTA, or out of place: no cluster
+  if (exact && inplace) return cudaErrorInvalidValue;  // the exact form sweeps out of place
+  if (filt && !exact && (cs == 1 || !inplace)) {  // whole lines per CTA, or out of place: no cluster
     count_launch();
-    sweep_filter_kernel<T><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
+    sweep_filter_kernel<T, false><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
         d_fields, nfields, group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
-        nlo, cs, 0);
+        nlo, cs, 0, g0idx);
     return cudaGetLastError();
   }
   cudaLaunchConfig_t cfg = {};
@@ -1568,14 +1688,19 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   count_launch();
+  if (exact)  // one cluster per tile: the cs segments of its lines
+    return cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T, true>, d_fields, nfields,
+                              group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
+                              nlo, cs, 0, g0idx);
   if (filt)  // group_base in CTAs
-    return cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T>, d_fields, nfields, group_base * cs,
-                              toff, data, lc_max, halo, d_status, jstep, nslice, nlo, cs, 1);
+    return cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T, false>, d_fields, nfields,
+                              group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
+                              nlo, cs, 1, g0idx);
   if (fast)
     return cudaLaunchKernelEx(&cfg, sweep_fast_kernel<T>, d_fields, nfields, group_base, toff,
-                              data, lc_max, halo, d_status, jstep, nslice, nlo);
+                              data, lc_max, halo, d_status, jstep, nslice, nlo, g0idx);
   return cudaLaunchKernelEx(&cfg, sweep_kernel<T>, d_fields, nfields, group_base, toff, data,
-                            lc_max, halo, d_status, jstep, nslice, nlo);
+                            lc_max, halo, d_status, jstep, nslice, nlo, g0idx);
 }
 
 template <typename T>
@@ -1583,7 +1708,7 @@ cudaError_t launch_sweep(int variant, const SweepField *d_fields, int nfields, i
                          int groups_total, int cs, int lc_max, int halo, double toff, void *data,
                          unsigned *d_status, cudaStream_t stream, int jstep, bool inplace) {
   return launch_impl<T>(variant, d_fields, nfields, group_base, groups_total, cs, lc_max, halo,
-                        toff, data, d_status, jstep, 0, nullptr, inplace, stream);
+                        toff, data, d_status, jstep, 0, nullptr, inplace, stream, nullptr);
 }
 
 template <typename T>
@@ -1591,7 +1716,8 @@ cudaError_t launch_sweep_batch(int variant, const SweepField *d_fields, int nfie
                                int group_base, int groups_total, int cs, int lc_max, int halo,
                                const BatchStep &bs, unsigned *d_status, cudaStream_t stream) {
   return launch_impl<T>(variant, d_fields, nfields, group_base, groups_total, cs, lc_max, halo,
-                        0.0, nullptr, d_status, bs.jstep, bs.nslice, bs.nlo, bs.inplace, stream);
+                        0.0, nullptr, d_status, bs.jstep, bs.nslice, bs.nlo, bs.inplace, stream,
+                        bs.g0idx);
 }
 
 template cudaError_t launch_sweep<double>(int, const SweepField *, int, int, int, int, int, int,

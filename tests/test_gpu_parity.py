@@ -187,6 +187,43 @@ def test_periodic_filter_segments_match_oracle(oracle, ccfv, nx, K):
     assert rel_l2(host(c), ref) < TOL
 
 
+@pytest.mark.parametrize("nx,ny,K", [(96, 96, 0.3), (300, 200, 0.2), (1000, 520, 0.05),
+                                     (2048, 64, 0.02)])
+def test_periodic_exact_filter_matches_oracle(oracle, ccfv, nx, ny, K):
+    """Strong diffusion (diffusion numbers 6 - 14: the recurrence warm-up
+    would exceed 64 cells): the filter kernel's cluster form, 1 to 8
+    segments per line, closes the periodic system exactly across them."""
+    vp = (0.9, -1.7)
+    dt = 0.8 / max(nx, ny) / 1.7
+    C0 = periodic_field(nx, 23, ny=ny)
+    g = oracle.grid(nx, ny, bc=1, vel=1, vp=vp, K=K, threads=THREADS, scheme=1)
+    ref = oracle.run(g, C0, 0.0, dt, 2)
+    s = ccfv.Solver(ccfv.make_grid(nx, ny, bc=1, velocity=1, vel_params=vp, K=K, scheme=1))
+    assert "filter_exact" in [v for v, _ in s.sweep_plan(dt)]
+    c = dev(C0)
+    s.run(c, 0.0, dt, 2)
+    s.check()
+    out = host(c)
+    assert rel_l2(out, ref) < TOL
+    assert abs(out.sum() - C0.sum()) < 1e-12 * np.abs(C0).sum()
+
+
+def test_fp32_exact_filter_coarse_close_to_fp64(ccfv):
+    N, K = 640, 0.05  # coarse steps of diffusion number ~60: the exact cluster form
+    C0 = periodic_field(N, 13)
+    s = ccfv.Solver(ccfv.make_grid(N, bc=1, velocity=1, vel_params=(0.6, 0.3), K=K, scheme=1))
+    assert "filter_exact" in [v for v, _ in s.sweep_plan(0.003, ccfv.FP32)]
+    a, b = dev(C0), dev(C0)
+    s.coarse(a, 0.0, 0.006, 2, ccfv.FP64)
+    s.coarse(b, 0.0, 0.006, 2, ccfv.FP32)
+    # FP32 rounding (6e-8) grows with the condition number of the y sub-step's
+    # cyclic system, (b + 2|a|) / (b - 2|a|) with a = 1/12 - nu/2, b = 10/12 + nu
+    nu = K * 0.003 * N * N
+    kappa = (10 / 12 + nu + 2 * abs(1 / 12 - nu / 2)) / (10 / 12 + nu - 2 * abs(1 / 12 - nu / 2))
+    assert kappa > 100
+    assert rel_l2(host(b), host(a)) < 6e-8 * kappa
+
+
 def test_fp32_filter_coarse_close_to_fp64(ccfv):
     N = 256
     C0 = periodic_field(N, 12)

@@ -32,8 +32,14 @@ MIX = [(96, 1, (1.0, -0.4), 1e-3), (160, 2, (2 * np.pi, 0.5, 0.5), 1e-3),
        (64, 3, (1.5,), 5e-4), (300, 1, (-0.3, 0.8), 1e-4), (128, 2, (2 * np.pi, 0.5, 0.5), 1e-2)]
 
 
+# long enough (tens of milliseconds) that requests submitted once they run
+# are admitted while they still run
+EARLY = [(400, 2, (2 * np.pi, 0.5, 0.5), 1e-3), (512, 1, (1.0, -0.4), 1e-3)]
+
+
 def test_server_results_equal_alone_and_late_arrivals_overlap(ccfv):
-    reqs = [_req(ccfv, N, v, vp, K, i) for i, (N, v, vp, K) in enumerate(MIX)]
+    reqs = [_req(ccfv, N, v, vp, K, i, S=16) for i, (N, v, vp, K) in enumerate(EARLY)]
+    reqs += [_req(ccfv, N, v, vp, K, i) for i, (N, v, vp, K) in enumerate(MIX[2:], start=2)]
     refs = [_alone(ccfv, p) for p in reqs]
     srv = ccfv.Server(hbm_budget_bytes=8 << 30)
     try:
