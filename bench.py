@@ -46,6 +46,8 @@ def parse():
                     help="reference arm: the oracle port on the host cores (cpu) or the "
                          "reference binary's own GPU step (gpu)")
     ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--nu", type=float, default=1e-3,
+                    help="diffusivity of the plain / step workload (1e-3: the benchmark)")
     ap.add_argument("--slices", type=int, default=64)
     ap.add_argument("--ratio", type=int, default=8)
     ap.add_argument("--tol", type=float, default=1e-10)
@@ -88,7 +90,7 @@ def workload(a):
     N = a.n
     nt = 4 * N
     return dict(N=N, T=1.0, nt=nt, slices=a.slices, ratio=a.ratio, tol=a.tol, kmax=a.kmax,
-                nu=1e-3, omega=2 * np.pi, center=(0.5, 0.5), hump=(0.5, 0.75), sigma=0.05)
+                nu=a.nu, omega=2 * np.pi, center=(0.5, 0.5), hump=(0.5, 0.75), sigma=0.05)
 
 
 def workload_name(w, a):
