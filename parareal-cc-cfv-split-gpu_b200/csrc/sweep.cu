@@ -1470,23 +1470,33 @@ __global__ void __launch_bounds__(NTH, 4)
       e = __shfl_sync(fm, e, cend, FLANES);
       if (c == 0) S.ex[ln] = e;
       cg::this_cluster().sync();
-      T cr = T(0);
-      if (c == 0) {  // carry into this segment: periodic closure over the cluster
-        cg::cluster_group cl = cg::this_cluster();
-        T at = T(1), et = T(0);
-        for (int r = 0; r < cs; ++r) {
-          const int a0 = min(L, r * Lc), a1 = min(L, a0 + Lc);
-          const T ar = S.pwa[a1 - a0];
-          et = ar * et + cl.map_shared_rank(S.ex, r)[ln];
-          at = ar * at;
+      // carry into this segment: lane r (< cs) loads segment r's map
+      // w -> (-mu)^np_r w + E_r, one scan composes them left to right, and
+      // the periodic closure of the whole line fixes the first carry
+      T cr;
+      {
+        T sa = T(1), sb = T(0);
+        if (c < cs) {
+          const int a0 = min(L, c * Lc), a1 = min(L, a0 + Lc);
+          sa = S.pwa[a1 - a0];
+          sb = cg::this_cluster().map_shared_rank(S.ex, c)[ln];
         }
-        cr = et / (T(1) - at);
-        for (int r = 0; r < rank; ++r) {
-          const int a0 = min(L, r * Lc), a1 = min(L, a0 + Lc);
-          cr = S.pwa[a1 - a0] * cr + cl.map_shared_rank(S.ex, r)[ln];
+#pragma unroll
+        for (int dd = 1; dd < FLANES; dd <<= 1) {
+          const T pa = __shfl_up_sync(fm, sa, dd, FLANES);
+          const T pb = __shfl_up_sync(fm, sb, dd, FLANES);
+          if (c >= dd) {
+            sb = sa * pb + sb;
+            sa = sa * pa;
+          }
         }
+        const T at = __shfl_sync(fm, sa, FLANES - 1, FLANES);  // lanes >= cs: identity
+        const T et = __shfl_sync(fm, sb, FLANES - 1, FLANES);
+        const T ea = __shfl_sync(fm, sa, rank > 0 ? rank - 1 : 0, FLANES);
+        const T eb = __shfl_sync(fm, sb, rank > 0 ? rank - 1 : 0, FLANES);
+        const T c0 = et / (T(1) - at);
+        cr = rank > 0 ? ea * c0 + eb : c0;
       }
-      cr = __shfl_sync(fm, cr, 0, FLANES);
 #pragma unroll
       for (int i = 0; i < FCH; ++i) {
         const T cv = cr * S.pwa[c * FCH + i + 1];
@@ -1540,27 +1550,37 @@ __global__ void __launch_bounds__(NTH, 4)
       const T xs = __shfl_sync(fm, v[0], 0, FLANES);
       if (c == 0) S.ex[LPG + ln] = xs;
       cg::this_cluster().sync();
-      T d = T(0);
-      if (c == 0) {  // carry from the right: periodic closure, last segment first
-        cg::cluster_group cl = cg::this_cluster();
-        T at = T(1), xt = T(0);
-        for (int r = cs - 1; r >= 0; --r) {
-          const int a0 = min(L, r * Lc), a1 = min(L, a0 + Lc);
-          const T ar = S.pwa[a1 - a0];
-          xt = ar * xt + cl.map_shared_rank(S.ex, r)[LPG + ln];
-          at = ar * at;
+      // carry from the right: lane r loads segment r's map x_start =
+      // (-mu)^np_r x_in + X_r, one scan composes them right to left
+      T d;
+      {
+        T sa = T(1), sb = T(0);
+        if (c < cs) {
+          const int a0 = min(L, c * Lc), a1 = min(L, a0 + Lc);
+          sa = S.pwa[a1 - a0];
+          sb = cg::this_cluster().map_shared_rank(S.ex, c)[LPG + ln];
         }
-        d = xt / (T(1) - at);
-        for (int r = cs - 1; r > rank; --r) {
-          const int a0 = min(L, r * Lc), a1 = min(L, a0 + Lc);
-          d = S.pwa[a1 - a0] * d + cl.map_shared_rank(S.ex, r)[LPG + ln];
+#pragma unroll
+        for (int dd = 1; dd < FLANES; dd <<= 1) {
+          const T pa = __shfl_down_sync(fm, sa, dd, FLANES);
+          const T pb = __shfl_down_sync(fm, sb, dd, FLANES);
+          if (c + dd < FLANES) {
+            sb = sa * pb + sb;
+            sa = sa * pa;
+          }
         }
+        const T at = __shfl_sync(fm, sa, 0, FLANES);
+        const T xt = __shfl_sync(fm, sb, 0, FLANES);
+        const bool last = rank + 1 >= cs;
+        const T ea = __shfl_sync(fm, sa, last ? 0 : rank + 1, FLANES);
+        const T eb = __shfl_sync(fm, sb, last ? 0 : rank + 1, FLANES);
+        const T x0 = xt / (T(1) - at);
+        d = last ? x0 : ea * x0 + eb;
       }
       // this CTA's reads of the cluster's shared memory are done; it waits
-      // for the others' before it exits
-      // (non-aligned forms: the warp has just left the c == 0 branch)
+      // for the others' before it exits (non-aligned forms: the wait follows
+      // the divergent store loops)
       asm volatile("barrier.cluster.arrive;\n" ::: "memory");
-      d = __shfl_sync(fm, d, 0, FLANES);
 #pragma unroll
       for (int i = 0; i < FCH; ++i)
         if (i < nb) v[i] += d * S.pwa[nb - i];
