@@ -131,6 +131,14 @@ int ccfv_fine(ccfv_ctx *ctx, double *d_C, double tn, double DT, int J, void *str
 int ccfv_coarse(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, int precision,
                 void *stream);
 
+/* ccfv_coarse with the coarse steps' implicit diffusion weight `theta`
+ * (ccfv_parareal_opts::coarse_theta: 0 or 0.5 Crank-Nicolson, a value in
+ * (0.5, 1], or CCFV_COARSE_THETA_AUTO, resolved for steps of DT/m): the
+ * coarse propagator of the slice-distributed drivers.  No counterpart in the
+ * reference. */
+int ccfv_coarse_ex(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, int precision,
+                   double theta, void *stream);
+
 /* nsteps serial steps of dt from t0 on `C` (device or host memory).  The
  * reference's serial fine run (T2S4_Parareal.cu:1224-1247). */
 int ccfv_run(ccfv_ctx *ctx, double *C, int mem, double t0, double dt, int nsteps, void *stream);
@@ -170,6 +178,11 @@ typedef struct ccfv_parareal_opts {
  * grid-scale mode by at least 1/5 (0.5 when Crank-Nicolson already does,
  * i.e. K dtc/h^2 below ~0.58; ~0.8 for stiff diffusion). */
 #define CCFV_COARSE_THETA_AUTO (-1.0)
+
+/* The coarse diffusion weight a Parareal run with these options uses on this
+ * grid (CCFV_COARSE_THETA_AUTO resolved); no device work.  Introspection, no
+ * counterpart in the reference. */
+int ccfv_coarse_theta(const ccfv_grid *grid, const ccfv_parareal_opts *opts, double *theta);
 
 #define CCFV_MAX_ITERS 128
 

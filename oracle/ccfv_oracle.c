@@ -600,7 +600,7 @@ int or_parareal_ref(const or_grid *g, const double *C0, double T_min, double T_m
  * second difference 4, RHS difference of the fourth-order edge derivatives
  * 16/3); theta is the smallest value >= 1/2 that makes its magnitude at most
  * 1/5 at the largest nu of a coarse step (x sub-steps dtc/2, y dtc). */
-static double auto_theta(const or_grid *g, double dtc) {
+double or_auto_theta(const or_grid *g, double dtc) {
   const double hx = (g->x_max - g->x_min) / g->nx, hy = (g->y_max - g->y_min) / g->ny;
   double nu = 0.5 * dtc / (hx * hx);
   if (dtc / (hy * hy) > nu) nu = dtc / (hy * hy);
@@ -628,7 +628,7 @@ int or_parareal(const or_grid *g, const or_parareal_opts *o, const double *C0, d
   /* every coarse step, the first sweep included, uses the coarse weight */
   or_grid gc = *g;
   gc.theta = o->coarse_theta > 0 ? o->coarse_theta
-             : o->coarse_theta == -1.0 ? auto_theta(g, DT / m) : 0.5;
+             : o->coarse_theta == -1.0 ? or_auto_theta(g, DT / m) : 0.5;
   double *U = (double *)malloc(sizeof(double) * NN * (S + 1));
   double *F = (double *)malloc(sizeof(double) * NN * (S + 1));
   double *Gold = (double *)malloc(sizeof(double) * NN * (S + 1));

@@ -64,6 +64,9 @@ int or_run(const or_grid *g, double *C, double t0, double dt, int nsteps);
 int or_fine(const or_grid *g, double *C, double tn, double DT, int J);
 /* Generalised CoarsePropagator: m steps of DT/m (m = 1 is the reference). */
 int or_coarse(const or_grid *g, double *C, double tn, double DT, int m);
+/* The automatic coarse diffusion weight for coarse steps of dtc: the
+ * smallest theta >= 0.5 whose sub-steps damp the grid-scale mode by 1/5. */
+double or_auto_theta(const or_grid *g, double dtc);
 
 /* The reference's Parareal schedule (40 slices, fixed kmax, duplicated
  * k=0 coarse sweep, G(U_k) recomputed).  err[k] = max|U_k(T) - Uref| when

@@ -73,6 +73,8 @@ def lib():
         L.or_run.argtypes = [G, _DP, C.c_double, C.c_double, C.c_int]
         L.or_fine.argtypes = [G, _DP, C.c_double, C.c_double, C.c_int]
         L.or_coarse.argtypes = [G, _DP, C.c_double, C.c_double, C.c_int]
+        L.or_auto_theta.argtypes = [G, C.c_double]
+        L.or_auto_theta.restype = C.c_double
         L.or_parareal_ref.argtypes = [G, _DP, C.c_double, C.c_double, C.c_int, C.c_int,
                                       C.c_int, C.c_void_p, C.c_void_p, _DP]
         L.or_parareal.argtypes = [G, C.POINTER(OrPararealOpts), _DP, _DP,
@@ -132,7 +134,16 @@ def fine(g, C0, tn, DT, J):
     return c.reshape(g.nx, g.ny)
 
 
-def coarse(g, C0, tn, DT, m=1):
+def auto_theta(g, dtc):
+    return lib().or_auto_theta(C.byref(g), dtc)
+
+
+def coarse(g, C0, tn, DT, m=1, theta=None):
+    """m coarse steps of DT/m; `theta` (None: the grid's own) the diffusion
+    weight, COARSE_THETA_AUTO resolved for steps of DT/m."""
+    if theta is not None:
+        g = type(g).from_buffer_copy(g)
+        g.theta = auto_theta(g, DT / max(m, 1)) if theta == COARSE_THETA_AUTO else theta
     c = np.array(C0, dtype=np.float64, order="C").reshape(-1).copy()
     _chk(lib().or_coarse(C.byref(g), c, tn, DT, m))
     return c.reshape(g.nx, g.ny)

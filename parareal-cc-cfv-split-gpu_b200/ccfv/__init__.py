@@ -111,6 +111,10 @@ _SIGS = {
     "ccfv_fine": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_void_p]),
     "ccfv_coarse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_int,
                               C.c_void_p]),
+    "ccfv_coarse_ex": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int,
+                                 C.c_int, C.c_double, C.c_void_p]),
+    "ccfv_coarse_theta": (C.c_int, [C.POINTER(Grid), C.POINTER(PararealOpts),
+                                    C.POINTER(C.c_double)]),
     "ccfv_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int,
                            C.c_void_p]),
     "ccfv_parareal": (C.c_int, [C.c_void_p, C.POINTER(PararealOpts), C.c_void_p, C.c_void_p,
@@ -247,9 +251,15 @@ class Solver:
     def fine(self, C_dev, tn, DT, J, stream=None):
         self._chk(lib().ccfv_fine(self._h, _dptr(C_dev), tn, DT, int(J), _stream_ptr(stream)))
 
-    def coarse(self, C_dev, tn, DT, m=1, precision=FP64, stream=None):
-        self._chk(lib().ccfv_coarse(self._h, _dptr(C_dev), tn, DT, int(m), int(precision),
-                                    _stream_ptr(stream)))
+    def coarse(self, C_dev, tn, DT, m=1, precision=FP64, stream=None, theta=0.5):
+        """m coarse steps of DT/m; `theta` the implicit diffusion weight
+        (0.5 Crank-Nicolson as the reference, COARSE_THETA_AUTO, or (0.5, 1])."""
+        if theta == 0.5:
+            self._chk(lib().ccfv_coarse(self._h, _dptr(C_dev), tn, DT, int(m), int(precision),
+                                        _stream_ptr(stream)))
+        else:
+            self._chk(lib().ccfv_coarse_ex(self._h, _dptr(C_dev), tn, DT, int(m),
+                                           int(precision), float(theta), _stream_ptr(stream)))
 
     def run(self, field, t0, dt, nsteps, stream=None):
         """Serial steps; `field` is a CUDA tensor (in place) or a numpy array
@@ -418,6 +428,18 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def coarse_theta(grid, *, t0, t1, nt_fine, n_slices, coarse_ratio=0, coarse_theta=0.5):
+    """The coarse diffusion weight a Parareal run with these options uses on
+    `grid` (COARSE_THETA_AUTO resolved); no device work."""
+    o = PararealOpts(t0, t1, int(nt_fine), int(n_slices), int(coarse_ratio), 0.0, 1, FP64,
+                     FORM_DELTA, MEM_DEVICE, None, float(coarse_theta))
+    th = C.c_double()
+    rc = lib().ccfv_coarse_theta(C.byref(grid), C.byref(o), C.byref(th))
+    if rc:
+        raise CcfvError(rc, lib().ccfv_strerror(rc).decode())
+    return th.value
 
 
 def batch_solve(problems, device=0, stream=None):

@@ -16,6 +16,8 @@ The compute backend is pluggable (``CudaSlices`` runs libccfv); the
 exchange and ordering logic is the same for any backend.  The delta form
 propagates slice increments with the linear part of G: a backend whose grid
 has a source term provides ``coarse_increment`` (G without the source).
+The coarse diffusion weight (ccfv_parareal_opts::coarse_theta) is a property
+of the backend's G (``CudaSlices(solver, coarse_theta=...)``).
 """
 from __future__ import annotations
 
@@ -30,11 +32,12 @@ from . import FORM_DELTA, FORM_STANDARD, FP64, SRC_NONE, Solver
 class CudaSlices:
     """Compute backend on libccfv for one grid on the rank's GPU."""
 
-    def __init__(self, solver):
+    def __init__(self, solver, coarse_theta=0.5):
         self.s = solver
         self.nx, self.ny = solver.grid.nx, solver.grid.ny
         self.device = torch.device("cuda", solver.device)
         self._hom = None
+        self.theta = coarse_theta
 
     def zeros(self, n):
         return torch.zeros(n, self.nx, self.ny, dtype=torch.float64, device=self.device)
@@ -43,7 +46,7 @@ class CudaSlices:
         self.s.fine_slices(fields, t0, slice_dt, DT, J)
 
     def coarse(self, field, t, DT, m):
-        self.s.coarse(field, t, DT, m, FP64)
+        self.s.coarse(field, t, DT, m, FP64, theta=self.theta)
 
     def coarse_increment(self, field, t, DT, m):
         if self.s.grid.source == SRC_NONE:
@@ -52,7 +55,7 @@ class CudaSlices:
             g = type(self.s.grid).from_buffer_copy(self.s.grid)
             g.source = SRC_NONE
             self._hom = Solver(g, self.s.device)
-        self._hom.coarse(field, t, DT, m, FP64)
+        self._hom.coarse(field, t, DT, m, FP64, theta=self.theta)
 
     def correct(self, form, U, F, W, Gold=None):
         return self.s.correct(form, U, F, W, Gold)

@@ -134,6 +134,37 @@ int ccfv_coarse(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, int pre
   return rc ? rc : last_launch(ctx);
 }
 
+int ccfv_coarse_ex(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, int precision,
+                   double theta, void *stream) {
+  if (!ctx || !d_C || m < 1 || !(DT > 0.0)) return CCFV_ERR_INVALID;
+  if (precision != CCFV_FP64 && precision != CCFV_FP32) return CCFV_ERR_INVALID;
+  if (!coarse_theta_ok(theta)) return CCFV_ERR_INVALID;
+  ccfv_parareal_opts o;
+  std::memset(&o, 0, sizeof(o));
+  o.coarse_theta = theta;
+  const double th = coarse_theta(o, ctx->grid, DT / (double)m);
+  int rc = use_device(ctx);
+  if (rc) return rc;
+  if (precision == CCFV_FP64)
+    rc = steps(ctx, d_C, true, tn, DT / (double)m, m, (cudaStream_t)stream, th);
+  else
+    rc = coarse_fp32(ctx, d_C, tn, DT, m, (cudaStream_t)stream, th);
+  return rc ? rc : last_launch(ctx);
+}
+
+int ccfv_coarse_theta(const ccfv_grid *grid, const ccfv_parareal_opts *opts, double *theta) {
+  if (!grid || !opts || !theta || !grid_ok(grid)) return CCFV_ERR_INVALID;
+  const ccfv_parareal_opts &o = *opts;
+  if (o.n_slices < 1 || o.nt_fine < o.n_slices || o.nt_fine % o.n_slices || !(o.t1 > o.t0))
+    return CCFV_ERR_INVALID;
+  const int J = o.nt_fine / o.n_slices;
+  if (o.coarse_ratio < 0 || (o.coarse_ratio > 0 && J % o.coarse_ratio)) return CCFV_ERR_INVALID;
+  if (!coarse_theta_ok(o.coarse_theta)) return CCFV_ERR_INVALID;
+  const int m = o.coarse_ratio > 0 ? J / o.coarse_ratio : 1;
+  *theta = coarse_theta(o, *grid, (o.t1 - o.t0) / o.n_slices / (double)m);
+  return CCFV_OK;
+}
+
 int ccfv_run(ccfv_ctx *ctx, double *C, int mem, double t0, double dt, int nsteps, void *stream) {
   if (!ctx || !C || nsteps < 0) return CCFV_ERR_INVALID;
   if (mem != CCFV_MEM_DEVICE && mem != CCFV_MEM_HOST) return CCFV_ERR_INVALID;

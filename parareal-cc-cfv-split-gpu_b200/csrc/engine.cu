@@ -926,14 +926,15 @@ int correct(ccfv_ctx *ctx, int form, double *U, const double *Fv, double *Gold, 
   return CCFV_OK;
 }
 
-int coarse_fp32(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, cudaStream_t st) {
+int coarse_fp32(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, cudaStream_t st,
+                double theta) {
   const long long NN = (long long)ctx->grid.nx * ctx->grid.ny;
   CK(ctx->C32.alloc(sizeof(float) * NN));
   float *w = ctx->C32.as<float>();
   int rc = convert(ctx, d_C, w, NN, st);
   if (rc) return rc;
   const double dtc = DT / (double)m;
-  if ((rc = steps(ctx, w, false, tn, dtc, m, st))) return rc;
+  if ((rc = steps(ctx, w, false, tn, dtc, m, st, theta))) return rc;
   return convert(ctx, w, d_C, NN, st);
 }
 

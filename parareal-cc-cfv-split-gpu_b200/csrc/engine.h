@@ -122,7 +122,8 @@ int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int
                   double toff, void *data_override, cudaStream_t st, int jstep = 0);
 int steps(ccfv_ctx *ctx, void *d_C, bool fp64, double t0, double dt, int nsteps, cudaStream_t st,
           double theta = 0.5);
-int coarse_fp32(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, cudaStream_t st);
+int coarse_fp32(ccfv_ctx *ctx, double *d_C, double tn, double DT, int m, cudaStream_t st,
+                double theta = 0.5);
 int fine_slices(ccfv_ctx *ctx, double *d_fields, int n, double t0, double slice_dt, double DT,
                 int J, cudaStream_t st);
 int correct(ccfv_ctx *ctx, int form, double *U, const double *Fv, double *Gold, double *W,

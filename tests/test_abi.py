@@ -44,3 +44,31 @@ def test_null_arguments_rejected(ccfv):
     assert L.ccfv_step(None, None, 0.0, 0.1, None) == ccfv.ERR_INVALID
     assert L.ccfv_destroy(None) == ccfv.ERR_INVALID
     assert L.ccfv_parareal(None, None, None, None, None, None) == ccfv.ERR_INVALID
+
+
+def test_coarse_theta_resolves_like_the_oracle_rule(ccfv, oracle):
+    """ccfv_coarse_theta (host only): 0 -> 0.5, fixed weights pass through,
+    the automatic weight equals the oracle's restatement of the rule for
+    coarse steps of (t1 - t0) / n_slices / m, and invalid weights are
+    rejected."""
+    kw = dict(t0=0.0, t1=1.0, nt_fine=512, n_slices=64, coarse_ratio=8)
+    g = ccfv.make_grid(128, bc=ccfv.BC_PERIODIC, velocity=ccfv.VEL_CONST, vel_params=(1.0, 0.5),
+                       K=0.01, scheme=ccfv.SCHEME_CONSISTENT)
+    assert ccfv.coarse_theta(g, coarse_theta=0.0, **kw) == 0.5
+    assert ccfv.coarse_theta(g, coarse_theta=0.8, **kw) == 0.8
+    for bad in (0.3, 1.2, -2.0):
+        with pytest.raises(ccfv.CcfvError):
+            ccfv.coarse_theta(g, coarse_theta=bad, **kw)
+    for nx, ny, K, ratio, dom in [(128, 128, 0.01, 8, None), (200, 96, 0.1, 4, None),
+                                  (64, 64, 1e-4, 8, None), (300, 300, 0.05, 2, None),
+                                  (100, 150, 0.2, 8, (0.0, 2.0, 0.0, 1.0))]:
+        g = ccfv.make_grid(nx, ny, bc=ccfv.BC_PERIODIC, velocity=ccfv.VEL_CONST,
+                           vel_params=(1.0, 0.5), K=K, domain=dom,
+                           scheme=ccfv.SCHEME_CONSISTENT)
+        o = oracle.grid(nx, ny, bc=oracle.BC_PERIODIC, vel=oracle.VEL_CONST, vp=(1.0, 0.5), K=K,
+                        domain=dom, scheme=1)
+        k2 = dict(kw, coarse_ratio=ratio)
+        th = ccfv.coarse_theta(g, coarse_theta=ccfv.COARSE_THETA_AUTO, **k2)
+        dtc = (k2["t1"] - k2["t0"]) / k2["n_slices"] / ((k2["nt_fine"] // k2["n_slices"]) // ratio)
+        assert th == pytest.approx(oracle.auto_theta(o, dtc), rel=1e-14, abs=1e-15)
+        assert 0.5 <= th <= 1.0

@@ -280,3 +280,19 @@ def test_source_sweep_plan(ccfv):
     s0 = ccfv.Solver(ccfv.make_grid(128, bc=1, velocity=1, vel_params=(1.0, 0.5), K=1e-3,
                                     scheme=1))
     assert [v for v, _ in s0.sweep_plan(1e-3)] == ["filter"] * 3
+
+
+@pytest.mark.parametrize("theta,prec", [(0.8, 0), (-1.0, 0), (-1.0, 1)])
+def test_coarse_ex_matches_oracle(oracle, ccfv, theta, prec):
+    """ccfv_coarse_ex: coarse steps with a fixed or automatic diffusion weight
+    (stiff: K dtc/h^2 = 12, automatic weight ~0.8) equal the oracle's."""
+    N, K, DT, m = 120, 0.1, 0.02, 2
+    vp = (0.7, -0.3)
+    C0 = periodic_field(N, 31)
+    g = oracle.grid(N, bc=1, vel=1, vp=vp, K=K, threads=THREADS, scheme=1)
+    ref = oracle.coarse(g, C0, 0.1, DT, m, theta=theta)
+    s = ccfv.Solver(ccfv.make_grid(N, bc=1, velocity=1, vel_params=vp, K=K, scheme=1))
+    c = dev(C0)
+    s.coarse(c, 0.1, DT, m, prec, theta=theta)
+    s.check()
+    assert rel_l2(host(c), ref) < (TOL if prec == 0 else 1e-5)
