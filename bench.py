@@ -215,11 +215,15 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(N):
+def ncu_traffic(N, variants=()):
     """DRAM bytes per cell per sweep of the fine sweep kernel, read from the
-    committed ncu summary (the `| bytes_per_cell_sweep | X |` row of
-    profiles/sweep_filter_4096_fp64.md); scaled by the caller to a launch."""
-    p = ROOT / "profiles" / "sweep_filter_4096_fp64.md"
+    committed ncu summary of the kernel form the sweeps run (the
+    `| bytes_per_cell_sweep | X |` row of profiles/sweep_filter_4096_fp64.md,
+    or of profiles/sweep_filter_exact_4096_fp64.md when any sub-step runs the
+    exact cluster form); scaled by the caller to a launch."""
+    name = ("sweep_filter_exact_4096_fp64.md" if "filter_exact" in variants
+            else "sweep_filter_4096_fp64.md")
+    p = ROOT / "profiles" / name
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
@@ -391,7 +395,7 @@ def run_ours(a, w, ws, rank, local):
     f_cells = sum(s["fine_sweep_cells"] for s in stats)
     peak, peak_kind = measured_peak()
     achieved = f_cells * BYTES_PER_FINE_CELL_SWEEP / (f_ms * 1e-3) / 1e9 if f_ms > 0 else None
-    tpc = ncu_traffic(N)
+    tpc = ncu_traffic(N, [v for v, _ in solver.sweep_plan(w["T"] / nt)])
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None,
             "traffic": (tpc * f_cells / f_launch) if (tpc and f_launch) else None,
@@ -701,7 +705,7 @@ def run_step(a, w, ws, rank, local):
     peak, peak_kind = measured_peak()
     sweeps = 3 * n * a.steps
     achieved = N * N * sweeps * BYTES_PER_FINE_CELL_SWEEP / (ms * 1e-3) / 1e9
-    tpc = ncu_traffic(N)
+    tpc = ncu_traffic(N, [v for v, _ in solver.sweep_plan(dt)])
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(w, a.cpu_sample_s)
