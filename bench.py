@@ -215,24 +215,21 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
+# DRAM bytes per cell per sweep of the fine sweep kernel, from one-launch ncu
+# captures (dram__bytes_read.sum + dram__bytes_write.sum / cells) of a 4096^2
+# FP64 sweep of each kernel form; the commands and counters are in
+# profiles/sweep_filter_4096_fp64.md and profiles/sweep_filter_exact_4096_fp64.md.
+NCU_BYTES_PER_CELL_SWEEP = {"filter": 13.39, "filter_exact": 13.24}
+
+
 def ncu_traffic(N, variants=()):
-    """DRAM bytes per cell per sweep of the fine sweep kernel, read from the
-    committed ncu summary of the kernel form the sweeps run (the
-    `| bytes_per_cell_sweep | X |` row of profiles/sweep_filter_4096_fp64.md,
-    or of profiles/sweep_filter_exact_4096_fp64.md when any sub-step runs the
-    exact cluster form); scaled by the caller to a launch."""
-    name = ("sweep_filter_exact_4096_fp64.md" if "filter_exact" in variants
-            else "sweep_filter_4096_fp64.md")
-    p = ROOT / "profiles" / name
-    if not p.exists():
-        return None
-    for line in p.read_text().splitlines():
-        f = [x.strip() for x in line.strip().strip("|").split("|")]
-        if len(f) == 2 and f[0] == "bytes_per_cell_sweep":
-            try:
-                return float(f[1])
-            except ValueError:
-                return None
+    """Measured DRAM bytes per cell per sweep of the kernel form the fine
+    sweeps run (the exact cluster form when any sub-step runs it); scaled by
+    the caller to a launch.  None for forms without a capture."""
+    if "filter_exact" in variants:
+        return NCU_BYTES_PER_CELL_SWEEP["filter_exact"]
+    if variants and all(v == "filter" for v in variants):
+        return NCU_BYTES_PER_CELL_SWEEP["filter"]
     return None
 
 

@@ -319,8 +319,13 @@ int ccfv_error_norms(ccfv_ctx *ctx, const double *d_a, const double *d_b, double
  * 340 KB that every GPU loading the library holds until exit.  Limit:
  * nx, ny <= 4096, else CCFV_ERR_UNSUPPORTED.  The first call on a device
  * looks up the array's address with that device current: make it before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * race.  Synchronises `stream` before returning. */
+ * stream capture (and do not call it on a device after cudaDeviceReset of
+ * that device: the cached address would be stale).  All calls share the
+ * array: calls that overlap on the GPU race.  Synchronises `stream` before
+ * returning.  Unlike ccfv_step, which leaves a foot that left the staged halo
+ * in the context's status word for ccfv_check, this call returns
+ * CCFV_ERR_HALO itself; d_C has been updated (with the out-of-halo reads
+ * taken as zero) when it does. */
 int ccfv_step_noalloc(const ccfv_grid *grid, double *d_C, double tn, double dt, void *stream);
 
 /* ---- tuning ------------------------------------------------------------ */

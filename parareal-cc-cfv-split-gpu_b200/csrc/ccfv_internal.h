@@ -26,6 +26,7 @@ constexpr int CPW = 32 / LPG;    // chunks per warp
 constexpr int NCH = NW * CPW;    // chunks per line per CTA
 constexpr int LC_MAX = 256;      // max positions per CTA
 constexpr int MAX_CLUSTER = 16;  // non-portable cluster size (lines <= 4096)
+constexpr int MAX_DEVICES = 64;  // device ordinals with per-device library state
 
 // One field (one instance at one time slice) in one sweep launch.
 // x-sweep: lines are columns j (s_line = 1, s_pos = ny), positions i.

@@ -17,7 +17,12 @@
 //    the process exits.
 //  - The first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture.
+//    before any stream capture.  The address is cached per device ordinal:
+//    after cudaDeviceReset of a device the module is reloaded and the cached
+//    address is stale, so the call must not be used on that device again.
+//  - A foot that left the staged halo is returned as CCFV_ERR_HALO (the
+//    context path leaves it in the status word for ccfv_check); the field has
+//    been updated, with the out-of-halo reads taken as zero, when it is.
 //  - All calls share the array, which keeps the last call's contents: calls
 //    that overlap on the GPU (different streams, or host threads) race.  The
 //    call synchronises its stream before returning.
@@ -47,7 +52,6 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 double h_tab[2][NOALLOC_TAB_LEN];
 SweepField h_fields[3];
 
-constexpr int MAX_DEVICES = 64;
 void *g_dev_ptr[MAX_DEVICES] = {};
 std::mutex g_mu;
 

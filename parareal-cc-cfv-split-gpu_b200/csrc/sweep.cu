@@ -31,8 +31,10 @@
 // adds a Sherman-Morrison rank-one correction with a line-invariant vector.
 #include <cooperative_groups.h>
 
+#include <atomic>
 #include <climits>
 #include <cstdio>
+#include <mutex>
 
 #include "ccfv_internal.h"
 
@@ -1673,18 +1675,33 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   const size_t smem = filt ? sweep_filter_smem_bytes(lc_max, halo, sizeof(T) == 8, exact)
                       : fast ? sweep_fast_smem_bytes(lc_max, halo, sizeof(T) == 8)
                              : sweep_smem_bytes(lc_max, halo, sizeof(T) == 8, src);
-  static bool configured = false;
-  if (!configured) {
-    for (const void *fn : {(const void *)sweep_kernel<T>, (const void *)sweep_fast_kernel<T>,
-                           (const void *)sweep_filter_kernel<T, false>,
-                           (const void *)sweep_filter_kernel<T, true>}) {
-      cudaError_t err =
-          cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-      if (err != cudaSuccess) return err;
-      err = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-      if (err != cudaSuccess) return err;
+  {
+    // Function attributes apply to the device that is current when they are
+    // set: configure each device once (contexts, batches, servers and the
+    // allocation-free step may run on different devices of one process, from
+    // several host threads).
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
+    static std::atomic<bool> configured[MAX_DEVICES];
+    static std::mutex config_mu;
+    if (!configured[dev].load(std::memory_order_acquire)) {
+      std::lock_guard<std::mutex> lk(config_mu);
+      if (!configured[dev].load(std::memory_order_relaxed)) {
+        for (const void *fn :
+             {(const void *)sweep_kernel<T>, (const void *)sweep_fast_kernel<T>,
+              (const void *)sweep_filter_kernel<T, false>,
+              (const void *)sweep_filter_kernel<T, true>}) {
+          err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     227 * 1024);
+          if (err != cudaSuccess) return err;
+          err = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+          if (err != cudaSuccess) return err;
+        }
+        configured[dev].store(true, std::memory_order_release);
+      }
     }
-    configured = true;
   }
   if (groups_total <= 0) return cudaSuccess;
   if (exact && inplace) return cudaErrorInvalidValue;  // the exact form sweeps out of place
