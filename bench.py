@@ -56,16 +56,27 @@ def parse():
     ap.add_argument("--form", default="delta", choices=["standard", "delta"])
     ap.add_argument("--cpu-sample-s", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "step", "split"],
+    ap.add_argument("--mode", default="plain",
+                    choices=["plain", "batch", "serve", "step", "split", "dist"],
                     help="plain: one instance (default workload); batch: a mixed batch of "
                          "instances in shared launches; serve: Poisson arrivals through the "
                          "continuous-batching server; step: serial fine time-stepping of the "
                          "workload's field (the sweep kernels alone); split: the precision-split "
-                         "case (swirl, 128 slices): FP32 vs FP64 coarse against the serial fine")
+                         "case (swirl, 128 slices): FP32 vs FP64 coarse against the serial "
+                         "fine; dist: the slice-distributed solve (the default for N > 1) "
+                         "also on one GPU")
     ap.add_argument("--inner", type=int, default=16,
                     help="step mode: fine steps per timed step")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--serve-nmax", type=int, default=1024,
+                    help="serve: largest grid side of the requests (log-uniform from 128)")
+    ap.add_argument("--multi", default="dist", choices=["dist", "instances"],
+                    help="N > 1 GPUs: dist = one Parareal solve with its time slices spread "
+                         "over the ranks (ccfv.dist, NCCL; strong scaling); instances = an "
+                         "independent solve per rank (weak scaling)")
+    ap.add_argument("--no-batch-serve", action="store_true",
+                    help="plain mode: leave out the batched and served sub-measurements")
     ap.add_argument("--seed", type=int, default=20261206)
     ap.add_argument("--plain-sample", type=int, default=0,
                     help="instances solved one at a time (FP64 coarse) for the plain rate "
@@ -169,11 +180,31 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
+def spawn_ranks(a):
+    """--gpus N > 1 without a launcher: start N ranks on this node through
+    torch.distributed.run (rendezvous on 127.0.0.1) and return its exit
+    code; NCCL's initialisation log stays on, so the communicator's ranks
+    show in the output."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    env = dict(os.environ)
+    env.setdefault("NCCL_DEBUG", "INFO")
+    env.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={a.gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           str(Path(__file__).resolve())] + sys.argv[1:]
+    return subprocess.call(cmd, env=env)
+
+
 def dist_setup(a):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
+    if "WORLD_SIZE" in os.environ and ws != a.gpus:
+        raise SystemExit(f"bench.py: WORLD_SIZE={ws} but --gpus {a.gpus}")
+    if ws > 1 or (a.mode == "dist" and a.impl == "ours"):
         import datetime
         import torch.distributed as dist
         backend = "nccl"
@@ -183,7 +214,15 @@ def dist_setup(a):
                 backend = "gloo"
         except Exception:
             backend = "gloo"
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        if ws > 1:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        else:  # --mode dist on one GPU: a one-rank group
+            import socket
+            with socket.socket() as sk:
+                sk.bind(("127.0.0.1", 0))
+                port = sk.getsockname()[1]
+            dist.init_process_group(backend, init_method=f"tcp://127.0.0.1:{port}", rank=0,
+                                    world_size=1, timeout=datetime.timedelta(seconds=600))
     return ws, rank, local
 
 
@@ -440,6 +479,13 @@ def run_ours(a, w, ws, rank, local):
             e2e={"value": e2e_value, "unit": "cell-updates/s",
                  "h2d_bytes_per_step": 8 * N * N, "d2h_bytes_per_step": 8 * N * N},
             roofline=roof, cpu_baseline=cpu, clocks=ck, gpu_launches=launches)
+        if ws == 1 and not a.no_batch_serve:
+            # the batched and served forms of the metric on the same GPU (one
+            # timed batch solve after one warm-up; one served request stream)
+            line["batch"] = measure_batch(a, ws, rank, local, 1, 1)
+            line["serve"] = measure_serve(a, ws, rank, local)
+            line["batched_vs_plain"] = line["batch"].get("batched_vs_plain_same_coarse_theta")
+            line["served_vs_plain"] = line["serve"].get("served_vs_plain_same_coarse_theta")
         print(json.dumps(line))
 
 
@@ -529,15 +575,130 @@ def plain_rate(probs, device, theta=0.5):
     return cells / (ms * 1e-3)
 
 
-def run_batch(a, ws, rank, local):
+def run_dist(a, w, ws, rank, local):
+    """One Parareal solve of the workload with its time slices spread over
+    the ranks (ccfv.dist.parareal_dist on the CudaSlices backend: the F
+    phases of all ranks run concurrently, the coarse sweep is pipelined rank
+    to rank with one N^2 boundary state per rank boundary over NCCL).  The
+    whole job solves one problem: strong scaling.  Rank 0 checks the result
+    against the single-GPU engine (ccfv_parareal) on its own GPU."""
+    import torch
+    import ccfv
+    from ccfv.dist import CudaSlices, parareal_dist
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    N, nt = w["N"], w["nt"]
+    grid = ccfv.make_grid(N, bc=ccfv.BC_PERIODIC, velocity=ccfv.VEL_ROTATION,
+                          vel_params=(w["omega"], *w["center"]), K=w["nu"],
+                          scheme=ccfv.SCHEME_CONSISTENT)
+    solver = ccfv.Solver(grid, local)
+    C0 = initial_field(w, solver, dev)
+    be = CudaSlices(solver, timed=True)
+    kw = dict(t0=0.0, t1=w["T"], nt_fine=nt, n_slices=w["slices"], coarse_ratio=w["ratio"],
+              tol=w["tol"], kmax=w["kmax"], form=ccfv.FORM_DELTA)
+    for _ in range(a.warmup):
+        out, st = parareal_dist(be, C0, **kw)
+    torch.cuda.synchronize()
+    be.reset_timers()
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = ccfv.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(a.steps):
+        out, st = parareal_dist(be, C0, **kw)
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = ccfv.kernel_launches() - l0
+    ck = clocks.stop()
+    barrier(ws)
+    ms_max = reduce_max(ev0.elapsed_time(ev1), ws)
+    value = (N * N * nt) * a.steps / (ms_max * 1e-3)
+    f_ms = be.fine_phase_ms()
+    peak, peak_kind = measured_peak()
+    achieved = be.fine_cells * BYTES_PER_FINE_CELL_SWEEP / (f_ms * 1e-3) / 1e9 if f_ms else 0.0
+    achieved_min = -reduce_max(-achieved, ws)  # the slowest rank's F phase
+    # e2e: initial field from pinned host memory on rank 0 (passed on to the
+    # other ranks by the pipeline), result read back to the host on rank 0
+    h_in = torch.empty(N, N, dtype=torch.float64, pin_memory=True)
+    h_in.copy_(C0.cpu())
+    h_out = torch.empty(N, N, dtype=torch.float64, pin_memory=True)
+    barrier(ws)
+    e0 = time.perf_counter()
+    for _ in range(a.steps):
+        c0 = h_in.to(dev, non_blocking=True) if rank == 0 else C0
+        o, _ = parareal_dist(be, c0, **kw)
+        if rank == 0:
+            h_out.copy_(o)
+    torch.cuda.synchronize()
+    e_s = reduce_max(time.perf_counter() - e0, ws)
+    err = None
+    if rank == 0:
+        ref, _ = solver.parareal(C0, t0=0.0, t1=w["T"], nt_fine=nt, n_slices=w["slices"],
+                                 coarse_ratio=w["ratio"], tol=w["tol"], kmax=w["kmax"],
+                                 coarse_precision=ccfv.FP64, form=ccfv.FORM_DELTA)
+        err = float(torch.linalg.norm(out - ref) / torch.linalg.norm(ref))
+    barrier(ws)
+    if rank == 0:
+        line = dict(
+            metric="parareal_cell_updates_per_s", value=value, unit="cell-updates/s",
+            n_gpus=ws, steps=a.steps, warmup=a.warmup, ms_per_step=ms_max / a.steps,
+            higher_is_better=True, scaling="strong", vs_baseline=None, dtype="f64",
+            data="synthetic",
+            config={"workload": workload_name(w, a), "N": N, "nt_fine": nt,
+                    "n_slices": w["slices"], "coarse_ratio": w["ratio"],
+                    "coarse_precision": "fp64", "form": "delta",
+                    "l2_flush": "working set (slice states) > L2",
+                    "parallelism": f"time slices over {ws} rank(s) (ccfv.dist: NCCL send/recv "
+                                   "of boundary states, max all-reduce of updates)"},
+            iterations=st["iterations"], converged=st["converged"],
+            final_update=st["update"][-1] if st["update"] else None,
+            l2_err_vs_single_gpu_parareal=err,
+            e2e={"value": (N * N * nt) * a.steps / e_s, "unit": "cell-updates/s",
+                 "h2d_bytes_per_step": 8 * N * N, "d2h_bytes_per_step": 8 * N * N},
+            roofline={"bound": "hbm", "achieved": achieved_min, "peak": peak, "unit": "GB/s",
+                      "frac": achieved_min / peak if achieved_min else None, "traffic": None,
+                      "kernel": "F phase (slowest rank, in-place sweeps): " +
+                                solver.variant_names(w["T"] / nt),
+                      "peak_source": peak_kind},
+            cpu_baseline=None, clocks=ck, gpu_launches=launches)
+        print(json.dumps(line))
+
+
+def fine_errors(probs, device):
+    """Relative L2 of every problem's Parareal result against its own serial
+    fine solve on the GPU (same fine steps, untimed)."""
+    import torch
+    import ccfv
+    errs = []
+    for p in probs:
+        s = ccfv.Solver(p["grid"], device)
+        c0 = p["C0"]
+        fine = (torch.from_numpy(c0).cuda(device) if isinstance(c0, np.ndarray)
+                else c0.clone())
+        s.run(fine, p["t0"], (p["t1"] - p["t0"]) / p["nt_fine"], p["nt_fine"])
+        out = p["C_T"]
+        out = torch.from_numpy(out).cuda(device) if isinstance(out, np.ndarray) else out
+        errs.append(float(torch.linalg.norm(out - fine) / torch.linalg.norm(fine)))
+        s.close()
+    return errs
+
+
+def measure_batch(a, ws, rank, local, steps, warmup):
+    """The batched form on `a.instances` mixed instances: rate of the whole
+    batch, every instance's error against its serial fine solve, and the
+    plain single-instance FP64 rate of the same instances (with the batch's
+    coarse weight, and with Crank-Nicolson coarse steps)."""
     import torch
     import ccfv
     torch.cuda.set_device(local)
     rng = np.random.default_rng(a.seed + rank)
     probs = batch_problems(a, rng, a.instances)
     _fields(probs, local)
-    cells = sum(p["N"] ** 2 * p["nt_fine"] for p in probs)
-    for _ in range(a.warmup):
+    cells = [p["N"] ** 2 * p["nt_fine"] for p in probs]
+    for _ in range(warmup):
         st = ccfv.batch_solve(probs, device=local)
     torch.cuda.synchronize()
     barrier(ws)
@@ -546,56 +707,84 @@ def run_batch(a, ws, rank, local):
     l0 = ccfv.kernel_launches()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
-    for _ in range(a.steps):
+    for _ in range(steps):
         st = ccfv.batch_solve(probs, device=local)
     ev1.record()
     torch.cuda.synchronize()
     launches = ccfv.kernel_launches() - l0
     ck = clocks.stop()
     ms = reduce_max(ev0.elapsed_time(ev1), ws)
-    value = ws * cells * a.steps / (ms * 1e-3)
+    value = ws * sum(cells) * steps / (ms * 1e-3)
+    res = dict(value=value, unit="cell-updates/s", ms_per_step=ms / steps, steps=steps,
+               warmup=warmup, clocks=ck, gpu_launches=launches, instances=len(probs))
+    if rank != 0:
+        return res
+    errs = fine_errors(probs, local)
+    ok = [e <= 1e-10 for e in errs]
+    its = [x["iterations"] for x in st]
     sample = plain_sample(probs, a.plain_sample)
-    plain = plain_rate(sample, local) if rank == 0 else None
     th = coarse_theta_arg(a)
-    plain_th = plain_rate(sample, local, th) if rank == 0 and th != 0.5 else plain
+    plain = plain_rate(sample, local)
+    plain_th = plain_rate(sample, local, th) if th != 0.5 else plain
+    # the batch's shared F phases: 48 algorithmic bytes per executed fine
+    # cell-update (3 FP64 sweeps, read + write)
+    fine_cu = float(sum(x["fine_cell_updates"] for x in st))
+    peak, peak_kind = measured_peak()
+    f_gbs = 48.0 * fine_cu / (st[0]["fine_ms"] * 1e-3) / 1e9 if st[0]["fine_ms"] else None
+    res.update(
+        # the instances whose result meets 1e-10 against the serial fine solve:
+        # their share of the cell-updates over the whole batch time
+        value_meeting_1e10=ws * sum(c for c, g in zip(cells, ok) if g) * steps / (ms * 1e-3),
+        max_l2_err_vs_serial_fine=max(errs), instances_meeting_1e10=int(sum(ok)),
+        all_meet_1e10=all(ok), all_converged=all(x["converged"] for x in st),
+        converged=int(sum(1 for x in st if x["converged"])),
+        not_converged=[dict(instance=i, N=p["N"], iterations=x["iterations"],
+                            slices=p["n_slices"],
+                            last_update=x["update"][-1] if x["update"] else None,
+                            l2_err_vs_serial_fine=errs[i])
+                       for i, (p, x) in enumerate(zip(probs, st)) if not x["converged"]],
+        iterations_mean=float(np.mean(its)), fine_ms=st[0]["fine_ms"],
+        coarse_ms=st[0]["coarse_ms"],
+        fine_phase={"executed_fine_cell_updates": fine_cu, "achieved_gbs": f_gbs,
+                    "peak_gbs": peak, "frac": (f_gbs / peak) if f_gbs else None,
+                    "peak_source": peak_kind},
+        plain_fp64_same_coarse_theta_cell_updates_per_s=plain_th,
+        batched_vs_plain_same_coarse_theta=(value / ws / plain_th) if plain_th else None,
+        plain_fp64_crank_nicolson_cell_updates_per_s=plain,
+        batched_vs_plain_crank_nicolson=(value / ws / plain) if plain else None,
+        config={"workload": f"{a.instances} periodic instances per GPU, N log-uniform "
+                            "64..1024, constant velocity U[-2,2]^2, nu log-uniform "
+                            "1e-4..1e-1, 1-8 Gaussians, T=1, fine dt at CFL 0.8, 16-64 "
+                            "slices, coarse dt = 8 x fine, FP32 coarse / FP64 fine, "
+                            f"coarse diffusion weight {a.coarse_theta}, "
+                            "tol 1e-10 (cap = slices)", "seed": a.seed,
+                "plain": "each instance alone, FP64 coarse steps, with the batch's coarse "
+                         "weight (headline ratio) and with Crank-Nicolson "
+                         f"({len(sample)} instances)"})
+    return res
+
+
+def run_batch(a, ws, rank, local):
+    r = measure_batch(a, ws, rank, local, a.steps, a.warmup)
     if rank == 0:
-        its = [x["iterations"] for x in st]
-        conv = sum(1 for x in st if x["converged"])
-        # the batch's shared F phases: 48 algorithmic bytes per executed fine
-        # cell-update (3 FP64 sweeps, read + write)
-        fine_cu = float(sum(x["fine_cell_updates"] for x in st))
-        peak, peak_kind = measured_peak()
-        f_gbs = 48.0 * fine_cu / (st[0]["fine_ms"] * 1e-3) / 1e9 if st[0]["fine_ms"] else None
-        fine_phase = {"executed_fine_cell_updates": fine_cu, "achieved_gbs": f_gbs, "peak_gbs": peak,
-                      "frac": (f_gbs / peak) if f_gbs else None, "peak_source": peak_kind}
-        print(json.dumps(dict(
-            metric="parareal_cell_updates_per_s", value=value, unit="cell-updates/s",
-            mode="batch", n_gpus=ws, steps=a.steps, warmup=a.warmup,
-            ms_per_step=ms / a.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
-            dtype="f64", data="synthetic",
-            config={"workload": f"{a.instances} periodic instances per GPU, N log-uniform "
-                                "64..1024, constant velocity U[-2,2]^2, nu log-uniform "
-                                "1e-4..1e-1, 1-8 Gaussians, T=1, fine dt at CFL 0.8, 16-64 "
-                                "slices, coarse dt = 8 x fine, FP32 coarse / FP64 fine, "
-                                f"coarse diffusion weight {a.coarse_theta}, "
-                                "tol 1e-10 (cap = slices)", "seed": a.seed,
-                    "plain": "each instance alone, FP64 Crank-Nicolson coarse steps "
-                             f"({len(sample)} instances)"},
-            iterations_mean=float(np.mean(its)), converged=conv, instances=len(st),
-            fine_ms=st[0]["fine_ms"], coarse_ms=st[0]["coarse_ms"], fine_phase=fine_phase,
-            plain_fp64_single_instance_cell_updates_per_s=plain,
-            batched_vs_plain=(value / ws / plain) if plain else None,
-            plain_fp64_same_coarse_theta_cell_updates_per_s=plain_th,
-            batched_vs_plain_same_coarse_theta=(value / ws / plain_th) if plain_th else None,
-            clocks=ck, gpu_launches=launches)))
+        line = dict(metric="parareal_cell_updates_per_s", value=r.pop("value"),
+                    unit=r.pop("unit"), mode="batch", n_gpus=ws, higher_is_better=True,
+                    scaling="weak", vs_baseline=None, dtype="f64", data="synthetic")
+        line.update(r)
+        print(json.dumps(line))
 
 
-def run_serve(a, ws, rank, local):
+def measure_serve(a, ws, rank, local):
+    """The served form: `a.requests` mixed requests, first all at once
+    (closed-loop capacity), then as Poisson arrivals at 80% of that capacity
+    through the continuous-batching server; latency percentiles, every
+    request's error against its serial fine solve, and the plain
+    single-instance FP64 rate of the same requests."""
     import torch
     import ccfv
     torch.cuda.set_device(local)
     rng = np.random.default_rng(a.seed + 1000 + rank)
-    probs = batch_problems(a, rng, a.requests, nmin=128, nmax=1024, mixed_velocity=True)
+    probs = batch_problems(a, rng, a.requests, nmin=128, nmax=a.serve_nmax, mixed_velocity=True)
     _fields(probs, local, host=True)
     cells = [p["N"] ** 2 * p["nt_fine"] for p in probs]
     budget = int(96e9)
@@ -619,38 +808,60 @@ def run_serve(a, ws, rank, local):
         while time.perf_counter() < t_next:
             time.sleep(0.0002)
         tickets.append(srv.submit(p))
-    its = []
+    its, conv = [], []
     for t in tickets:
         st, l_ms = srv.wait(t)
         lat.append(l_ms)
         its.append(st["iterations"])
+        conv.append(st["converged"])
     span = time.perf_counter() - t_start
     srv.close()
+    value = sum(cells) / span
+    res = dict(value=value, unit="cell-updates/s", requests=len(probs))
+    if rank != 0:
+        return res
+    errs = fine_errors(probs, local)
+    ok10 = [e <= 1e-10 for e in errs]
+    ok_tol = [e <= p["tol"] for e, p in zip(errs, probs)]
     sample = plain_sample(probs, a.plain_sample)
     for p in sample:
         p["C0"] = torch.from_numpy(p["C0"]).cuda(local)
         p["C_T"] = torch.empty_like(p["C0"])
-    plain = plain_rate(sample, local) if rank == 0 else None
+    th = coarse_theta_arg(a)
+    plain = plain_rate(sample, local)
+    plain_th = plain_rate(sample, local, th) if th != 0.5 else plain
+    res.update(
+        latency_ms_p50=float(np.percentile(lat, 50)),
+        latency_ms_p99=float(np.percentile(lat, 99)),
+        capacity_cell_updates_per_s=cap, arrival_rate_per_s=rate,
+        iterations_mean=float(np.mean(its)), all_converged=all(conv),
+        max_l2_err_vs_serial_fine=max(errs), requests_meeting_1e10=int(sum(ok10)),
+        requests_meeting_own_tol=int(sum(ok_tol)),
+        value_meeting_1e10=sum(c for c, g in zip(cells, ok10) if g) / span,
+        plain_fp64_same_coarse_theta_cell_updates_per_s=plain_th,
+        served_vs_plain_same_coarse_theta=(value / plain_th) if plain_th else None,
+        plain_fp64_crank_nicolson_cell_updates_per_s=plain,
+        served_vs_plain_crank_nicolson=(value / plain) if plain else None,
+        capacity_vs_plain_same_coarse_theta=(cap / plain_th) if plain_th else None,
+        config={"workload": f"{a.requests} requests, Poisson arrivals at 80% of measured "
+                            f"capacity, N log-uniform 128..{a.serve_nmax}, velocity from "
+                            "{constant, rotation, swirl}, nu log-uniform 1e-4..1e-2, T "
+                            "U[0.25,2], tol in {1e-8,1e-10}, HBM budget 96 GB, FP32 coarse, "
+                            f"coarse diffusion weight {a.coarse_theta}", "seed": a.seed,
+                "plain": "each request alone, FP64 coarse steps, with the served coarse "
+                         "weight (headline ratio) and with Crank-Nicolson "
+                         f"({len(sample)} requests)"})
+    return res
+
+
+def run_serve(a, ws, rank, local):
+    r = measure_serve(a, ws, rank, local)
     if rank == 0:
-        value = sum(cells) / span
-        print(json.dumps(dict(
-            metric="parareal_cell_updates_per_s", value=value, unit="cell-updates/s",
-            mode="serve", n_gpus=ws, requests=len(probs), higher_is_better=True,
-            scaling="weak", vs_baseline=None, dtype="f64", data="synthetic",
-            config={"workload": f"{a.requests} requests, Poisson arrivals at 80% of measured "
-                                "capacity, N log-uniform 128..1024, velocity from {constant, "
-                                "rotation, swirl}, nu log-uniform 1e-4..1e-2, T U[0.25,2], "
-                                "tol in {1e-8,1e-10}, HBM budget 96 GB, FP32 coarse, "
-                                f"coarse diffusion weight {a.coarse_theta}",
-                    "seed": a.seed,
-                    "plain": "each request alone, FP64 Crank-Nicolson coarse steps "
-                             f"({len(sample)} requests)"},
-            latency_ms_p50=float(np.percentile(lat, 50)),
-            latency_ms_p99=float(np.percentile(lat, 99)),
-            capacity_cell_updates_per_s=cap, arrival_rate_per_s=rate,
-            iterations_mean=float(np.mean(its)),
-            plain_fp64_single_instance_cell_updates_per_s=plain,
-            served_vs_plain=(value / plain) if plain else None)))
+        line = dict(metric="parareal_cell_updates_per_s", value=r.pop("value"),
+                    unit=r.pop("unit"), mode="serve", n_gpus=ws, higher_is_better=True,
+                    scaling="weak", vs_baseline=None, dtype="f64", data="synthetic")
+        line.update(r)
+        print(json.dumps(line))
 
 
 def run_step(a, w, ws, rank, local):
@@ -783,6 +994,8 @@ def run_split(a, ws, rank, local):
 
 def main():
     a = parse()
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(a))
     w = workload(a)
     ws, rank, local = dist_setup(a)
     try:
@@ -796,11 +1009,13 @@ def main():
             run_step(a, w, ws, rank, local)
         elif a.mode == "split":
             run_split(a, ws, rank, local)
+        elif (ws > 1 and a.multi == "dist") or a.mode == "dist":
+            run_dist(a, w, ws, rank, local)
         else:
             run_ours(a, w, ws, rank, local)
     finally:
-        if ws > 1:
-            import torch.distributed as dist
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
             dist.destroy_process_group()
 
 

@@ -32,18 +32,42 @@ from . import FORM_DELTA, FORM_STANDARD, FP64, SRC_NONE, Solver
 class CudaSlices:
     """Compute backend on libccfv for one grid on the rank's GPU."""
 
-    def __init__(self, solver, coarse_theta=0.5):
+    def __init__(self, solver, coarse_theta=0.5, timed=False):
         self.s = solver
         self.nx, self.ny = solver.grid.nx, solver.grid.ny
         self.device = torch.device("cuda", solver.device)
         self._hom = None
         self.theta = coarse_theta
+        # timed: CUDA events around every F phase (fine_phase_ms, fine_cells)
+        self.timed = timed
+        self._ev = []
+        self.fine_cells = 0
+        self.fine_sweeps = 0
 
     def zeros(self, n):
         return torch.zeros(n, self.nx, self.ny, dtype=torch.float64, device=self.device)
 
     def fine(self, fields, t0, slice_dt, DT, J):
+        if self.timed:
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
         self.s.fine_slices(fields, t0, slice_dt, DT, J)
+        if self.timed:
+            b.record()
+            self._ev.append((a, b))
+            self.fine_cells += 3 * J * fields.shape[0] * self.nx * self.ny
+            self.fine_sweeps += 3 * J
+
+    def fine_phase_ms(self):
+        """Device time of the F phases since the last reset (synchronises)."""
+        torch.cuda.synchronize(self.device)
+        return sum(a.elapsed_time(b) for a, b in self._ev)
+
+    def reset_timers(self):
+        self._ev = []
+        self.fine_cells = 0
+        self.fine_sweeps = 0
 
     def coarse(self, field, t, DT, m):
         self.s.coarse(field, t, DT, m, FP64, theta=self.theta)
