@@ -295,7 +295,8 @@ class Solver:
                                       _stream_ptr(stream)))
         return seg.value
 
-    SWEEP_NAMES = ("general", "uniform", "filter", "source", "filter_exact")
+    SWEEP_NAMES = ("general", "uniform", "filter", "source", "filter_exact", "cell",
+                   "cell_exact")
 
     def sweep_plan(self, dt, precision=FP64):
         """Kernel variant and segment length of the three sub-steps of a step
@@ -306,7 +307,8 @@ class Solver:
 
     SWEEP_KERNELS = {"general": "sweep_kernel", "uniform": "sweep_fast_kernel",
                      "filter": "sweep_filter_kernel", "source": "sweep_kernel",
-                     "filter_exact": "sweep_filter_kernel"}
+                     "filter_exact": "sweep_filter_kernel", "cell": "sweep_filter_kernel",
+                     "cell_exact": "sweep_filter_kernel"}
 
     def variant_names(self, dt, precision=FP64):
         """Names of the sweep kernels a step of dt launches (x, y, x)."""

@@ -118,15 +118,28 @@ constexpr size_t FD_BYTES = (sizeof(SweepField) + 63) & ~size_t(63);
 // SWEEP_GENERAL_SRC is the per-cell kernel with the source tile staged;
 // SWEEP_FILTER_EXACT the filter kernel's cluster form (any diffusion number,
 // out of place).
+// SWEEP_CELL / SWEEP_CELL_EXACT: the filter kernel's two forms with a
+// per-cell right-hand side (feet that differ from edge to edge).
 enum { SWEEP_GENERAL = 0, SWEEP_FAST = 1, SWEEP_FILTER = 2, SWEEP_GENERAL_SRC = 3,
-       SWEEP_FILTER_EXACT = 4 };
-inline bool filter_variant(int v) { return v == SWEEP_FILTER || v == SWEEP_FILTER_EXACT; }
+       SWEEP_FILTER_EXACT = 4, SWEEP_CELL = 5, SWEEP_CELL_EXACT = 6 };
+// Variants run by the filter kernel (factored cyclic solve).
+inline bool filter_variant(int v) {
+  return v == SWEEP_FILTER || v == SWEEP_FILTER_EXACT || v == SWEEP_CELL ||
+         v == SWEEP_CELL_EXACT;
+}
+// Variants whose right-hand side is the per-line stencil table (SweepField::wt).
+inline bool stencil_filter_variant(int v) { return v == SWEEP_FILTER || v == SWEEP_FILTER_EXACT; }
+// Variants with the per-cell right-hand side.
+inline bool cell_filter_variant(int v) { return v == SWEEP_CELL || v == SWEEP_CELL_EXACT; }
+// The filter kernel's cluster form (exact periodic closure, out of place).
+inline bool exact_filter_variant(int v) { return v == SWEEP_FILTER_EXACT || v == SWEEP_CELL_EXACT; }
 constexpr int FILTER_JMAX = 64;  // longest recurrence warm-up of the filter kernel
 
 // Shared-memory bytes of the sweep kernels for a launch.
 size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source = false);
 size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64);
-size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact = false);
+size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact = false,
+                               bool cell = false);
 // Longest segment (cells per CTA along a line) of the filter kernel for a
 // recurrence warm-up of J cells.
 int filter_segment_max(int J);

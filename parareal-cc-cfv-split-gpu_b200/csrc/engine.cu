@@ -290,7 +290,10 @@ LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64
   const bool uniform = g.velocity == CCFV_VEL_REF_ROT4 || g.velocity == CCFV_VEL_CONST ||
                        g.velocity == CCFV_VEL_ROTATION;
   G.variant = g.source ? SWEEP_GENERAL_SRC : SWEEP_GENERAL;
-  if (!g.source && uniform && g.bc == CCFV_BC_PERIODIC && dsrc == 0) {
+  if (!g.source && g.bc == CCFV_BC_PERIODIC && dsrc == 0) {
+    // periodic, derivative of the sweep input: the filter kernel, with the
+    // per-line stencil (uniform displacement) or the per-cell right-hand side
+    const LaunchGeom general = G;
     int J = 0;
     const bool warm = filter_params(g, dir, Dt, fp64, nullptr, nullptr, &J, theta) && L > 2 * J;
     const int seg_exact = filter_segment_max(0);  // cells per CTA without warm-up
@@ -299,12 +302,12 @@ LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64
       // (exact periodic closure across the segments, no warm-up)
       const int lc = std::min(seg_exact, std::max({32, (L + MAX_CLUSTER - 1) / MAX_CLUSTER,
                                                    std::min(L, filter_lc(L, fp64))}));
-      G.variant = SWEEP_FILTER_EXACT;
+      G.variant = uniform ? SWEEP_FILTER_EXACT : SWEEP_CELL_EXACT;
       G.cs = (L + lc - 1) / lc;
       G.lc_max = (L + G.cs - 1) / G.cs;
       G.halo = sh + 6;
     } else if (warm) {
-      G.variant = SWEEP_FILTER;
+      G.variant = uniform ? SWEEP_FILTER : SWEEP_CELL;
       G.halo = J + sh + 6;
       // segment length from the tuner; the segments of a line form one
       // cluster (at most MAX_CLUSTER CTAs)
@@ -314,15 +317,16 @@ LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64
       G.cs = (L + lc - 1) / lc;
       G.lc_max = (L + G.cs - 1) / G.cs;
       if (inplace && G.cs > MAX_CLUSTER) {  // in place, a line's segments form one cluster
-        G = LaunchGeom();
-        G.cs = (L + LC_MAX - 1) / LC_MAX;
-        G.lc_max = (L + G.cs - 1) / G.cs;
-        G.halo = sh + 5;
-        G.variant = SWEEP_FAST;
+        G = general;
+        if (uniform) G.variant = SWEEP_FAST;
       }
-    } else {
+    } else if (uniform) {
       G.variant = SWEEP_FAST;
     }
+    if (cell_filter_variant(G.variant) &&
+        sweep_filter_smem_bytes(G.lc_max, G.halo, fp64, exact_filter_variant(G.variant), true) >
+            227 * 1024)
+      G = general;  // the per-cell form's two tiles do not fit: per-cell scan kernel
   }
   return G;
 }
@@ -351,7 +355,8 @@ int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen) 
     g_lc_override = lc;
     StepPlan plan;
     int rc = build_step_plan(ctx, &plan, dt, fp64, pf);
-    if (rc == CCFV_OK && plan.geom[0].variant != SWEEP_FILTER && plan.geom[1].variant != SWEEP_FILTER) {
+    if (rc == CCFV_OK && plan.geom[0].variant != SWEEP_FILTER && plan.geom[1].variant != SWEEP_FILTER &&
+        plan.geom[0].variant != SWEEP_CELL && plan.geom[1].variant != SWEEP_CELL) {
       g_lc_override = 0;
       break;  // nothing to tune: this grid does not use the filter kernel
     }
@@ -435,11 +440,13 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
     const bool plan_pp = !fields.empty() && fields[0].B != nullptr;
     LaunchGeom G = step_geom(g, dir, Dt, dsrc, fp64, !plan_pp, theta);
     if (ctx->force_general && G.variant != SWEEP_GENERAL_SRC) G.variant = SWEEP_GENERAL;
-    if (G.cs > MAX_CLUSTER && !(G.variant == SWEEP_FILTER && plan_pp))
+    if (G.cs > MAX_CLUSTER &&
+        !((G.variant == SWEEP_FILTER || G.variant == SWEEP_CELL) && plan_pp))
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
     if (std::max({sweep_smem_bytes(G.lc_max, G.halo, fp64, g.source != 0),
                   sweep_fast_smem_bytes(G.lc_max, G.halo, fp64),
-                  sweep_filter_smem_bytes(G.lc_max, G.halo, fp64, true)}) > 227 * 1024)
+                  sweep_filter_smem_bytes(G.lc_max, G.halo, fp64, true,
+                                          cell_filter_variant(G.variant))}) > 227 * 1024)
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
     for (int i = 0; i < nf; ++i) {
       const PlanField &pfi = fields[i];
@@ -468,7 +475,7 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
   // kernel do not depend on time)
   int lines[3] = {0, 0, 0};
   for (int kind = 0; kind < 3 && nf > 0; ++kind) {
-    if (!filter_variant(plan->geom[kind].variant)) continue;
+    if (!stencil_filter_variant(plan->geom[kind].variant)) continue;
     lines[kind] = h[(size_t)kind * nf].groups * LPG;
     CK(plan->wt[kind].alloc((fp64 ? 8 : 4) * 8 * (size_t)lines[kind]));
     CK(plan->nt[kind].alloc(sizeof(int) * (size_t)lines[kind]));

@@ -158,8 +158,8 @@ static void prepare_field(std::vector<PreparedField> &out, int kind, const ccfv_
   pf.level = std::get<1>(tkey);
   pf.f = f0;
   pf.f.halo_f = pf.G.halo;
-  if (filt) {
-    filter_field(g, pf.f, fp64);
+  if (filt) filter_field(g, pf.f, fp64);
+  if (stencil_filter_variant(pf.G.variant)) {
     FilterTable &T = (*tabs)[tkey];  // shared by every field of this key
     if (!T.lines) {
       T.lines = pf.f.groups * LPG;
@@ -302,11 +302,12 @@ int MultiEngine::add(const ccfv_problem &pr, int *slot) {
       const int dsrc = (kind == 2 && P->g.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
       const LaunchGeom G = step_geom(P->g, dir, Dt, dsrc, level == 0 || P->g64, false,
                                      level == 0 ? 0.5 : th);
-      if (G.variant != SWEEP_FILTER && G.cs > MAX_CLUSTER)
+      if (G.variant != SWEEP_FILTER && G.variant != SWEEP_CELL && G.cs > MAX_CLUSTER)
         return fail(CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
       if (std::max({sweep_smem_bytes(G.lc_max, G.halo, true, P->g.source != 0),
                     sweep_fast_smem_bytes(G.lc_max, G.halo, true),
-                    sweep_filter_smem_bytes(G.lc_max, G.halo, true, true)}) > 227 * 1024)
+                    sweep_filter_smem_bytes(G.lc_max, G.halo, true, true,
+                                            cell_filter_variant(G.variant))}) > 227 * 1024)
         return fail(CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
     }
   MCK(cudaMallocAsync(&P->mem, P->bytes, st_));

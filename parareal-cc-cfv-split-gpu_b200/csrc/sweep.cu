@@ -1164,6 +1164,7 @@ constexpr int FPW = FLANES * FCH + 8;
 template <typename T>
 struct FiltSmem {
   T *C;      // [filter_tile_rows * PITCH]  input cells, then w, then x
+  T *B;      // per-cell form: [filter_tile_rows * PITCH]  b of every position
   T *om;     // [8 * LPG]  weights of w's input (1/c) M b as an 8-tap stencil of C
   T *pwt;    // [32]       (-mu)^(i+1), i = 0 .. FCH-1
   T *pwa;    // exact form: [FPW] (-mu)^e
@@ -1173,7 +1174,7 @@ struct FiltSmem {
   int rows;
 };
 
-template <typename T, bool EXACT>
+template <typename T, bool EXACT, bool CELL>
 __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max, int H) {
   FiltSmem<T> s;
   s.fd = reinterpret_cast<SweepField *>(raw);
@@ -1189,6 +1190,7 @@ __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max
   }
   s.C = p;
   s.rows = filter_tile_rows(lc_max, H);
+  s.B = CELL ? p + (size_t)s.rows * PITCH : nullptr;
   return s;
 }
 
@@ -1240,6 +1242,84 @@ __device__ __forceinline__ void filter_line_stencil(const SweepField &F, long lo
   }
 }
 
+// Per-cell right-hand side of the filter kernel (velocity fields whose feet
+// differ from edge to edge, periodic cells, derivative of the sweep input).
+// One edge e of a line: its foot's cell kf and offset xi, the PPM
+// antiderivative of cell kf at xi (I(xi), d_intC_ppm4th, T2S4:63-65) and the
+// fourth-order derivative at the foot (dcdx_bar_on_gpu, T2S4:440-547).  The
+// remap of cell k is then I_{k+1} - I_k plus the whole cells between the two
+// feet (x_step_intC_ppm_on_gpu, T2S4:306-347), so every foot, PPM
+// reconstruction and derivative is evaluated once per edge instead of twice
+// per cell.
+template <typename T>
+struct CellEdge {
+  int kf;
+  T phi, d;
+};
+
+template <typename T>
+__device__ __forceinline__ CellEdge<T> cell_edge(const SweepField &F, const LineFeet &lf,
+                                                 const T *ccol, int rb, int nrows, int e,
+                                                 unsigned *status) {
+  const double f = lf.foot(F, e);
+  const double u = (f - F.s_min) / F.h;
+  const double fk = floor(u);
+  CellEdge<T> r;
+  r.kf = (int)fk;
+  const T xi = T(u - fk);
+  const int row = r.kf + rb;
+  if (row < 2 || row + 2 >= nrows) {  // cannot happen within the staged halo
+    atomicOr(status, STATUS_HALO);
+    r.phi = T(0);
+    r.d = T(0);
+    return r;
+  }
+  const T *cp = ccol + (row - 2) * PITCH;
+  const T cm2 = cp[0], cm1 = cp[PITCH], c0 = cp[2 * PITCH], cp1 = cp[3 * PITCH],
+          cp2 = cp[4 * PITCH];
+  // PPM edge values and curvature of cell kf (x_step_ppm_coef_on_gpu, T2S4:260-304)
+  const T cl = T(7.0 / 12.0) * (c0 + cm1) - T(1.0 / 12.0) * (cp1 + cm2);
+  const T cr = T(7.0 / 12.0) * (cp1 + c0) - T(1.0 / 12.0) * (cp2 + cm1);
+  const T D = cr - cl;
+  const T C6 = T(6.0) * (c0 - T(0.5) * (cl + cr));
+  const T xi2 = xi * xi, xi3 = xi2 * xi;
+  r.phi = T(-1.0 / 3) * C6 * xi3 + T(0.5) * (D + C6) * xi2 + cl * xi;
+  r.d = T(F.inv12h) * ((T(2.0) * xi3 - T(6.0) * xi2 + T(3.0) * xi + T(1.0)) * cm2 +
+                       (T(-8.0) * xi3 + T(18.0) * xi2 + T(6.0) * xi - T(15.0)) * cm1 +
+                       (T(12.0) * xi3 - T(18.0) * xi2 - T(24.0) * xi + T(15.0)) * c0 +
+                       (T(-8.0) * xi3 + T(6.0) * xi2 + T(18.0) * xi - T(1.0)) * cp1 +
+                       (T(2.0) * xi3 - T(3.0) * xi) * cp2);
+  return r;
+}
+
+// b of the cell between edges l and l+1: remap + (1-theta) K Dt/h (D_r - D_l)
+// (x_b_RHS_on_gpu, T2S4:564-613, source-free); the whole cells between the
+// feet are summed with Neumaier compensation (periodic remap of sweep_kernel).
+template <typename T>
+__device__ __forceinline__ T cell_rhs(const CellEdge<T> &l, const CellEdge<T> &r, const T *ccol,
+                                      int rb, int nrows, T kbc, unsigned *status) {
+  T remap;
+  if (r.kf == l.kf) {
+    remap = r.phi - l.phi;
+  } else {
+    const int lo = min(l.kf, r.kf), hi = max(l.kf, r.kf) - 1;
+    T s = T(0), comp = T(0);
+    if (lo + rb < 0 || hi + rb >= nrows) {
+      atomicOr(status, STATUS_HALO);
+    } else {
+      for (int k = lo; k <= hi; ++k) {
+        const T x = ccol[(k + rb) * PITCH];
+        const T t = s + x;
+        comp += (fabs(s) >= fabs(x)) ? ((s - t) + x) : ((x - t) + s);
+        s = t;
+      }
+    }
+    s += comp;
+    remap = r.kf > l.kf ? (s + r.phi) - l.phi : -((s + l.phi) - r.phi);
+  }
+  return remap + kbc * (r.d - l.d);
+}
+
 // The per-line stencil table of one field (one thread per line).
 template <typename T>
 __global__ void filter_weights_kernel(const SweepField *__restrict__ f, T *__restrict__ wt,
@@ -1274,8 +1354,15 @@ __global__ void filter_weights_kernel(const SweepField *__restrict__ f, T *__res
 // segment; each cell adds carry * (-mu)^distance from a power table.  The
 // field, its activity and the segment length are uniform over a cluster, so
 // every CTA of a cluster reaches every cluster barrier.
-template <typename T, bool EXACT>
-__global__ void __launch_bounds__(NTH, 4)
+//
+// CELL (velocity fields whose feet differ from edge to edge): the staged
+// cells first give every position's b (per-edge feet, PPM antiderivatives and
+// foot derivatives, cell_edge / cell_rhs) in a second tile, each line's
+// half-warp filling its own column; the forward filter then takes w's input
+// as the mass-matrix stencil (1/12c)(b_{k-1} + 10 b_k + b_{k+1}).  Two tiles
+// and the per-edge arithmetic: two CTAs per SM.
+template <typename T, bool EXACT, bool CELL>
+__global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
     sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
                         double toff, void *data_override, int lc_max, int H, unsigned *status,
                         int jstep, int nslice, const int *nlo, int cs, int clustered,
@@ -1286,7 +1373,7 @@ __global__ void __launch_bounds__(NTH, 4)
   // of different segment lengths share one launch (lc_max and H size the
   // shared memory only)
   const int cta = (int)blockIdx.x + group_base;
-  FiltSmem<T> S = carve_filt<T, EXACT>(smem_raw, lc_max, H);
+  FiltSmem<T> S = carve_filt<T, EXACT, CELL>(smem_raw, lc_max, H);
   {
     // a field's CTAs start at cta0 = group0 * cs (cs is uniform over a launch)
     const int lo = find_field(fields, g0idx, nfields, cta / cs);
@@ -1373,7 +1460,9 @@ __global__ void __launch_bounds__(NTH, 4)
       }
     }
   }
-  if (F.wt) {  // per-line stencil from the plan's table, copied with the cells
+  if (CELL) {
+    // per-cell form: no per-line stencil (b is computed per cell below)
+  } else if (F.wt) {  // per-line stencil from the plan's table, copied with the cells
     if (threadIdx.x < 8 * LPG) {
       const T *src = reinterpret_cast<const T *>(F.wt) + line0 * 8 + threadIdx.x;
       if (sizeof(T) == 8) cp_async8(S.om + threadIdx.x, src); else cp_async4(S.om + threadIdx.x, src);
@@ -1383,7 +1472,7 @@ __global__ void __launch_bounds__(NTH, 4)
     }
   }
   cp_async_commit();
-  if (!F.wt && threadIdx.x < LPG) {
+  if (!CELL && !F.wt && threadIdx.x < LPG) {
     filter_line_stencil<T>(F, line0 + threadIdx.x, toff, S.om + 8 * threadIdx.x,
                            S.n0 + threadIdx.x);
   } else if (threadIdx.x == 9 * LPG) {
@@ -1420,16 +1509,62 @@ __global__ void __launch_bounds__(NTH, 4)
     const T mmu = -mu;
     const T pw = S.pwt[FCH - 1];      // (-mu)^FCH
 
+    if (CELL) {
+      // b of positions [p0 - J - 1, p0 - J + FLANES * FCH + 1) into this
+      // line's column of the second tile: every row the forward walk reads
+      // (zero past p1 + J + 1, where the walk's values are masked); lane c
+      // takes a contiguous run and carries the previous edge
+      const long long gl = line0 + ln;
+      const int kb = p0 - J - 1;
+      const int kw = p0 - J + FLANES * FCH + 1;
+      const int kv = min(kw, p1 + J + 1);
+      const int mm = (kw - kb + FLANES - 1) / FLANES;
+      const int s0 = kb + c * mm, s1 = min(kw, s0 + mm);
+      const double tau0 = F.t_min + F.ht * (double)gl;
+      const LineFeet lf(F, tau0, tau0 + F.ht, toff + F.ta_rel, toff + F.tb_rel);
+      const T *ccol = S.C + ln;
+      T *bcol = S.B + ln;
+      const T kbc = T(F.kb);
+      if (s0 < s1) {
+        CellEdge<T> el{0, T(0), T(0)};
+        if (s0 < kv) el = cell_edge<T>(F, lf, ccol, rb, nrows, s0, status);
+        for (int k = s0; k < s1; ++k) {
+          T b = T(0);
+          if (k < kv) {
+            const CellEdge<T> er = cell_edge<T>(F, lf, ccol, rb, nrows, k + 1, status);
+            b = cell_rhs<T>(el, er, ccol, rb, nrows, kbc, status);
+            el = er;
+          }
+          bcol[(k + rb) * PITCH] = b;
+        }
+      }
+      __syncwarp(fm);
+    }
+
     // forward: w_k = (1/c) M b_k - mu w_{k-1} over [p0 - J, qb), qb = p1 + J.
     // Lanes past qb walk stage rows that are allocated but not staged: their
     // values only flow further right and are masked by the backward load.
     const int qb = p1 + J;
     const int k0 = p0 - J + c * FCH;
-    const int r0 = k0 + S.n0[ln] - 3 + rb;  // row of tap -3 of position k0
-    const bool ok = r0 >= 0 && r0 + FCH + 7 <= S.rows;
+    const int r0 = CELL ? k0 - 1 + rb : k0 + S.n0[ln] - 3 + rb;  // row of the first tap
+    const bool ok = r0 >= 0 && r0 + FCH + (CELL ? 2 : 7) <= S.rows;
     if (!ok) atomicOr(status, STATUS_HALO);
     T v[FCH];
-    {
+    if (CELL) {
+      // w_k = (1/12c)(b_{k-1} + 10 b_k + b_{k+1}) - mu w_{k-1}
+      const T icw = T(F.sm_inv_den / 12.0);
+      const T *bp = S.B + (ok ? r0 : 0) * PITCH + ln;
+      T b0 = bp[0], b1 = bp[PITCH];
+      T w = T(0);
+#pragma unroll
+      for (int i = 0; i < FCH; ++i) {
+        const T b2 = bp[(2 + i) * PITCH];
+        w = icw * ((b0 + b2) + T(10.0) * b1) + mmu * w;
+        v[i] = w;
+        b0 = b1;
+        b1 = b2;
+      }
+    } else {
       const T *omp = S.om + 8 * ln;
       const T o0 = omp[0], o1 = omp[1], o2 = omp[2], o3 = omp[3], o4 = omp[4], o5 = omp[5],
               o6 = omp[6], o7 = omp[7];
@@ -1445,6 +1580,8 @@ __global__ void __launch_bounds__(NTH, 4)
         v[i] = w;
         w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6; w6 = w7;
       }
+    }
+    {
       // carries: chunk map x -> pw x + e_c, inclusive scan over the line's lanes
       T sa = pw, sb = v[FCH - 1];
 #pragma unroll
@@ -1633,11 +1770,11 @@ size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source) {
   return FD_BYTES + n * el;
 }
 
-size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact) {
+size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact, bool cell) {
   size_t el = fp64 ? 8 : 4;
   return FD_BYTES + 64 * sizeof(int) +
          (8 * (size_t)LPG + 32 + (exact ? (size_t)FPW + 2 * LPG : 0) +
-          (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el;
+          (cell ? 2 : 1) * (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el;
 }
 
 int filter_segment_max(int J) { return filter_seg_max(J); }
@@ -1669,10 +1806,11 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
                                int nslice, const int *nlo, bool inplace, cudaStream_t stream,
                                const int *g0idx) {
   const bool fast = (variant == SWEEP_FAST);
-  const bool exact = (variant == SWEEP_FILTER_EXACT);
-  const bool filt = (variant == SWEEP_FILTER) || exact;
+  const bool cell = (variant == SWEEP_CELL) || (variant == SWEEP_CELL_EXACT);
+  const bool exact = exact_filter_variant(variant);
+  const bool filt = filter_variant(variant);
   const bool src = (variant == SWEEP_GENERAL_SRC);
-  const size_t smem = filt ? sweep_filter_smem_bytes(lc_max, halo, sizeof(T) == 8, exact)
+  const size_t smem = filt ? sweep_filter_smem_bytes(lc_max, halo, sizeof(T) == 8, exact, cell)
                       : fast ? sweep_fast_smem_bytes(lc_max, halo, sizeof(T) == 8)
                              : sweep_smem_bytes(lc_max, halo, sizeof(T) == 8, src);
   {
@@ -1691,8 +1829,10 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
       if (!configured[dev].load(std::memory_order_relaxed)) {
         for (const void *fn :
              {(const void *)sweep_kernel<T>, (const void *)sweep_fast_kernel<T>,
-              (const void *)sweep_filter_kernel<T, false>,
-              (const void *)sweep_filter_kernel<T, true>}) {
+              (const void *)sweep_filter_kernel<T, false, false>,
+              (const void *)sweep_filter_kernel<T, true, false>,
+              (const void *)sweep_filter_kernel<T, false, true>,
+              (const void *)sweep_filter_kernel<T, true, true>}) {
           err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      227 * 1024);
           if (err != cudaSuccess) return err;
@@ -1707,9 +1847,14 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   if (exact && inplace) return cudaErrorInvalidValue;  // the exact form sweeps out of place
   if (filt && !exact && (cs == 1 || !inplace)) {  // whole lines per CTA, or out of place: no cluster
     count_launch();
-    sweep_filter_kernel<T, false><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
-        d_fields, nfields, group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
-        nlo, cs, 0, g0idx);
+    if (cell)
+      sweep_filter_kernel<T, false, true><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
+          d_fields, nfields, group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
+          nlo, cs, 0, g0idx);
+    else
+      sweep_filter_kernel<T, false, false><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
+          d_fields, nfields, group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
+          nlo, cs, 0, g0idx);
     return cudaGetLastError();
   }
   cudaLaunchConfig_t cfg = {};
@@ -1726,13 +1871,19 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   cfg.numAttrs = 1;
   count_launch();
   if (exact)  // one cluster per tile: the cs segments of its lines
-    return cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T, true>, d_fields, nfields,
-                              group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
-                              nlo, cs, 0, g0idx);
+    return cell ? cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T, true, true>, d_fields, nfields,
+                                     group_base * cs, toff, data, lc_max, halo, d_status, jstep,
+                                     nslice, nlo, cs, 0, g0idx)
+                : cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T, true, false>, d_fields,
+                                     nfields, group_base * cs, toff, data, lc_max, halo,
+                                     d_status, jstep, nslice, nlo, cs, 0, g0idx);
   if (filt)  // group_base in CTAs
-    return cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T, false>, d_fields, nfields,
-                              group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
-                              nlo, cs, 1, g0idx);
+    return cell ? cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T, false, true>, d_fields,
+                                     nfields, group_base * cs, toff, data, lc_max, halo,
+                                     d_status, jstep, nslice, nlo, cs, 1, g0idx)
+                : cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T, false, false>, d_fields,
+                                     nfields, group_base * cs, toff, data, lc_max, halo,
+                                     d_status, jstep, nslice, nlo, cs, 1, g0idx);
   if (fast)
     return cudaLaunchKernelEx(&cfg, sweep_fast_kernel<T>, d_fields, nfields, group_base, toff,
                               data, lc_max, halo, d_status, jstep, nslice, nlo, g0idx);

@@ -208,6 +208,41 @@ def test_periodic_exact_filter_matches_oracle(oracle, ccfv, nx, ny, K):
     assert abs(out.sum() - C0.sum()) < 1e-12 * np.abs(C0).sum()
 
 
+@pytest.mark.parametrize("nx,ny,K,form", [(64, 64, 1e-3, "cell"), (300, 260, 1e-4, "cell"),
+                                          (2048, 40, 1e-3, "cell"), (4096, 24, 1e-4, "cell"),
+                                          (96, 96, 0.3, "cell_exact"),
+                                          (1000, 520, 0.05, "cell_exact"),
+                                          (2048, 64, 0.02, "cell_exact")])
+def test_periodic_cell_filter_matches_oracle(oracle, ccfv, nx, ny, K, form):
+    """Swirling deformation (feet differ from edge to edge): the filter
+    kernel with the per-cell right-hand side, warm-up form (1 to 18 segments
+    per line) and cluster form (strong diffusion), against the oracle's
+    per-cell remap and Sherman-Morrison cyclic solve."""
+    dt = 0.8 / max(nx, ny)
+    C0 = periodic_field(nx, 31, ny=ny)
+    g = oracle.grid(nx, ny, bc=1, vel=3, vp=(1.5,), K=K, threads=THREADS, scheme=1)
+    ref = oracle.run(g, C0, 0.35, dt, 2)
+    s = ccfv.Solver(ccfv.make_grid(nx, ny, bc=1, velocity=3, vel_params=(1.5,), K=K, scheme=1))
+    assert form in [v for v, _ in s.sweep_plan(dt)]
+    c = dev(C0)
+    s.run(c, 0.35, dt, 2)
+    s.check()
+    out = host(c)
+    assert rel_l2(out, ref) < TOL
+    assert abs(out.sum() - C0.sum()) < 1e-12 * np.abs(C0).sum()
+
+
+def test_fp32_cell_filter_coarse_close_to_fp64(ccfv):
+    N = 256
+    C0 = periodic_field(N, 14)
+    s = ccfv.Solver(ccfv.make_grid(N, bc=1, velocity=3, vel_params=(1.5,), K=1e-3, scheme=1))
+    assert "cell" in [v for v, _ in s.sweep_plan(0.01, ccfv.FP32)]
+    a, b = dev(C0), dev(C0)
+    s.coarse(a, 0.2, 0.02, 2, ccfv.FP64)
+    s.coarse(b, 0.2, 0.02, 2, ccfv.FP32)
+    assert rel_l2(host(b), host(a)) < 2e-6
+
+
 def test_fp32_exact_filter_coarse_close_to_fp64(ccfv):
     N, K = 640, 0.05  # coarse steps of diffusion number ~60: the exact cluster form
     C0 = periodic_field(N, 13)
