@@ -327,6 +327,33 @@ LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64
         sweep_filter_smem_bytes(G.lc_max, G.halo, fp64, exact_filter_variant(G.variant), true) >
             227 * 1024)
       G = general;  // the per-cell form's two tiles do not fit: per-cell scan kernel
+  } else if (!g.source && g.bc == CCFV_BC_COMPAT) {
+    // the reference's boundaries: the filter kernel's per-cell form with the
+    // non-cyclic closure.  A line of at most one segment is solved exactly
+    // (the recurrences start at its ends, no warm-up, any diffusion number);
+    // longer lines need the warm-up between segments.
+    const LaunchGeom general = G;
+    const int extra = dsrc ? (sh + 4) + sh + 4 : sh + 6;  // foot + stencil (+ remapped field)
+    int J = 0;
+    const bool jok = filter_params(g, dir, Dt, fp64, nullptr, nullptr, &J, theta) && L > 2 * J;
+    if (L <= filter_segment_max(0)) {
+      G.variant = SWEEP_CELL;
+      G.cs = 1;
+      G.lc_max = L;
+      G.halo = extra;
+    } else if (jok) {
+      G.variant = SWEEP_CELL;
+      G.halo = J + extra;
+      const int lc = std::min(filter_segment_max(J),
+                              std::max({32, (L + MAX_CLUSTER - 1) / MAX_CLUSTER,
+                                        std::min(L, filter_lc(L, fp64))}));
+      G.cs = (L + lc - 1) / lc;
+      G.lc_max = (L + G.cs - 1) / G.cs;
+      if (inplace && G.cs > MAX_CLUSTER) G = general;
+    }
+    if (G.variant == SWEEP_CELL &&
+        sweep_filter_smem_bytes(G.lc_max, G.halo, fp64, false, true) > 227 * 1024)
+      G = general;
   }
   return G;
 }
@@ -401,7 +428,9 @@ void filter_field(const ccfv_grid &g, SweepField &f, bool fp64) {
   filter_params(g, f.dir, f.Dt, fp64, &mu, &ic, &J, f.theta);
   f.sm_fac = mu;
   f.sm_inv_den = ic;
-  f.jf = J;
+  // compat lines of one segment: the non-cyclic recurrences start exactly at
+  // the line's ends (no warm-up)
+  f.jf = (g.bc == CCFV_BC_COMPAT && f.L <= filter_segment_max(0)) ? 0 : J;
 }
 
 // Sub-steps of one split step: x(dt/2) over [t, t+dt/2], y(dt) over

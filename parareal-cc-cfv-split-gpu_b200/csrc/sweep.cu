@@ -1320,6 +1320,49 @@ __device__ __forceinline__ T cell_rhs(const CellEdge<T> &l, const CellEdge<T> &r
   return remap + kbc * (r.d - l.d);
 }
 
+// Compat boundaries (the reference's): an edge whose foot lies inside
+// [s_min + eps, s_max - eps] is "normal" (its remap clamps are no-ops); cells
+// next to an edge that is not, or whose feet cross, take the reference's
+// per-cell remap with its clamps and zero inflow (remap_cell, T2S4:306-438).
+// The foot derivative keeps the reference's ghost selection (foot_derivative).
+template <typename T>
+struct CompatEdge {
+  double f;
+  int kf;
+  bool normal;
+  T phi, d;
+};
+
+template <typename T>
+__device__ __forceinline__ CompatEdge<T> compat_edge(const SweepField &F, const LineFeet &lf,
+                                                     const LineView<T> &vc,
+                                                     const LineView<T> &vd, int e) {
+  CompatEdge<T> r;
+  r.f = lf.foot(F, e);
+  r.normal = r.f >= F.s_min + F.eps_remap && r.f <= F.s_max - F.eps_remap;
+  r.kf = 0;
+  r.phi = T(0);
+  if (r.normal) {
+    const double u = (r.f - F.s_min) / F.h;
+    const double fk = floor(u);
+    r.kf = (int)fk;
+    r.phi = ppm_int(ppm(vc, r.kf), T(u - fk));
+  }
+  r.d = foot_derivative(F, vd, r.f);
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T compat_remap(const SweepField &F, const CompatEdge<T> &l,
+                                          const CompatEdge<T> &r, const LineView<T> &vc) {
+  if (l.normal && r.normal && r.kf >= l.kf && l.f != r.f) {
+    T s = T(0);
+    for (int k = l.kf; k < r.kf; ++k) s += vc(k);
+    return (s + r.phi) - l.phi;
+  }
+  return remap_cell(F, vc, l.f, r.f);
+}
+
 // The per-line stencil table of one field (one thread per line).
 template <typename T>
 __global__ void filter_weights_kernel(const SweepField *__restrict__ f, T *__restrict__ wt,
@@ -1419,6 +1462,9 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
   // stores would otherwise make the compiler reload it every iteration.
   const long long s_pos = F.s_pos, s_line = F.s_line, M = F.M;
   const bool xsweep = s_line == 1;
+  // compat boundaries (per-cell form only): zero outside the line, ghost
+  // cells, non-cyclic solve
+  const bool compat = CELL && F.bc == BC_COMPAT;
 
   // ---- stage rows p0-H .. p1+H-1 (periodic wrap) ----
   if (xsweep) {
@@ -1430,7 +1476,11 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
       const T *gcol = gsrc + gl;
       for (int row = row0; row < nrows; row += 2 * NW) {
         int pos = p0 - H + row;
-        if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
+        if (pos < 0 || pos >= L) {  // halo rows: periodic wrap, or zero (compat)
+          if (compat) {
+            dcol[row * PITCH] = T(0);
+            continue;
+          }
           pos %= L;
           if (pos < 0) pos += L;
         }
@@ -1448,7 +1498,11 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
         const T *lbase = gsrc + gl * s_line;
         for (int row = lane; row < nrows; row += 32) {
           int pos = p0 - H + row;
-          if (pos < 0 || pos >= L) {  // halo rows: periodic wrap
+          if (pos < 0 || pos >= L) {  // halo rows: periodic wrap, or zero (compat)
+            if (compat) {
+              dcol[row * PITCH] = T(0);
+              continue;
+            }
             pos %= L;
             if (pos < 0) pos += L;
           }
@@ -1487,6 +1541,10 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
     for (int e = threadIdx.x; e < FPW; e += NTH) S.pwa[e] = T(powi(-F.sm_fac, e));
   cp_async_wait_all_committed();
   __syncthreads();
+  if (compat) {  // extrapolated ghost cells C_{-2}, C_{-1}, C_L, C_{L+1} (T2S4:275-286)
+    if (threadIdx.x < LPG) compat_ghosts(S.C + threadIdx.x, H - p0, p0 - H, p1 + H, L);
+    __syncthreads();
+  }
   // In place, the segments of a line are read (halo) by the neighbouring CTAs
   // of its cluster: this CTA's reads are complete here, and no CTA of the
   // cluster stores before every CTA has arrived.  Out of place (ping-pong),
@@ -1523,19 +1581,71 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
       const double tau0 = F.t_min + F.ht * (double)gl;
       const LineFeet lf(F, tau0, tau0 + F.ht, toff + F.ta_rel, toff + F.tb_rel);
       const T *ccol = S.C + ln;
-      T *bcol = S.B + ln;
       const T kbc = T(F.kb);
-      if (s0 < s1) {
-        CellEdge<T> el{0, T(0), T(0)};
-        if (s0 < kv) el = cell_edge<T>(F, lf, ccol, rb, nrows, s0, status);
-        for (int k = s0; k < s1; ++k) {
-          T b = T(0);
-          if (k < kv) {
-            const CellEdge<T> er = cell_edge<T>(F, lf, ccol, rb, nrows, k + 1, status);
-            b = cell_rhs<T>(el, er, ccol, rb, nrows, kbc, status);
-            el = er;
+      if (!compat) {
+        T *bcol = S.B + ln;
+        if (s0 < s1) {
+          CellEdge<T> el{0, T(0), T(0)};
+          if (s0 < kv) el = cell_edge<T>(F, lf, ccol, rb, nrows, s0, status);
+          for (int k = s0; k < s1; ++k) {
+            T b = T(0);
+            if (k < kv) {
+              const CellEdge<T> er = cell_edge<T>(F, lf, ccol, rb, nrows, k + 1, status);
+              b = cell_rhs<T>(el, er, ccol, rb, nrows, kbc, status);
+              el = er;
+            }
+            bcol[(k + rb) * PITCH] = b;
           }
-          bcol[(k + rb) * PITCH] = b;
+        }
+      } else {
+        // b = 0 outside the line (the compact mass matrix's zero ghosts)
+        const int ka = max(s0, 0), kz = min(min(s1, kv), L);
+        const LineView<T> vc{S.C + ln, rb, nrows, status};
+        if (!F.dsrc) {
+          T *bcol = S.B + ln;
+          if (ka < kz) {
+            CompatEdge<T> el = compat_edge<T>(F, lf, vc, vc, ka);
+            for (int k = ka; k < kz; ++k) {
+              const CompatEdge<T> er = compat_edge<T>(F, lf, vc, vc, k + 1);
+              bcol[(k + rb) * PITCH] = compat_remap<T>(F, el, er, vc) + kbc * (er.d - el.d);
+              el = er;
+            }
+          }
+          for (int k = s0; k < s1; ++k)
+            if (k < ka || k >= kz) bcol[(k + rb) * PITCH] = T(0);
+        } else {
+          // the reference's third sweep differentiates the remapped field
+          // (dcdx_bar_on_gpu(v_d_Cnphf_bar_x, ...), T2S4:929-932): remap the
+          // cells [ra0, ra1) into the second tile, its ghosts, then
+          // b = R + kbc (D_R(f_{k+1}) - D_R(f_k)) into the first tile (this
+          // line's cells are no longer read)
+          const int ra0 = max(0, kb - F.hd), ra1 = min(L, kv + F.hd);
+          const int m1 = (ra1 - ra0 + FLANES - 1) / FLANES;
+          const int q0 = ra0 + c * m1, q1 = min(ra1, q0 + m1);
+          T *rcol = S.B + ln;
+          if (q0 < q1) {
+            CompatEdge<T> el = compat_edge<T>(F, lf, vc, vc, q0);
+            for (int k = q0; k < q1; ++k) {
+              const CompatEdge<T> er = compat_edge<T>(F, lf, vc, vc, k + 1);
+              rcol[(k + rb) * PITCH] = compat_remap<T>(F, el, er, vc);
+              el = er;
+            }
+          }
+          __syncwarp(fm);
+          if (c == 0) compat_ghosts(rcol, rb, ra0 - 2, ra1 + 2, L);
+          __syncwarp(fm);
+          const LineView<T> vr{rcol, rb, nrows, status};
+          T *bcol = S.C + ln;
+          if (ka < kz) {
+            T dl = foot_derivative(F, vr, lf.foot(F, ka));
+            for (int k = ka; k < kz; ++k) {
+              const T dr = foot_derivative(F, vr, lf.foot(F, k + 1));
+              bcol[(k + rb) * PITCH] = vr(k) + kbc * (dr - dl);
+              dl = dr;
+            }
+          }
+          for (int k = s0; k < s1; ++k)
+            if (k < ka || k >= kz) bcol[(k + rb) * PITCH] = T(0);
         }
       }
       __syncwarp(fm);
@@ -1551,15 +1661,18 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
     if (!ok) atomicOr(status, STATUS_HALO);
     T v[FCH];
     if (CELL) {
-      // w_k = (1/12c)(b_{k-1} + 10 b_k + b_{k+1}) - mu w_{k-1}
+      // w_k = (1/12c)(b_{k-1} + 10 b_k + b_{k+1}) - mu w_{k-1}; compat: zero
+      // input outside the line (non-cyclic system, exact zero start at 0)
       const T icw = T(F.sm_inv_den / 12.0);
-      const T *bp = S.B + (ok ? r0 : 0) * PITCH + ln;
+      const T *bp = ((compat && F.dsrc) ? S.C : S.B) + (ok ? r0 : 0) * PITCH + ln;
       T b0 = bp[0], b1 = bp[PITCH];
       T w = T(0);
 #pragma unroll
       for (int i = 0; i < FCH; ++i) {
         const T b2 = bp[(2 + i) * PITCH];
-        w = icw * ((b0 + b2) + T(10.0) * b1) + mmu * w;
+        T in = icw * ((b0 + b2) + T(10.0) * b1);
+        if (compat && (unsigned)(k0 + i) >= (unsigned)L) in = T(0);
+        w = in + mmu * w;
         v[i] = w;
         b0 = b1;
         b1 = b2;
@@ -1595,11 +1708,20 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
       }
       T cin = __shfl_up_sync(fm, sb, 1, FLANES);
       if (c == 0) cin = T(0);
+      // + cin (-mu)^(i+1), the powers by a running product (no table loads)
 #pragma unroll
-      for (int i = 0; i < FCH; ++i) v[i] += cin * S.pwt[i];
+      for (int i = 0; i < FCH; ++i) {
+        cin *= mmu;
+        v[i] += cin;
+      }
     }
-    const int k1 = p0 + c * FCH;
-    const int nb = qb - k1;  // positions of this lane inside the backward range
+    // The backward filter runs on the same positions k0 .. k0+FCH-1 of each
+    // lane (w stays in registers); positions left of p0 are warm-up values
+    // whose x is discarded, positions from qb on start it from zero.
+    const int k1 = k0;
+    // positions of this lane inside the backward range (compat: the zero
+    // start is at the line's end, x_L = 0)
+    const int nb = (compat ? min(qb, L) : qb) - k1;
     if (EXACT) {
       // forward end of the segment from a zero carry (position p1 - 1)
       const int cend = (np - 1) / FCH, iend = (np - 1) - cend * FCH;
@@ -1636,33 +1758,19 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
         const T c0 = et / (T(1) - at);
         cr = rank > 0 ? ea * c0 + eb : c0;
       }
+      T cv = cr * S.pwa[c * FCH];
 #pragma unroll
       for (int i = 0; i < FCH; ++i) {
-        const T cv = cr * S.pwa[c * FCH + i + 1];
+        cv *= mmu;  // cr (-mu)^(c FCH + i + 1)
         v[i] = (i < nb) ? v[i] + cv : T(0);  // backward input; zero past p1
       }
     } else {
-      // every stencil read of this line is done (the shuffles order the
-      // lanes); w of positions k0 .. k0+FCH-1 into this line's column
-      __syncwarp(fm);
-      {
-        T *wp = S.C + (k0 + rb) * PITCH + ln;
 #pragma unroll
-        for (int i = 0; i < FCH; ++i) wp[i * PITCH] = v[i];
-      }
-      __syncwarp(fm);
+      for (int i = 0; i < FCH; ++i) v[i] = (i < nb) ? v[i] : T(0);  // zero from qb on
     }
 
-    // backward: x over [p0, qb), zero start at qb
+    // backward: x over [k0, qb), zero start at qb
     {
-      if (!EXACT) {
-        const T *xp = S.C + (k1 + rb) * PITCH + ln;
-#pragma unroll
-        for (int i = 0; i < FCH; ++i) {
-          const T val = xp[i * PITCH];
-          v[i] = (i < nb) ? val : T(0);
-        }
-      }
       T x = T(0);
 #pragma unroll
       for (int i = FCH - 1; i >= 0; --i) {
@@ -1682,7 +1790,10 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
       T cin = __shfl_down_sync(fm, sb, 1, FLANES);
       if (c == FLANES - 1) cin = T(0);
 #pragma unroll
-      for (int i = 0; i < FCH; ++i) v[i] += cin * S.pwt[FCH - 1 - i];
+      for (int i = FCH - 1; i >= 0; --i) {
+        cin *= mmu;  // cin (-mu)^(FCH - i)
+        v[i] += cin;
+      }
     }
     if (EXACT) {
       // backward start of the segment from a zero carry (position p0)
@@ -1720,9 +1831,36 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
       // for the others' before it exits (non-aligned forms: the wait follows
       // the divergent store loops)
       asm volatile("barrier.cluster.arrive;\n" ::: "memory");
+      T dv = d * S.pwa[max(nb - FCH, 0)];
 #pragma unroll
-      for (int i = 0; i < FCH; ++i)
-        if (i < nb) v[i] += d * S.pwa[nb - i];
+      for (int i = FCH - 1; i >= 0; --i)
+        if (i < nb) {
+          dv *= mmu;  // d (-mu)^(nb - i)
+          v[i] += dv;
+        }
+    }
+    if (compat && p0 == 0) {
+      // non-cyclic system: A = c (1 + mu S^-1)(1 + mu S) + c mu^2 e_0 e_0^T,
+      // so x = y - y_0 g with g_k = mu^2 ((-mu)^k - (-mu)^(2L-k)) /
+      // (1 - mu^(2L+2)) (Sherman-Morrison); y_0 is this segment's x at 0
+      const int c0 = J / FCH, i0 = J - c0 * FCH;
+      T y0 = T(0);
+#pragma unroll
+      for (int i = 0; i < FCH; ++i) y0 = (i == i0) ? v[i] : y0;
+      y0 = __shfl_sync(fm, y0, c0, FLANES);
+      const double q = -F.sm_fac;
+      const double A = q * q / (1.0 - powi(q * q, L + 1));
+      const bool tail = powi(fabs(q), L) >= 0x1p-60;  // (-mu)^(2L-k) still matters
+      double qk = powi(q, max(k0, 0));
+#pragma unroll
+      for (int i = 0; i < FCH; ++i) {
+        const int k = k0 + i;
+        if (k >= 0 && k < L) {
+          const double gk = A * (tail ? qk - powi(q, 2 * L - k) : qk);
+          v[i] -= y0 * T(gk);
+          qk *= q;
+        }
+      }
     }
     __syncwarp(fm);
     {
