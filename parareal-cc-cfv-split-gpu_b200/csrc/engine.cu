@@ -267,16 +267,32 @@ bool filter_params(const ccfv_grid &g, int dir, double Dt, bool fp64, double *mu
 }
 
 // Autotuned segment length (cells per CTA) of the filter kernel, per line
-// length and precision; the default until ccfv_autotune measures it.
+// length and precision (ccfv_autotune), and per line-length class (the next
+// power of two, tuned by the batched engine on the first problem of each
+// class); the default until either is measured.
 static std::mutex g_tune_mu;
-static std::map<std::pair<int, int>, int> g_filter_lc;
+static std::map<std::pair<int, int>, int> g_filter_lc;        // (L, fp64)
+static std::map<std::pair<int, int>, int> g_filter_lc_class;  // (class, fp64)
 static thread_local int g_lc_override = 0;
+
+int line_class(int L) {
+  int c = 64;
+  while (c < L) c *= 2;
+  return c;
+}
 
 int filter_lc(int L, bool fp64) {
   if (g_lc_override > 0) return g_lc_override;
   std::lock_guard<std::mutex> lk(g_tune_mu);
   auto it = g_filter_lc.find({L, fp64 ? 1 : 0});
-  return it == g_filter_lc.end() ? LC_MAX : it->second;
+  if (it != g_filter_lc.end()) return it->second;
+  auto ic = g_filter_lc_class.find({line_class(L), fp64 ? 1 : 0});
+  return ic == g_filter_lc_class.end() ? LC_MAX : ic->second;
+}
+
+bool class_tuned(int L, bool fp64) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  return g_filter_lc_class.count({line_class(L), fp64 ? 1 : 0}) > 0;
 }
 
 LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64, bool inplace,
@@ -360,10 +376,14 @@ LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64
 
 // Times the filter kernel's candidate segment lengths on this grid (x and y
 // sweeps of one step of dt on a scratch field) and keeps the fastest.
-int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen) {
+int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen, bool for_class) {
   const ccfv_grid &g = ctx->grid;
   const size_t el = fp64 ? 8 : 4;
   const size_t NN = (size_t)g.nx * g.ny;
+  if (!ctx->status.p) {  // contexts of the batched engine's problems have none
+    CK(ctx->status.alloc(sizeof(unsigned) * 4));
+    CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(unsigned) * 4, st));
+  }
   CK(ctx->io.alloc(2 * el * NN));
   CK(cudaMemsetAsync(ctx->io.p, 0, 2 * el * NN, st));
   // timed as the Parareal engines run it: out of place over a buffer pair
@@ -412,11 +432,17 @@ int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen) 
   cudaEventDestroy(b);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_filter_lc[{g.nx, fp64 ? 1 : 0}] = best_lc;
-    g_filter_lc[{g.ny, fp64 ? 1 : 0}] = best_lc;
+    if (for_class) {  // the class of each line length, unless tuned already
+      g_filter_lc_class.insert({{line_class(g.nx), fp64 ? 1 : 0}, best_lc});
+      g_filter_lc_class.insert({{line_class(g.ny), fp64 ? 1 : 0}, best_lc});
+    } else {
+      g_filter_lc[{g.nx, fp64 ? 1 : 0}] = best_lc;
+      g_filter_lc[{g.ny, fp64 ? 1 : 0}] = best_lc;
+    }
   }
   ctx->step_plans.clear();  // plans built with the old geometry
   ctx->fine_plan.reset();
+  if (for_class) ctx->io.release();  // scratch of the timing runs only
   if (chosen) *chosen = best_lc;
   return CCFV_OK;
 }

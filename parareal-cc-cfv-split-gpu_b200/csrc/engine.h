@@ -24,6 +24,11 @@ struct DevBuf {
   DevBuf &operator=(const DevBuf &) = delete;
   ~DevBuf() { if (p) cudaFree(p); }
   cudaError_t alloc(size_t b);
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
   template <typename T> T *as() const { return reinterpret_cast<T *>(p); }
 };
 
@@ -106,7 +111,14 @@ inline bool coarse_theta_ok(double th) {
   return th == 0.0 || th == CCFV_COARSE_THETA_AUTO || (th >= 0.5 && th <= 1.0);
 }
 void filter_field(const ccfv_grid &g, SweepField &f, bool fp64);
-int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen);
+// for_class: keep the choice for the line-length classes of this grid (the
+// batched engine) instead of its exact line lengths (ccfv_autotune).
+int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen,
+             bool for_class = false);
+// Whether the line-length class of L has a tuned segment length.
+bool class_tuned(int L, bool fp64);
+// The next power of two >= L (at least 64): the batched engine's tuning class.
+int line_class(int L);
 int batch_solve(int n, const ccfv_problem *probs, ccfv_stats *stats, int device,
                 cudaStream_t st, std::string *errmsg);
 // homogeneous: the source term is left out (the linear part of the step,

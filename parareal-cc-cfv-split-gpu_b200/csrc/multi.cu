@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <tuple>
@@ -279,6 +280,21 @@ int MultiEngine::live() const {
   return n;
 }
 
+// Host-side fault injection for tests: with CCFV_INJECT_ALLOC_FAIL=k in the
+// environment, the k-th problem allocation of every engine reports an
+// allocation failure instead of allocating (nothing reaches the device).
+static bool inject_alloc_failure(long long nth) {
+  const char *e = std::getenv("CCFV_INJECT_ALLOC_FAIL");
+  if (!e || !*e) return false;
+  const long long k = std::atoll(e);
+  return k > 0 && nth == k;
+}
+
+static bool autotune_enabled() {
+  const char *e = std::getenv("CCFV_AUTOTUNE");
+  return !(e && e[0] == '0');
+}
+
 int MultiEngine::add(const ccfv_problem &pr, int *slot) {
   auto P = std::make_unique<Problem>();
   std::string e;
@@ -295,6 +311,19 @@ int MultiEngine::add(const ccfv_problem &pr, int *slot) {
                           t < 2 ? 0.5 : th);
     if (!P->tab[t]) return fail(rc, P->ctx->last_error);
   }
+  // line-tile shape: the filter kernel's segment length is tuned once per
+  // line-length class and precision (fine FP64 steps, coarse steps in the
+  // coarse precision) on the first problem of the class, before its plans
+  // are built (CCFV_AUTOTUNE=0 keeps the default)
+  if (autotune_enabled()) {
+    const bool fps[2] = {true, P->g64};
+    const double dts[2] = {P->dt, P->dtc};
+    for (int lv = 0; lv < 2; ++lv)
+      if (!class_tuned(P->g.nx, fps[lv]) || !class_tuned(P->g.ny, fps[lv])) {
+        rc = autotune(P->ctx.get(), dts[lv], fps[lv], st_, nullptr, /*for_class=*/true);
+        if (rc) return fail(rc, P->ctx->last_error);
+      }
+  }
   for (int kind = 0; kind < 3; ++kind)
     for (int level = 0; level < 2; ++level) {
       const int dir = kind == 1 ? 1 : 0;
@@ -310,6 +339,8 @@ int MultiEngine::add(const ccfv_problem &pr, int *slot) {
                                             cell_filter_variant(G.variant))}) > 227 * 1024)
         return fail(CCFV_ERR_UNSUPPORTED, "time step too large for the staged halo");
     }
+  if (inject_alloc_failure(++allocs_))
+    return fail(CCFV_ERR_NOMEM, "injected allocation failure (CCFV_INJECT_ALLOC_FAIL)");
   MCK(cudaMallocAsync(&P->mem, P->bytes, st_));
   unsigned char *q = static_cast<unsigned char *>(P->mem);
   auto take = [&](size_t b) {

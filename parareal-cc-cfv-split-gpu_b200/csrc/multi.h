@@ -148,6 +148,7 @@ class MultiEngine {
   std::vector<double> hnorms_;
   std::string err_;
   double ms_ = 0, fine_ms_ = 0;
+  long long allocs_ = 0;  // problem allocations attempted (fault injection counts them)
 };
 
 }  // namespace ccfv
