@@ -194,6 +194,7 @@ void fill_chunk_products(int L, T *tab);
 
 // Counts kernel launches made by the library.
 void count_launch(uint64_t n = 1);
+void uncount_launches(uint64_t n);  // launches recorded into a graph capture
 uint64_t launches();
 
 }  // namespace ccfv

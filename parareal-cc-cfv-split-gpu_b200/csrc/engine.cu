@@ -12,6 +12,7 @@ namespace ccfv {
 
 static std::atomic<uint64_t> g_launches{0};
 void count_launch(uint64_t n) { g_launches += n; }
+void uncount_launches(uint64_t n) { g_launches -= n; }
 uint64_t launches() { return g_launches.load(); }
 
 cudaError_t DevBuf::alloc(size_t b) {

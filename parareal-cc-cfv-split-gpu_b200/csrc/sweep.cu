@@ -85,10 +85,32 @@ __device__ __forceinline__ double edge_foot(const SweepField &f, int e, double t
 // h(ta), h(tb) are computed once per line, and sin^2(pi s) at the edge is
 // shared by both corners, so an edge foot costs three sinpi instead of
 // twelve transcendental calls.  Other fields use edge_foot.
+// sin(pi d), cos(pi d) for the small displacement d of a corner foot: the
+// Taylor series of sin and cos to degree 15 / 16 (remainder below 2e-25 for
+// |pi d| <= 1/4), else the library's sincospi.
+__device__ __forceinline__ void small_sincospi(double d, double *sn, double *cs) {
+  const double x = 3.141592653589793 * d;
+  if (fabs(x) > 0.25) {
+    sincospi(d, sn, cs);
+    return;
+  }
+  const double x2 = x * x;
+  *sn = x * (1.0 + x2 * (-1.0 / 6 + x2 * (1.0 / 120 + x2 * (-1.0 / 5040 + x2 * (1.0 / 362880 +
+             x2 * (-1.0 / 39916800 + x2 * (1.0 / 6227020800.0 - x2 / 1307674368000.0)))))));
+  *cs = 1.0 + x2 * (-0.5 + x2 * (1.0 / 24 + x2 * (-1.0 / 720 + x2 * (1.0 / 40320 +
+             x2 * (-1.0 / 3628800 + x2 * (1.0 / 479001600 - x2 / 87178291200.0))))));
+}
+
 struct LineFeet {
   double tau0, tau1, ta, tb;
   bool swirl;
   double a0a = 0, a0b = 0, a1a = 0, a1b = 0;  // along-line speed factors: corner line, time
+  // optional table of sin(pi s_e), cos(pi s_e) for edges e0 .. (shared by the
+  // lines of a tile): a corner foot then needs only the small-angle
+  // sin/cos of its displacement, sin(pi (s - d)) = sin(pi s) cos(pi d) -
+  // cos(pi s) sin(pi d)
+  const double *tsn = nullptr, *tcs = nullptr;
+  int te0 = 0;
   __device__ __forceinline__ LineFeet(const SweepField &f, double tau0_, double tau1_, double ta_,
                                       double tb_)
       : tau0(tau0_), tau1(tau1_), ta(ta_), tb(tb_), swirl(f.vel == VEL_SWIRL) {
@@ -105,6 +127,17 @@ struct LineFeet {
   __device__ __forceinline__ double foot(const SweepField &f, int e) const {
     if (!swirl) return edge_foot(f, e, tau0, tau1, ta, tb);
     const double s = f.s_min + f.h * e;
+    if (tsn) {
+      const double ss = tsn[e - te0], cs = tcs[e - te0], s2 = ss * ss;
+      const double w0 = a0b * s2, w1 = a1b * s2;  // speed at the corners at tb
+      double sn0, cs0, sn1, cs1;
+      small_sincospi(f.Dt * w0, &sn0, &cs0);
+      small_sincospi(f.Dt * w1, &sn1, &cs1);
+      const double q0 = ss * cs0 - cs * sn0, q1 = ss * cs1 - cs * sn1;
+      const double c0 = s - 0.5 * f.Dt * (w0 + a0a * q0 * q0);
+      const double c1 = s - 0.5 * f.Dt * (w1 + a1a * q1 * q1);
+      return 0.5 * (c0 + c1);
+    }
     const double ss = sinpi(s), s2 = ss * ss;
     const double w0 = a0b * s2, w1 = a1b * s2;  // speed at the corners at tb
     const double q0 = sinpi(s - f.Dt * w0), q1 = sinpi(s - f.Dt * w1);
@@ -330,6 +363,42 @@ __device__ double src_cell(const SweepField &f, int pos, long long gl, double t)
           16.0 * src_f(f, x_i, y_j, t));
 }
 
+// Uniform displacement: every edge foot of a line sits at e - sigma
+// (position units), -sigma = n0 + xi0 from the foot f0 of edge 0.  Remap,
+// foot derivative and RHS then reduce to fixed 6-tap stencils whose weights
+// depend on xi0 only:
+//   remap_k = sum_t w_t C_{k+n0+t},  kb (D_{k+1}-D_k) = sum_t q_t C_{k+n0+t}
+// (t = -2..3; q includes (1-theta) K Dt/h and 1/(12h)), the same PPM integral
+// and cubic derivative weights as the per-cell formulas (T2S4:63-65,
+// 440-547), so the stencil and per-cell paths agree to rounding.
+template <typename T>
+__device__ __forceinline__ void uniform_weights(const SweepField &F, double f0, T w[6], T qd[6],
+                                                int *n0) {
+  const double u = (f0 - F.s_min) / F.h;
+  const double fl = floor(u);
+  *n0 = (int)fl;
+  const double x = u - fl, x2 = x * x, x3 = x2 * x;
+  const double A = x - 2.0 * x2 + x3, B = x3 - x2, Cc = 3.0 * x2 - 2.0 * x3;
+  w[0] = T(A / 12.0);
+  w[1] = T((B - 8.0 * A) / 12.0);
+  w[2] = T(1.0 - Cc - 2.0 * B / 3.0);
+  w[3] = T(Cc + 2.0 * A / 3.0);
+  w[4] = T((8.0 * B - A) / 12.0);
+  w[5] = T(-B / 12.0);
+  const double pm2 = 2.0 * x3 - 6.0 * x2 + 3.0 * x + 1.0;
+  const double pm1 = -8.0 * x3 + 18.0 * x2 + 6.0 * x - 15.0;
+  const double pz = 12.0 * x3 - 18.0 * x2 - 24.0 * x + 15.0;
+  const double pp1 = -8.0 * x3 + 6.0 * x2 + 18.0 * x - 1.0;
+  const double pp2 = 2.0 * x3 - 3.0 * x;
+  const double kq = F.kb * F.inv12h;
+  qd[0] = T(kq * -pm2);
+  qd[1] = T(kq * (pm2 - pm1));
+  qd[2] = T(kq * (pm1 - pz));
+  qd[3] = T(kq * (pz - pp1));
+  qd[4] = T(kq * (pp1 - pp2));
+  qd[5] = T(kq * pp2);
+}
+
 // Shared-memory carve-up of the sweep kernel.
 template <typename T>
 struct Smem {
@@ -508,39 +577,11 @@ __global__ void __launch_bounds__(NTH, 2) sweep_kernel(const SweepField *__restr
     const double ta = toff + F.ta_rel, tb = toff + F.tb_rel;
     const LineFeet lf(F, tau0, tau1, ta, tb);
     const T kbc = T(F.kb);
-    // Uniform displacement: every edge foot of this line sits at e - sigma
-    // (position units), -sigma = n0 + xi0.  Remap, foot derivative and RHS
-    // then reduce to fixed 6-tap stencils with weights depending on xi0 only:
-    //   remap_k = sum_t w_t C_{k+n0+t},  D_{k+1}-D_k = inv12h sum_t q_t C_{k+n0+t}
-    // (t = -2..3), the same PPM integral and cubic derivative weights as the
-    // per-cell formulas, so the fast and per-cell paths agree to rounding.
+    // uniform displacement: shared-foot stencils (uniform_weights)
     int n0 = 0, klo = 1, khi = 0;
     T w[6], qd[6];
     if (stencil) {
-      const double f0 = lf.foot(F, 0);
-      const double u = (f0 - F.s_min) / F.h;
-      const double fl = floor(u);
-      n0 = (int)fl;
-      const double x = u - fl, x2 = x * x, x3 = x2 * x;
-      const double A = x - 2.0 * x2 + x3, B = x3 - x2, Cc = 3.0 * x2 - 2.0 * x3;
-      w[0] = T(A / 12.0);
-      w[1] = T((B - 8.0 * A) / 12.0);
-      w[2] = T(1.0 - Cc - 2.0 * B / 3.0);
-      w[3] = T(Cc + 2.0 * A / 3.0);
-      w[4] = T((8.0 * B - A) / 12.0);
-      w[5] = T(-B / 12.0);
-      const double pm2 = 2.0 * x3 - 6.0 * x2 + 3.0 * x + 1.0;
-      const double pm1 = -8.0 * x3 + 18.0 * x2 + 6.0 * x - 15.0;
-      const double pz = 12.0 * x3 - 18.0 * x2 - 24.0 * x + 15.0;
-      const double pp1 = -8.0 * x3 + 6.0 * x2 + 18.0 * x - 1.0;
-      const double pp2 = 2.0 * x3 - 3.0 * x;
-      const double kq = F.kb * F.inv12h;
-      qd[0] = T(kq * -pm2);
-      qd[1] = T(kq * (pm2 - pm1));
-      qd[2] = T(kq * (pm1 - pz));
-      qd[3] = T(kq * (pz - pp1));
-      qd[4] = T(kq * (pp1 - pp2));
-      qd[5] = T(kq * pp2);
+      uniform_weights<T>(F, lf.foot(F, 0), w, qd, &n0);
       if (periodic) { klo = INT_MIN; khi = INT_MAX; }
       else { klo = 2 - n0; khi = L - 4 - n0; }  // clear of clamps and ghost quirks
     }
@@ -1160,11 +1201,14 @@ __host__ __device__ inline int filter_tile_rows(int lc_max, int H) {
 // Exact (cluster) form: powers (-mu)^e for e = 0 .. FPW - 1 (a segment of at
 // most FLANES * FCH cells needs exponents up to FLANES * FCH).
 constexpr int FPW = FLANES * FCH + 8;
+// Per-cell form: edges kb .. kw of a tile (FLANES * FCH + 3 of them).
+constexpr int FEDGE = FLANES * FCH + 4;
 
 template <typename T>
 struct FiltSmem {
   T *C;      // [filter_tile_rows * PITCH]  input cells, then w, then x
   T *B;      // per-cell form: [filter_tile_rows * PITCH]  b of every position
+  double *tsn, *tcs;  // per-cell form: [FEDGE] sin / cos (pi s_e) of the tile's edges
   T *om;     // [8 * LPG]  weights of w's input (1/c) M b as an 8-tap stencil of C
   T *pwt;    // [32]       (-mu)^(i+1), i = 0 .. FCH-1
   T *pwa;    // exact form: [FPW] (-mu)^e
@@ -1191,6 +1235,14 @@ __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max
   s.C = p;
   s.rows = filter_tile_rows(lc_max, H);
   s.B = CELL ? p + (size_t)s.rows * PITCH : nullptr;
+  s.tsn = nullptr;
+  s.tcs = nullptr;
+  if (CELL) {  // per-CTA edge table of the swirling field (FP64)
+    unsigned char *q = reinterpret_cast<unsigned char *>(s.B + (size_t)s.rows * PITCH);
+    q = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(q) + 7) & ~uintptr_t(7));
+    s.tsn = reinterpret_cast<double *>(q);
+    s.tcs = s.tsn + FEDGE;
+  }
   return s;
 }
 
@@ -1539,6 +1591,9 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
   }
   if (EXACT)
     for (int e = threadIdx.x; e < FPW; e += NTH) S.pwa[e] = T(powi(-F.sm_fac, e));
+  if (CELL && F.vel == VEL_SWIRL && F.bc == BC_PERIODIC)
+    for (int i = threadIdx.x; i < FEDGE; i += NTH)  // edges p0 - J - 1 + i
+      sincospi(F.s_min + F.h * (p0 - J - 1 + i), &S.tsn[i], &S.tcs[i]);
   cp_async_wait_all_committed();
   __syncthreads();
   if (compat) {  // extrapolated ghost cells C_{-2}, C_{-1}, C_L, C_{L+1} (T2S4:275-286)
@@ -1579,10 +1634,15 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
       const int mm = (kw - kb + FLANES - 1) / FLANES;
       const int s0 = kb + c * mm, s1 = min(kw, s0 + mm);
       const double tau0 = F.t_min + F.ht * (double)gl;
-      const LineFeet lf(F, tau0, tau0 + F.ht, toff + F.ta_rel, toff + F.tb_rel);
+      LineFeet lf(F, tau0, tau0 + F.ht, toff + F.ta_rel, toff + F.tb_rel);
       const T *ccol = S.C + ln;
       const T kbc = T(F.kb);
       if (!compat) {
+        if (F.vel == VEL_SWIRL) {  // edge table of this tile (filled with the staging)
+          lf.tsn = S.tsn;
+          lf.tcs = S.tcs;
+          lf.te0 = kb;
+        }
         T *bcol = S.B + ln;
         if (s0 < s1) {
           CellEdge<T> el{0, T(0), T(0)};
@@ -1598,21 +1658,52 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
           }
         }
       } else {
-        // b = 0 outside the line (the compact mass matrix's zero ghosts)
+        // b = 0 outside the line (the compact mass matrix's zero ghosts).
+        // Uniform displacement (the reference's rotation, constant, rotation):
+        // cells clear of the clamps and ghost selections take the
+        // shared-foot stencils, the rest the per-cell formulas of the
+        // reference (remap_cell, foot_derivative); other velocity fields the
+        // per-edge path (compat_edge)
         const int ka = max(s0, 0), kz = min(min(s1, kv), L);
         const LineView<T> vc{S.C + ln, rb, nrows, status};
+        const bool uni = F.uniform != 0;
+        T wr[6], wq[6];
+        int n0 = 0, klo = 1, khi = 0;
+        if (uni) {
+          uniform_weights<T>(F, lf.foot(F, 0), wr, wq, &n0);
+          klo = 2 - n0;
+          khi = L - 4 - n0;
+        }
         if (!F.dsrc) {
           T *bcol = S.B + ln;
-          if (ka < kz) {
-            CompatEdge<T> el = compat_edge<T>(F, lf, vc, vc, ka);
-            for (int k = ka; k < kz; ++k) {
-              const CompatEdge<T> er = compat_edge<T>(F, lf, vc, vc, k + 1);
-              bcol[(k + rb) * PITCH] = compat_remap<T>(F, el, er, vc) + kbc * (er.d - el.d);
-              el = er;
+          if (uni) {
+            for (int k = s0; k < s1; ++k) {
+              T b = T(0);
+              if (k >= ka && k < kz) {
+                if (k >= klo && k <= khi) {
+                  const T *cp = S.C + (k + n0 - 2 + rb) * PITCH + ln;
+#pragma unroll
+                  for (int t = 0; t < 6; ++t) b += (wr[t] + wq[t]) * cp[t * PITCH];
+                } else {
+                  const double fa = lf.foot(F, k), fb = lf.foot(F, k + 1);
+                  b = remap_cell(F, vc, fa, fb) +
+                      kbc * (foot_derivative(F, vc, fb) - foot_derivative(F, vc, fa));
+                }
+              }
+              bcol[(k + rb) * PITCH] = b;
             }
+          } else {
+            if (ka < kz) {
+              CompatEdge<T> el = compat_edge<T>(F, lf, vc, vc, ka);
+              for (int k = ka; k < kz; ++k) {
+                const CompatEdge<T> er = compat_edge<T>(F, lf, vc, vc, k + 1);
+                bcol[(k + rb) * PITCH] = compat_remap<T>(F, el, er, vc) + kbc * (er.d - el.d);
+                el = er;
+              }
+            }
+            for (int k = s0; k < s1; ++k)
+              if (k < ka || k >= kz) bcol[(k + rb) * PITCH] = T(0);
           }
-          for (int k = s0; k < s1; ++k)
-            if (k < ka || k >= kz) bcol[(k + rb) * PITCH] = T(0);
         } else {
           // the reference's third sweep differentiates the remapped field
           // (dcdx_bar_on_gpu(v_d_Cnphf_bar_x, ...), T2S4:929-932): remap the
@@ -1623,7 +1714,19 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
           const int m1 = (ra1 - ra0 + FLANES - 1) / FLANES;
           const int q0 = ra0 + c * m1, q1 = min(ra1, q0 + m1);
           T *rcol = S.B + ln;
-          if (q0 < q1) {
+          if (uni) {
+            for (int k = q0; k < q1; ++k) {
+              T r = T(0);
+              if (k >= klo && k <= khi) {
+                const T *cp = S.C + (k + n0 - 2 + rb) * PITCH + ln;
+#pragma unroll
+                for (int t = 0; t < 6; ++t) r += wr[t] * cp[t * PITCH];
+              } else {
+                r = remap_cell(F, vc, lf.foot(F, k), lf.foot(F, k + 1));
+              }
+              rcol[(k + rb) * PITCH] = r;
+            }
+          } else if (q0 < q1) {
             CompatEdge<T> el = compat_edge<T>(F, lf, vc, vc, q0);
             for (int k = q0; k < q1; ++k) {
               const CompatEdge<T> er = compat_edge<T>(F, lf, vc, vc, k + 1);
@@ -1636,16 +1739,22 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
           __syncwarp(fm);
           const LineView<T> vr{rcol, rb, nrows, status};
           T *bcol = S.C + ln;
-          if (ka < kz) {
-            T dl = foot_derivative(F, vr, lf.foot(F, ka));
-            for (int k = ka; k < kz; ++k) {
-              const T dr = foot_derivative(F, vr, lf.foot(F, k + 1));
-              bcol[(k + rb) * PITCH] = vr(k) + kbc * (dr - dl);
-              dl = dr;
+          for (int k = s0; k < s1; ++k) {
+            T b = T(0);
+            if (k >= ka && k < kz) {
+              if (uni && k >= klo && k <= khi) {
+                const T *rp = rcol + (k + n0 - 2 + rb) * PITCH;
+                T acc = T(0);
+#pragma unroll
+                for (int t = 0; t < 6; ++t) acc += wq[t] * rp[t * PITCH];
+                b = rcol[(k + rb) * PITCH] + acc;
+              } else {
+                const double fa = lf.foot(F, k), fb = lf.foot(F, k + 1);
+                b = vr(k) + kbc * (foot_derivative(F, vr, fb) - foot_derivative(F, vr, fa));
+              }
             }
+            bcol[(k + rb) * PITCH] = b;
           }
-          for (int k = s0; k < s1; ++k)
-            if (k < ka || k >= kz) bcol[(k + rb) * PITCH] = T(0);
         }
       }
       __syncwarp(fm);
@@ -1912,7 +2021,8 @@ size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact, bool
   size_t el = fp64 ? 8 : 4;
   return FD_BYTES + 64 * sizeof(int) +
          (8 * (size_t)LPG + 32 + (exact ? (size_t)FPW + 2 * LPG : 0) +
-          (cell ? 2 : 1) * (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el;
+          (cell ? 2 : 1) * (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el +
+         (cell ? 8 + 2 * sizeof(double) * (size_t)FEDGE : 0);
 }
 
 int filter_segment_max(int J) { return filter_seg_max(J); }
