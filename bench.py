@@ -67,6 +67,11 @@ def parse():
                          "also on one GPU")
     ap.add_argument("--inner", type=int, default=16,
                     help="step mode: fine steps per timed step")
+    ap.add_argument("--vel", default="rotation", choices=["rotation", "swirl", "compat"],
+                    help="step mode: the workload's rotation field, the swirling deformation "
+                         "(per-cell feet), or the reference's own setting (compat boundaries)")
+    ap.add_argument("--noalloc", action="store_true",
+                    help="step mode: through the allocation-free entry point")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--serve-nmax", type=int, default=1024,
@@ -873,15 +878,42 @@ def run_step(a, w, ws, rank, local):
     dev = torch.device("cuda", local)
     N, nt = w["N"], w["nt"]
     dt = w["T"] / nt
-    grid = ccfv.make_grid(N, bc=ccfv.BC_PERIODIC, velocity=ccfv.VEL_ROTATION,
-                          vel_params=(w["omega"], *w["center"]), K=w["nu"],
-                          scheme=ccfv.SCHEME_CONSISTENT)
+    t0 = 0.0
+    if a.vel == "swirl":  # swirling deformation (T = 1.5), fine dt at CFL 0.8
+        grid = ccfv.make_grid(N, bc=ccfv.BC_PERIODIC, velocity=ccfv.VEL_SWIRL,
+                              vel_params=(1.5,), K=w["nu"], scheme=ccfv.SCHEME_CONSISTENT)
+        dt, t0 = 0.8 / N, 0.2
+        desc = f"periodic {N}^2 swirling-deformation field, nu={w['nu']}, dt=0.8/N"
+    elif a.vel == "compat":  # the reference's domain, velocity, boundaries and scheme
+        grid = ccfv.make_grid(N, K=w["nu"])
+        dt = 0.8 * (2.0 / N) / 4.0
+        desc = (f"{N}^2 field on the reference's domain [-1,1]^2, velocity (-4y, 4x), "
+                f"compat boundaries, reference scheme, K={w['nu']}, dt at CFL 0.8")
+    else:
+        grid = ccfv.make_grid(N, bc=ccfv.BC_PERIODIC, velocity=ccfv.VEL_ROTATION,
+                              vel_params=(w["omega"], *w["center"]), K=w["nu"],
+                              scheme=ccfv.SCHEME_CONSISTENT)
+        desc = f"periodic {N}^2 rotation field, nu={w['nu']}, dt=T/{nt}"
     solver = ccfv.Solver(grid, local)
     C = initial_field(w, solver, dev)
     n = a.inner
     stream = torch.cuda.current_stream()
+
+    def advance(field, t):
+        if a.noalloc:  # the allocation-free entry point (its scan kernels)
+            import ctypes
+            sp = ctypes.c_void_p(stream.cuda_stream)
+            for k in range(n):
+                rc = ccfv.lib().ccfv_step_noalloc(ctypes.byref(grid),
+                                                  ctypes.c_void_p(field.data_ptr()),
+                                                  t + k * dt, dt, sp)
+                if rc:
+                    raise ccfv.CcfvError(rc, "ccfv_step_noalloc")
+        else:
+            solver.run(field, t, dt, n)
+
     for i in range(a.warmup):
-        solver.run(C, i * n * dt, dt, n)
+        advance(C, t0 + i * n * dt)
     solver.check()
     torch.cuda.synchronize()
     barrier(ws)
@@ -891,7 +923,7 @@ def run_step(a, w, ws, rank, local):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for i in range(a.steps):
-        solver.run(C, i * n * dt, dt, n)
+        advance(C, t0 + i * n * dt)
     ev1.record(stream)
     torch.cuda.synchronize()
     launches = ccfv.kernel_launches() - l0
@@ -923,15 +955,16 @@ def run_step(a, w, ws, rank, local):
             n_gpus=ws, steps=a.steps, warmup=a.warmup, ms_per_step=ms / a.steps,
             higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
             data="synthetic",
-            config={"workload": f"serial fine split steps of the periodic {N}^2 rotation "
-                                f"field, nu={w['nu']}, dt=T/{nt}, {n} steps per timed step",
+            config={"workload": f"serial fine split steps of the {desc}, {n} steps per timed "
+                                "step" + (" (ccfv_step_noalloc)" if a.noalloc else ""),
                     "l2_flush": f"field {N * N * 8 / 1e6:.0f} MB per sweep (read + write "
                                 "stream; L2 not flushed)"},
             e2e={"value": ws * cells / e_s, "unit": "cell-updates/s",
                  "h2d_bytes_per_step": 8 * N * N, "d2h_bytes_per_step": 8 * N * N},
             roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                       "frac": achieved / peak, "traffic": tpc * N * N if tpc else None,
-                      "kernel": solver.variant_names(dt),
+                      "kernel": ("sweep_kernel / sweep_fast_kernel (ccfv_step_noalloc)"
+                                 if a.noalloc else solver.variant_names(dt)),
                       "bytes_per_launch": 16 * N * N, "avg_launch_us": ms * 1e3 / sweeps,
                       "peak_source": peak_kind},
             cpu_baseline=cpu, clocks=ck, gpu_launches=launches)))

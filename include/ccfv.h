@@ -346,11 +346,12 @@ int ccfv_autotune(ccfv_ctx *ctx, double dt, int precision, int *segment, void *s
  * periodic closure taken exactly across a line's segments: strong
  * diffusion), CCFV_SWEEP_CELL / CCFV_SWEEP_CELL_EXACT (the two factored forms
  * with a per-cell right-hand side: velocity fields whose feet differ from
- * edge to edge); segment[s] = cells per CTA along a line (either may be
- * NULL).  No device work. */
+ * edge to edge), CCFV_SWEEP_CELL_COMPAT (the factored solve of the
+ * reference's non-cyclic system with its boundaries); segment[s] = cells per
+ * CTA along a line (either may be NULL).  No device work. */
 enum { CCFV_SWEEP_GENERAL = 0, CCFV_SWEEP_UNIFORM = 1, CCFV_SWEEP_FILTER = 2,
        CCFV_SWEEP_SOURCE = 3, CCFV_SWEEP_FILTER_EXACT = 4, CCFV_SWEEP_CELL = 5,
-       CCFV_SWEEP_CELL_EXACT = 6 };
+       CCFV_SWEEP_CELL_EXACT = 6, CCFV_SWEEP_CELL_COMPAT = 7 };
 int ccfv_sweep_plan(ccfv_ctx *ctx, double dt, int precision, int variant[3], int segment[3]);
 
 /* ---- library info ---------------------------------------------------- */

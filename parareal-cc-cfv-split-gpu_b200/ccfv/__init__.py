@@ -296,7 +296,7 @@ class Solver:
         return seg.value
 
     SWEEP_NAMES = ("general", "uniform", "filter", "source", "filter_exact", "cell",
-                   "cell_exact")
+                   "cell_exact", "cell_compat")
 
     def sweep_plan(self, dt, precision=FP64):
         """Kernel variant and segment length of the three sub-steps of a step
@@ -308,7 +308,7 @@ class Solver:
     SWEEP_KERNELS = {"general": "sweep_kernel", "uniform": "sweep_fast_kernel",
                      "filter": "sweep_filter_kernel", "source": "sweep_kernel",
                      "filter_exact": "sweep_filter_kernel", "cell": "sweep_filter_kernel",
-                     "cell_exact": "sweep_filter_kernel"}
+                     "cell_exact": "sweep_filter_kernel", "cell_compat": "sweep_filter_kernel"}
 
     def variant_names(self, dt, precision=FP64):
         """Names of the sweep kernels a step of dt launches (x, y, x)."""

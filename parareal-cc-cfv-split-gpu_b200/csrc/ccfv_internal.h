@@ -119,18 +119,27 @@ constexpr size_t FD_BYTES = (sizeof(SweepField) + 63) & ~size_t(63);
 // SWEEP_FILTER_EXACT the filter kernel's cluster form (any diffusion number,
 // out of place).
 // SWEEP_CELL / SWEEP_CELL_EXACT: the filter kernel's two forms with a
-// per-cell right-hand side (feet that differ from edge to edge).
+// per-cell right-hand side (feet that differ from edge to edge);
+// SWEEP_CELL_COMPAT: the per-cell form with the reference's boundaries
+// (non-cyclic system).
 enum { SWEEP_GENERAL = 0, SWEEP_FAST = 1, SWEEP_FILTER = 2, SWEEP_GENERAL_SRC = 3,
-       SWEEP_FILTER_EXACT = 4, SWEEP_CELL = 5, SWEEP_CELL_EXACT = 6 };
-// Variants run by the filter kernel (factored cyclic solve).
+       SWEEP_FILTER_EXACT = 4, SWEEP_CELL = 5, SWEEP_CELL_EXACT = 6, SWEEP_CELL_COMPAT = 7 };
+// Variants run by the filter kernel (factored solve).
 inline bool filter_variant(int v) {
   return v == SWEEP_FILTER || v == SWEEP_FILTER_EXACT || v == SWEEP_CELL ||
-         v == SWEEP_CELL_EXACT;
+         v == SWEEP_CELL_EXACT || v == SWEEP_CELL_COMPAT;
+}
+// Warm-up (segmented) forms: lines longer than MAX_CLUSTER segments are
+// allowed out of place.
+inline bool warm_filter_variant(int v) {
+  return v == SWEEP_FILTER || v == SWEEP_CELL || v == SWEEP_CELL_COMPAT;
 }
 // Variants whose right-hand side is the per-line stencil table (SweepField::wt).
 inline bool stencil_filter_variant(int v) { return v == SWEEP_FILTER || v == SWEEP_FILTER_EXACT; }
 // Variants with the per-cell right-hand side.
-inline bool cell_filter_variant(int v) { return v == SWEEP_CELL || v == SWEEP_CELL_EXACT; }
+inline bool cell_filter_variant(int v) {
+  return v == SWEEP_CELL || v == SWEEP_CELL_EXACT || v == SWEEP_CELL_COMPAT;
+}
 // The filter kernel's cluster form (exact periodic closure, out of place).
 inline bool exact_filter_variant(int v) { return v == SWEEP_FILTER_EXACT || v == SWEEP_CELL_EXACT; }
 constexpr int FILTER_JMAX = 64;  // longest recurrence warm-up of the filter kernel
@@ -194,7 +203,6 @@ void fill_chunk_products(int L, T *tab);
 
 // Counts kernel launches made by the library.
 void count_launch(uint64_t n = 1);
-void uncount_launches(uint64_t n);  // launches recorded into a graph capture
 uint64_t launches();
 
 }  // namespace ccfv

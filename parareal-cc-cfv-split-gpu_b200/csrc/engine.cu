@@ -12,7 +12,6 @@ namespace ccfv {
 
 static std::atomic<uint64_t> g_launches{0};
 void count_launch(uint64_t n) { g_launches += n; }
-void uncount_launches(uint64_t n) { g_launches -= n; }
 uint64_t launches() { return g_launches.load(); }
 
 cudaError_t DevBuf::alloc(size_t b) {
@@ -354,12 +353,12 @@ LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64
     int J = 0;
     const bool jok = filter_params(g, dir, Dt, fp64, nullptr, nullptr, &J, theta) && L > 2 * J;
     if (L <= filter_segment_max(0)) {
-      G.variant = SWEEP_CELL;
+      G.variant = SWEEP_CELL_COMPAT;
       G.cs = 1;
       G.lc_max = L;
       G.halo = extra;
     } else if (jok) {
-      G.variant = SWEEP_CELL;
+      G.variant = SWEEP_CELL_COMPAT;
       G.halo = J + extra;
       const int lc = std::min(filter_segment_max(J),
                               std::max({32, (L + MAX_CLUSTER - 1) / MAX_CLUSTER,
@@ -368,7 +367,7 @@ LaunchGeom step_geom(const ccfv_grid &g, int dir, double Dt, int dsrc, bool fp64
       G.lc_max = (L + G.cs - 1) / G.cs;
       if (inplace && G.cs > MAX_CLUSTER) G = general;
     }
-    if (G.variant == SWEEP_CELL &&
+    if (G.variant == SWEEP_CELL_COMPAT &&
         sweep_filter_smem_bytes(G.lc_max, G.halo, fp64, false, true) > 227 * 1024)
       G = general;
   }
@@ -403,8 +402,8 @@ int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen, 
     g_lc_override = lc;
     StepPlan plan;
     int rc = build_step_plan(ctx, &plan, dt, fp64, pf);
-    if (rc == CCFV_OK && plan.geom[0].variant != SWEEP_FILTER && plan.geom[1].variant != SWEEP_FILTER &&
-        plan.geom[0].variant != SWEEP_CELL && plan.geom[1].variant != SWEEP_CELL) {
+    if (rc == CCFV_OK && !warm_filter_variant(plan.geom[0].variant) &&
+        !warm_filter_variant(plan.geom[1].variant)) {
       g_lc_override = 0;
       break;  // nothing to tune: this grid does not use the filter kernel
     }
@@ -496,8 +495,7 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
     const bool plan_pp = !fields.empty() && fields[0].B != nullptr;
     LaunchGeom G = step_geom(g, dir, Dt, dsrc, fp64, !plan_pp, theta);
     if (ctx->force_general && G.variant != SWEEP_GENERAL_SRC) G.variant = SWEEP_GENERAL;
-    if (G.cs > MAX_CLUSTER &&
-        !((G.variant == SWEEP_FILTER || G.variant == SWEEP_CELL) && plan_pp))
+    if (G.cs > MAX_CLUSTER && !(warm_filter_variant(G.variant) && plan_pp))
       return set_error(ctx, CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
     if (std::max({sweep_smem_bytes(G.lc_max, G.halo, fp64, g.source != 0),
                   sweep_fast_smem_bytes(G.lc_max, G.halo, fp64),

@@ -266,19 +266,8 @@ int problem_setup(Problem &P, const ccfv_problem &p, std::string *err) {
                   std::string(#call) + ": " + cudaGetErrorString(e_));                 \
   } while (0)
 
-void MultiEngine::drop_graphs() {
-  if (gF_) cudaGraphExecDestroy(gF_);
-  if (gG_) cudaGraphExecDestroy(gG_);
-  gF_ = gG_ = nullptr;
-}
-
 MultiEngine::~MultiEngine() {
   cudaSetDevice(device_);
-  drop_graphs();
-  if (gst_) {
-    cudaStreamSynchronize(gst_);
-    cudaStreamDestroy(gst_);
-  }
   cudaStreamSynchronize(st_);
   for (auto &p : slots_)
     if (p && p->mem) cudaFreeAsync(p->mem, st_);
@@ -342,7 +331,7 @@ int MultiEngine::add(const ccfv_problem &pr, int *slot) {
       const int dsrc = (kind == 2 && P->g.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
       const LaunchGeom G = step_geom(P->g, dir, Dt, dsrc, level == 0 || P->g64, false,
                                      level == 0 ? 0.5 : th);
-      if (G.variant != SWEEP_FILTER && G.variant != SWEEP_CELL && G.cs > MAX_CLUSTER)
+      if (!warm_filter_variant(G.variant) && G.cs > MAX_CLUSTER)
         return fail(CCFV_ERR_UNSUPPORTED, "line longer than 4096 cells");
       if (std::max({sweep_smem_bytes(G.lc_max, G.halo, true, P->g.source != 0),
                     sweep_fast_smem_bytes(G.lc_max, G.halo, true),
@@ -400,8 +389,6 @@ void MultiEngine::remove(int slot) {
 // Rebuilds the launch classes, element-wise descriptors and norm offsets
 // after problems joined or left.
 int MultiEngine::rebuild() {
-  drop_graphs();  // they hold the old classes, descriptors and buffers
-  stable_ = 0;
   fine_.clear();
   coarse_.clear();
   std::vector<FilterTable *> pending;  // stencil tables not computed yet
@@ -555,7 +542,6 @@ int MultiEngine::push_nlo() {
 
 // Host mirror of batch_elem_kernel's per-instance guard.
 bool MultiEngine::elem_active(int op, int n) const {
-  if (capture_all_) return true;  // graphs: the kernel's own guard decides
   for (size_t i = 0; i < slots_.size(); ++i) {
     const Problem *P = slots_[i].get();
     if (!P || P->state == Problem::DONE) continue;  // zeroed element: S = 0
@@ -590,7 +576,7 @@ int MultiEngine::sweeps(std::map<KKey, SweepClass> &classes, int kind, int jstep
     const int np = (int)(std::partition_point(K.bound.begin(), K.bound.end(),
                                               [&](int b) { return b > jstep; }) -
                          K.bound.begin());
-    bool any = capture_all_;  // the kernel's own guard, evaluated here on the host copy of nlo
+    bool any = false;  // the kernel's own guard, evaluated here on the host copy of nlo
     for (int i = 0; i < np && !any; ++i) any = field_active(K.h[i], jstep, nslice, nlo_.data());
     if (!any) continue;
     bs.g0idx = idxbuf_.as<int>() + K.ioff;
@@ -612,66 +598,10 @@ int MultiEngine::coarse_slice(int s, int mmax) {
   return CCFV_OK;
 }
 
-int MultiEngine::fine_phase(int Jmax) {
-  for (int j = 0; j < Jmax; ++j)
-    for (int kind = 0; kind < 3; ++kind)
-      if (int rc = sweeps(fine_, kind, j, 0)) return rc;
-  return CCFV_OK;
-}
-
-int MultiEngine::coarse_phase(int Smax, int mmax, bool any_std) {
-  for (int s = 0; s < Smax; ++s) {
-    int rc = any_std ? elem(OP_LOAD_W_STD, s) : CCFV_OK;
-    if (!rc) rc = coarse_slice(s, mmax);
-    if (!rc) rc = elem(OP_CORRECT, s);
-    if (rc) return rc;
-  }
-  return CCFV_OK;
-}
-
-// Captures the F phase (fine) or the G phase of an iteration over every
-// placed problem into an executable graph on the engine's own stream.  The
-// launches are those of the host-skipping path without the skipping: the
-// kernels' guards (nlo, step and slice bounds) leave out what is inactive,
-// so one graph serves every later iteration with the same problems.
-int MultiEngine::capture(bool fine, cudaGraphExec_t *out, uint64_t *nlaunch) {
-  const cudaStream_t keep = st_;
-  st_ = gst_;
-  capture_all_ = true;
-  const uint64_t l0 = launches();
-  cudaGraph_t g = nullptr;
-  cudaError_t e = cudaStreamBeginCapture(gst_, cudaStreamCaptureModeThreadLocal);
-  int rc = CCFV_OK;
-  if (e == cudaSuccess) {
-    rc = fine ? fine_phase(gJ_) : coarse_phase(gS_, gm_, gstd_);
-    const cudaError_t e2 = cudaStreamEndCapture(gst_, &g);
-    if (e == cudaSuccess) e = e2;
-  }
-  st_ = keep;
-  capture_all_ = false;
-  // the captured launches were counted when recorded; they run (and are
-  // counted) at every replay
-  *nlaunch = launches() - l0;
-  uncount_launches(*nlaunch);
-  if (rc || e != cudaSuccess) {
-    if (g) cudaGraphDestroy(g);
-    cudaGetLastError();
-    return rc ? rc : fail(CCFV_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-  }
-  e = cudaGraphInstantiate(out, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess)
-    return fail(CCFV_ERR_CUDA, std::string("graph instantiation: ") + cudaGetErrorString(e));
-  return CCFV_OK;
-}
-
 int MultiEngine::iterate(std::vector<int> *finished) {
   if (finished) finished->clear();
-  if (dirty_) {
+  if (dirty_)
     if (int rc = rebuild()) return rc;
-  } else {
-    ++stable_;
-  }
   const int n = (int)slots_.size();
   cudaEvent_t e0, ef, ef2, e1;
   MCK(cudaEventCreate(&e0));
@@ -728,36 +658,15 @@ int MultiEngine::iterate(std::vector<int> *finished) {
     if (int rc = push_nlo()) return rc;
     // F[s+1] = F(U[s]): the fine sequences read U[s] in their first sweep
     MCK(cudaEventRecord(ef, st_));
-    if (graphs_ && stable_ >= 1) {
-      // the same problems as in the last iteration: replay the two phases
-      // as graphs (captured over every running problem's bounds; problems
-      // that finish later stay placed and are skipped by their nlo)
-      if (!gst_) MCK(cudaStreamCreateWithFlags(&gst_, cudaStreamNonBlocking));
-      if (!gF_ || !gG_) {
-        gJ_ = gS_ = gm_ = 0;
-        gstd_ = false;
-        for (const auto &p : slots_)
-          if (p && p->state == Problem::RUNNING) {
-            gJ_ = std::max(gJ_, p->J);
-            gS_ = std::max(gS_, p->S);
-            gm_ = std::max(gm_, p->m);
-            gstd_ |= p->o.form == CCFV_FORM_STANDARD;
-          }
-        MCK(cudaStreamSynchronize(st_));
-        if (int rc = capture(true, &gF_, &nF_)) return rc;
-        if (int rc = capture(false, &gG_, &nG_)) return rc;
-      }
-      MCK(cudaStreamWaitEvent(gst_, ef, 0));
-      MCK(cudaGraphLaunch(gF_, gst_));
-      MCK(cudaEventRecord(ef2, gst_));
-      MCK(cudaGraphLaunch(gG_, gst_));
-      count_launch(nF_ + nG_);
-      MCK(cudaEventRecord(e1, gst_));
-      MCK(cudaStreamWaitEvent(st_, e1, 0));
-    } else {
-      if (int rc = fine_phase(Jmax)) return rc;
-      MCK(cudaEventRecord(ef2, st_));
-      if (int rc = coarse_phase(Smax, mmax, any_std)) return rc;
+    for (int j = 0; j < Jmax; ++j)
+      for (int kind = 0; kind < 3; ++kind)
+        if (int rc = sweeps(fine_, kind, j, 0)) return rc;
+    MCK(cudaEventRecord(ef2, st_));
+    for (int s = 0; s < Smax; ++s) {
+      int rc = any_std ? elem(OP_LOAD_W_STD, s) : CCFV_OK;
+      if (!rc) rc = coarse_slice(s, mmax);
+      if (!rc) rc = elem(OP_CORRECT, s);
+      if (rc) return rc;
     }
     MCK(cudaMemcpyAsync(hnorms_.data(), norms_d_.p, sizeof(double) * hnorms_.size(),
                         cudaMemcpyDeviceToHost, st_));
@@ -794,9 +703,7 @@ int MultiEngine::iterate(std::vector<int> *finished) {
     if (P->converged || P->k >= P->o.kmax || P->k >= P->S) {
       // after S iterations Parareal equals the serial fine solve exactly
       P->state = Problem::DONE;
-      // drop it from the launch classes; with graphs it stays placed (its
-      // nlo = S leaves it out on the device) unless the set changes anyway
-      if (!graphs_) dirty_ = true;
+      dirty_ = true;  // drop it from the launch classes
       if (finished) finished->push_back(i);
     }
   }

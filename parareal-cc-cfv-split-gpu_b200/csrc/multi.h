@@ -2,7 +2,6 @@
 // serving loop).
 #pragma once
 
-#include <cstdlib>
 #include <map>
 #include <memory>
 #include <string>
@@ -97,8 +96,6 @@ struct SweepClass {
 class MultiEngine {
  public:
   MultiEngine(int device, cudaStream_t st) : device_(device), st_(st) {
-    const char *g = std::getenv("CCFV_GRAPHS");
-    graphs_ = !(g && g[0] == '0');
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
       uint64_t thr = UINT64_MAX;  // keep released problem states cached in the pool
@@ -106,10 +103,6 @@ class MultiEngine {
     }
   }
   ~MultiEngine();
-  // Whether the F and G phases of an iteration run as two CUDA graphs
-  // (captured once the set of problems has stayed the same for an
-  // iteration; default on, CCFV_GRAPHS=0 turns it off).
-  bool graphs() const { return graphs_; }
   // Admits a problem (allocates its states stream-ordered, uploads C0).
   int add(const ccfv_problem &p, int *slot);
   // Copies the final state of a finished problem into its C_T (stream-ordered).
@@ -136,10 +129,6 @@ class MultiEngine {
   int sweeps(std::map<std::tuple<int, int, int, int, int>, SweepClass> &cls, int kind, int jstep,
              int nslice);
   int coarse_slice(int s, int mmax);
-  int fine_phase(int Jmax);
-  int coarse_phase(int Smax, int mmax, bool any_std);
-  int capture(bool fine, cudaGraphExec_t *out, uint64_t *nlaunch);
-  void drop_graphs();
   int fail(int code, const std::string &msg) {
     err_ = msg;
     return code;
@@ -160,16 +149,6 @@ class MultiEngine {
   std::string err_;
   double ms_ = 0, fine_ms_ = 0;
   long long allocs_ = 0;  // problem allocations attempted (fault injection counts them)
-  // CUDA graphs of the F and G phases (device-side activity: every class
-  // and slice is launched, the kernels skip inactive fields by nlo)
-  bool graphs_ = true;
-  bool capture_all_ = false;   // launching into a capture: no host-side skipping
-  int stable_ = 0;             // iterations since the last rebuild
-  cudaStream_t gst_ = nullptr; // capture / replay stream (the caller's may be the legacy one)
-  cudaGraphExec_t gF_ = nullptr, gG_ = nullptr;
-  uint64_t nF_ = 0, nG_ = 0;   // kernels per replay of each graph
-  int gJ_ = 0, gS_ = 0, gm_ = 0;
-  bool gstd_ = false;
 };
 
 }  // namespace ccfv

@@ -1456,7 +1456,9 @@ __global__ void filter_weights_kernel(const SweepField *__restrict__ f, T *__res
 // half-warp filling its own column; the forward filter then takes w's input
 // as the mass-matrix stencil (1/12c)(b_{k-1} + 10 b_k + b_{k+1}).  Two tiles
 // and the per-edge arithmetic: two CTAs per SM.
-template <typename T, bool EXACT, bool CELL>
+// COMPAT (per-cell form only): the reference's boundaries, a separate
+// instantiation so that the periodic per-cell form carries none of their code.
+template <typename T, bool EXACT, bool CELL, bool COMPAT>
 __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
     sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
                         double toff, void *data_override, int lc_max, int H, unsigned *status,
@@ -1516,7 +1518,7 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
   const bool xsweep = s_line == 1;
   // compat boundaries (per-cell form only): zero outside the line, ghost
   // cells, non-cyclic solve
-  const bool compat = CELL && F.bc == BC_COMPAT;
+  constexpr bool compat = CELL && COMPAT;
 
   // ---- stage rows p0-H .. p1+H-1 (periodic wrap) ----
   if (xsweep) {
@@ -2048,13 +2050,29 @@ size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64) {
 }
 
 template <typename T>
+using FilterKernelT = void (*)(const SweepField *, int, int, double, void *, int, int, unsigned *,
+                               int, int, const int *, int, int, const int *);
+
+// The filter kernel's instantiation of a variant.
+template <typename T>
+static FilterKernelT<T> filter_kernel_for(int variant) {
+  switch (variant) {
+    case SWEEP_FILTER_EXACT: return sweep_filter_kernel<T, true, false, false>;
+    case SWEEP_CELL: return sweep_filter_kernel<T, false, true, false>;
+    case SWEEP_CELL_EXACT: return sweep_filter_kernel<T, true, true, false>;
+    case SWEEP_CELL_COMPAT: return sweep_filter_kernel<T, false, true, true>;
+    default: return sweep_filter_kernel<T, false, false, false>;
+  }
+}
+
+template <typename T>
 static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfields,
                                int group_base, int groups_total, int cs, int lc_max, int halo,
                                double toff, void *data, unsigned *d_status, int jstep,
                                int nslice, const int *nlo, bool inplace, cudaStream_t stream,
                                const int *g0idx) {
   const bool fast = (variant == SWEEP_FAST);
-  const bool cell = (variant == SWEEP_CELL) || (variant == SWEEP_CELL_EXACT);
+  const bool cell = cell_filter_variant(variant);
   const bool exact = exact_filter_variant(variant);
   const bool filt = filter_variant(variant);
   const bool src = (variant == SWEEP_GENERAL_SRC);
@@ -2077,10 +2095,11 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
       if (!configured[dev].load(std::memory_order_relaxed)) {
         for (const void *fn :
              {(const void *)sweep_kernel<T>, (const void *)sweep_fast_kernel<T>,
-              (const void *)sweep_filter_kernel<T, false, false>,
-              (const void *)sweep_filter_kernel<T, true, false>,
-              (const void *)sweep_filter_kernel<T, false, true>,
-              (const void *)sweep_filter_kernel<T, true, true>}) {
+              (const void *)filter_kernel_for<T>(SWEEP_FILTER),
+              (const void *)filter_kernel_for<T>(SWEEP_FILTER_EXACT),
+              (const void *)filter_kernel_for<T>(SWEEP_CELL),
+              (const void *)filter_kernel_for<T>(SWEEP_CELL_EXACT),
+              (const void *)filter_kernel_for<T>(SWEEP_CELL_COMPAT)}) {
           err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      227 * 1024);
           if (err != cudaSuccess) return err;
@@ -2093,18 +2112,6 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   }
   if (groups_total <= 0) return cudaSuccess;
   if (exact && inplace) return cudaErrorInvalidValue;  // the exact form sweeps out of place
-  if (filt && !exact && (cs == 1 || !inplace)) {  // whole lines per CTA, or out of place: no cluster
-    count_launch();
-    if (cell)
-      sweep_filter_kernel<T, false, true><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
-          d_fields, nfields, group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
-          nlo, cs, 0, g0idx);
-    else
-      sweep_filter_kernel<T, false, false><<<(unsigned)(groups_total * cs), NTH, smem, stream>>>(
-          d_fields, nfields, group_base * cs, toff, data, lc_max, halo, d_status, jstep, nslice,
-          nlo, cs, 0, g0idx);
-    return cudaGetLastError();
-  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(groups_total * cs), 1, 1);
   cfg.blockDim = dim3(NTH, 1, 1);
@@ -2118,20 +2125,16 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   count_launch();
-  if (exact)  // one cluster per tile: the cs segments of its lines
-    return cell ? cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T, true, true>, d_fields, nfields,
-                                     group_base * cs, toff, data, lc_max, halo, d_status, jstep,
-                                     nslice, nlo, cs, 0, g0idx)
-                : cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T, true, false>, d_fields,
-                                     nfields, group_base * cs, toff, data, lc_max, halo,
-                                     d_status, jstep, nslice, nlo, cs, 0, g0idx);
-  if (filt)  // group_base in CTAs
-    return cell ? cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T, false, true>, d_fields,
-                                     nfields, group_base * cs, toff, data, lc_max, halo,
-                                     d_status, jstep, nslice, nlo, cs, 1, g0idx)
-                : cudaLaunchKernelEx(&cfg, sweep_filter_kernel<T, false, false>, d_fields,
-                                     nfields, group_base * cs, toff, data, lc_max, halo,
-                                     d_status, jstep, nslice, nlo, cs, 1, g0idx);
+  if (filt) {
+    // whole lines per CTA, or out of place: no cluster (exact form: one
+    // cluster per tile, the cs segments of its lines)
+    int clustered = 0;
+    if (!exact && (cs == 1 || !inplace)) cfg.numAttrs = 0;
+    else if (!exact) clustered = 1;
+    FilterKernelT<T> fn = filter_kernel_for<T>(variant);
+    return cudaLaunchKernelEx(&cfg, fn, d_fields, nfields, group_base * cs, toff, data, lc_max,
+                              halo, d_status, jstep, nslice, nlo, cs, clustered, g0idx);
+  }
   if (fast)
     return cudaLaunchKernelEx(&cfg, sweep_fast_kernel<T>, d_fields, nfields, group_base, toff,
                               data, lc_max, halo, d_status, jstep, nslice, nlo, g0idx);
