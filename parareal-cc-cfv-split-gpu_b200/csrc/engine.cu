@@ -384,13 +384,21 @@ int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen, 
     CK(ctx->status.alloc(sizeof(unsigned) * 4));
     CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(unsigned) * 4, st));
   }
-  CK(ctx->io.alloc(2 * el * NN));
-  CK(cudaMemsetAsync(ctx->io.p, 0, 2 * el * NN, st));
-  // timed as the Parareal engines run it: out of place over a buffer pair
-  std::vector<PlanField> pf(1);
-  pf[0].A = ctx->io.p;
-  pf[0].B = static_cast<unsigned char *>(ctx->io.p) + el * NN;
-  pf[0].in0 = ctx->io.p;
+  // timed as the Parareal engines run it: out of place over buffer pairs.
+  // For a line-length class (the batched engine) the launch holds copies of
+  // the field up to about 2^24 cells, so the timing is that of a launch that
+  // fills the GPU, as the batched launches do (a lone small field favours
+  // short segments, whose warm-up costs more once the GPU is full).
+  const size_t nf = for_class ? std::max<size_t>(1, ((size_t)1 << 24) / NN) : 1;
+  CK(ctx->io.alloc(2 * el * NN * nf));
+  CK(cudaMemsetAsync(ctx->io.p, 0, 2 * el * NN * nf, st));
+  std::vector<PlanField> pf(nf);
+  for (size_t i = 0; i < nf; ++i) {
+    unsigned char *base = static_cast<unsigned char *>(ctx->io.p) + 2 * el * NN * i;
+    pf[i].A = base;
+    pf[i].B = base + el * NN;
+    pf[i].in0 = base;
+  }
   static const int cand[] = {64, 96, 128, 192, 256, 384, 512};
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
@@ -407,11 +415,11 @@ int autotune(ccfv_ctx *ctx, double dt, bool fp64, cudaStream_t st, int *chosen, 
       g_lc_override = 0;
       break;  // nothing to tune: this grid does not use the filter kernel
     }
-    if (rc == CCFV_OK) rc = run_step_plan(ctx, plan, fp64, 0, 1, 0.0, nullptr, st, 0);  // warm-up
+    if (rc == CCFV_OK) rc = run_step_plan(ctx, plan, fp64, 0, (int)nf, 0.0, nullptr, st, 0);
     if (rc == CCFV_OK) {
       cudaEventRecord(a, st);
       for (int r = 0; r < 5 && rc == CCFV_OK; ++r)
-        rc = run_step_plan(ctx, plan, fp64, 0, 1, 0.0, nullptr, st, r);
+        rc = run_step_plan(ctx, plan, fp64, 0, (int)nf, 0.0, nullptr, st, r);
       cudaEventRecord(b, st);
       cudaEventSynchronize(b);
       float ms = 0;

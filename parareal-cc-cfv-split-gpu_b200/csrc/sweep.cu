@@ -85,32 +85,10 @@ __device__ __forceinline__ double edge_foot(const SweepField &f, int e, double t
 // h(ta), h(tb) are computed once per line, and sin^2(pi s) at the edge is
 // shared by both corners, so an edge foot costs three sinpi instead of
 // twelve transcendental calls.  Other fields use edge_foot.
-// sin(pi d), cos(pi d) for the small displacement d of a corner foot: the
-// Taylor series of sin and cos to degree 15 / 16 (remainder below 2e-25 for
-// |pi d| <= 1/4), else the library's sincospi.
-__device__ __forceinline__ void small_sincospi(double d, double *sn, double *cs) {
-  const double x = 3.141592653589793 * d;
-  if (fabs(x) > 0.25) {
-    sincospi(d, sn, cs);
-    return;
-  }
-  const double x2 = x * x;
-  *sn = x * (1.0 + x2 * (-1.0 / 6 + x2 * (1.0 / 120 + x2 * (-1.0 / 5040 + x2 * (1.0 / 362880 +
-             x2 * (-1.0 / 39916800 + x2 * (1.0 / 6227020800.0 - x2 / 1307674368000.0)))))));
-  *cs = 1.0 + x2 * (-0.5 + x2 * (1.0 / 24 + x2 * (-1.0 / 720 + x2 * (1.0 / 40320 +
-             x2 * (-1.0 / 3628800 + x2 * (1.0 / 479001600 - x2 / 87178291200.0))))));
-}
-
 struct LineFeet {
   double tau0, tau1, ta, tb;
   bool swirl;
   double a0a = 0, a0b = 0, a1a = 0, a1b = 0;  // along-line speed factors: corner line, time
-  // optional table of sin(pi s_e), cos(pi s_e) for edges e0 .. (shared by the
-  // lines of a tile): a corner foot then needs only the small-angle
-  // sin/cos of its displacement, sin(pi (s - d)) = sin(pi s) cos(pi d) -
-  // cos(pi s) sin(pi d)
-  const double *tsn = nullptr, *tcs = nullptr;
-  int te0 = 0;
   __device__ __forceinline__ LineFeet(const SweepField &f, double tau0_, double tau1_, double ta_,
                                       double tb_)
       : tau0(tau0_), tau1(tau1_), ta(ta_), tb(tb_), swirl(f.vel == VEL_SWIRL) {
@@ -127,17 +105,6 @@ struct LineFeet {
   __device__ __forceinline__ double foot(const SweepField &f, int e) const {
     if (!swirl) return edge_foot(f, e, tau0, tau1, ta, tb);
     const double s = f.s_min + f.h * e;
-    if (tsn) {
-      const double ss = tsn[e - te0], cs = tcs[e - te0], s2 = ss * ss;
-      const double w0 = a0b * s2, w1 = a1b * s2;  // speed at the corners at tb
-      double sn0, cs0, sn1, cs1;
-      small_sincospi(f.Dt * w0, &sn0, &cs0);
-      small_sincospi(f.Dt * w1, &sn1, &cs1);
-      const double q0 = ss * cs0 - cs * sn0, q1 = ss * cs1 - cs * sn1;
-      const double c0 = s - 0.5 * f.Dt * (w0 + a0a * q0 * q0);
-      const double c1 = s - 0.5 * f.Dt * (w1 + a1a * q1 * q1);
-      return 0.5 * (c0 + c1);
-    }
     const double ss = sinpi(s), s2 = ss * ss;
     const double w0 = a0b * s2, w1 = a1b * s2;  // speed at the corners at tb
     const double q0 = sinpi(s - f.Dt * w0), q1 = sinpi(s - f.Dt * w1);
@@ -1201,14 +1168,11 @@ __host__ __device__ inline int filter_tile_rows(int lc_max, int H) {
 // Exact (cluster) form: powers (-mu)^e for e = 0 .. FPW - 1 (a segment of at
 // most FLANES * FCH cells needs exponents up to FLANES * FCH).
 constexpr int FPW = FLANES * FCH + 8;
-// Per-cell form: edges kb .. kw of a tile (FLANES * FCH + 3 of them).
-constexpr int FEDGE = FLANES * FCH + 4;
 
 template <typename T>
 struct FiltSmem {
   T *C;      // [filter_tile_rows * PITCH]  input cells, then w, then x
   T *B;      // per-cell form: [filter_tile_rows * PITCH]  b of every position
-  double *tsn, *tcs;  // per-cell form: [FEDGE] sin / cos (pi s_e) of the tile's edges
   T *om;     // [8 * LPG]  weights of w's input (1/c) M b as an 8-tap stencil of C
   T *pwt;    // [32]       (-mu)^(i+1), i = 0 .. FCH-1
   T *pwa;    // exact form: [FPW] (-mu)^e
@@ -1235,14 +1199,6 @@ __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max
   s.C = p;
   s.rows = filter_tile_rows(lc_max, H);
   s.B = CELL ? p + (size_t)s.rows * PITCH : nullptr;
-  s.tsn = nullptr;
-  s.tcs = nullptr;
-  if (CELL) {  // per-CTA edge table of the swirling field (FP64)
-    unsigned char *q = reinterpret_cast<unsigned char *>(s.B + (size_t)s.rows * PITCH);
-    q = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(q) + 7) & ~uintptr_t(7));
-    s.tsn = reinterpret_cast<double *>(q);
-    s.tcs = s.tsn + FEDGE;
-  }
   return s;
 }
 
@@ -1593,9 +1549,6 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
   }
   if (EXACT)
     for (int e = threadIdx.x; e < FPW; e += NTH) S.pwa[e] = T(powi(-F.sm_fac, e));
-  if (CELL && F.vel == VEL_SWIRL && F.bc == BC_PERIODIC)
-    for (int i = threadIdx.x; i < FEDGE; i += NTH)  // edges p0 - J - 1 + i
-      sincospi(F.s_min + F.h * (p0 - J - 1 + i), &S.tsn[i], &S.tcs[i]);
   cp_async_wait_all_committed();
   __syncthreads();
   if (compat) {  // extrapolated ghost cells C_{-2}, C_{-1}, C_L, C_{L+1} (T2S4:275-286)
@@ -1636,15 +1589,10 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
       const int mm = (kw - kb + FLANES - 1) / FLANES;
       const int s0 = kb + c * mm, s1 = min(kw, s0 + mm);
       const double tau0 = F.t_min + F.ht * (double)gl;
-      LineFeet lf(F, tau0, tau0 + F.ht, toff + F.ta_rel, toff + F.tb_rel);
+      const LineFeet lf(F, tau0, tau0 + F.ht, toff + F.ta_rel, toff + F.tb_rel);
       const T *ccol = S.C + ln;
       const T kbc = T(F.kb);
       if (!compat) {
-        if (F.vel == VEL_SWIRL) {  // edge table of this tile (filled with the staging)
-          lf.tsn = S.tsn;
-          lf.tcs = S.tcs;
-          lf.te0 = kb;
-        }
         T *bcol = S.B + ln;
         if (s0 < s1) {
           CellEdge<T> el{0, T(0), T(0)};
@@ -1833,52 +1781,16 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
     // positions of this lane inside the backward range (compat: the zero
     // start is at the line's end, x_L = 0)
     const int nb = (compat ? min(qb, L) : qb) - k1;
+    T e_fwd = T(0);
     if (EXACT) {
       // forward end of the segment from a zero carry (position p1 - 1)
       const int cend = (np - 1) / FCH, iend = (np - 1) - cend * FCH;
-      T e = T(0);
 #pragma unroll
-      for (int i = 0; i < FCH; ++i) e = (c == cend && i == iend) ? v[i] : e;
-      e = __shfl_sync(fm, e, cend, FLANES);
-      if (c == 0) S.ex[ln] = e;
-      cg::this_cluster().sync();
-      // carry into this segment: lane r (< cs) loads segment r's map
-      // w -> (-mu)^np_r w + E_r, one scan composes them left to right, and
-      // the periodic closure of the whole line fixes the first carry
-      T cr;
-      {
-        T sa = T(1), sb = T(0);
-        if (c < cs) {
-          const int a0 = min(L, c * Lc), a1 = min(L, a0 + Lc);
-          sa = S.pwa[a1 - a0];
-          sb = cg::this_cluster().map_shared_rank(S.ex, c)[ln];
-        }
-#pragma unroll
-        for (int dd = 1; dd < FLANES; dd <<= 1) {
-          const T pa = __shfl_up_sync(fm, sa, dd, FLANES);
-          const T pb = __shfl_up_sync(fm, sb, dd, FLANES);
-          if (c >= dd) {
-            sb = sa * pb + sb;
-            sa = sa * pa;
-          }
-        }
-        const T at = __shfl_sync(fm, sa, FLANES - 1, FLANES);  // lanes >= cs: identity
-        const T et = __shfl_sync(fm, sb, FLANES - 1, FLANES);
-        const T ea = __shfl_sync(fm, sa, rank > 0 ? rank - 1 : 0, FLANES);
-        const T eb = __shfl_sync(fm, sb, rank > 0 ? rank - 1 : 0, FLANES);
-        const T c0 = et / (T(1) - at);
-        cr = rank > 0 ? ea * c0 + eb : c0;
-      }
-      T cv = cr * S.pwa[c * FCH];
-#pragma unroll
-      for (int i = 0; i < FCH; ++i) {
-        cv *= mmu;  // cr (-mu)^(c FCH + i + 1)
-        v[i] = (i < nb) ? v[i] + cv : T(0);  // backward input; zero past p1
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < FCH; ++i) v[i] = (i < nb) ? v[i] : T(0);  // zero from qb on
+      for (int i = 0; i < FCH; ++i) e_fwd = (c == cend && i == iend) ? v[i] : e_fwd;
+      e_fwd = __shfl_sync(fm, e_fwd, cend, FLANES);
     }
+#pragma unroll
+    for (int i = 0; i < FCH; ++i) v[i] = (i < nb) ? v[i] : T(0);  // zero from qb on
 
     // backward: x over [k0, qb), zero start at qb
     {
@@ -1907,47 +1819,79 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
       }
     }
     if (EXACT) {
-      // backward start of the segment from a zero carry (position p0)
+      // Both periodic closures after one cluster barrier.  From zero carries
+      // the segment gives w_zs (forward end E) and x_zs (backward start X).
+      // The forward carry cr into the segment adds cr (-mu)^(k-p0+1) to w,
+      // which the (linear) backward filter turns into cr h_k with
+      //   h_k = (-mu)^(k-p0+1) (1 - mu^(2(p1-k))) / (1 - mu^2),
+      // and the backward carry d from the right adds d (-mu)^(p1-k).  So
+      // the segment's backward map is x_start = (-mu)^np x_in + X + cr h_p0.
       const T xs = __shfl_sync(fm, v[0], 0, FLANES);
-      if (c == 0) S.ex[LPG + ln] = xs;
+      if (c == 0) {
+        S.ex[ln] = e_fwd;
+        S.ex[LPG + ln] = xs;
+      }
       cg::this_cluster().sync();
-      // carry from the right: lane r loads segment r's map x_start =
-      // (-mu)^np_r x_in + X_r, one scan composes them right to left
-      T d;
+      const T inv1m = T(1) / (T(1) - mu * mu);
+      T cr, d;
       {
-        T sa = T(1), sb = T(0);
+        // lane r (< cs) loads segment r's E_r and X_r
+        T sa = T(1), sb = T(0), xr = T(0), pr = T(1);
         if (c < cs) {
           const int a0 = min(L, c * Lc), a1 = min(L, a0 + Lc);
-          sa = S.pwa[a1 - a0];
-          sb = cg::this_cluster().map_shared_rank(S.ex, c)[LPG + ln];
+          pr = S.pwa[a1 - a0];
+          sa = pr;
+          const T *rex = cg::this_cluster().map_shared_rank(S.ex, c);
+          sb = rex[ln];
+          xr = rex[LPG + ln];
         }
+        // forward: compose w -> (-mu)^np_r w + E_r left to right, close the
+        // line periodically, carry into every segment
 #pragma unroll
         for (int dd = 1; dd < FLANES; dd <<= 1) {
-          const T pa = __shfl_down_sync(fm, sa, dd, FLANES);
-          const T pb = __shfl_down_sync(fm, sb, dd, FLANES);
-          if (c + dd < FLANES) {
+          const T pa = __shfl_up_sync(fm, sa, dd, FLANES);
+          const T pb = __shfl_up_sync(fm, sb, dd, FLANES);
+          if (c >= dd) {
             sb = sa * pb + sb;
             sa = sa * pa;
           }
         }
-        const T at = __shfl_sync(fm, sa, 0, FLANES);
-        const T xt = __shfl_sync(fm, sb, 0, FLANES);
+        const T at = __shfl_sync(fm, sa, FLANES - 1, FLANES);  // lanes >= cs: identity
+        const T et = __shfl_sync(fm, sb, FLANES - 1, FLANES);
+        const T c0 = et / (T(1) - at);
+        const T ea = __shfl_up_sync(fm, sa, 1, FLANES);
+        const T eb = __shfl_up_sync(fm, sb, 1, FLANES);
+        const T cr_c = c > 0 ? ea * c0 + eb : c0;  // carry into segment c
+        cr = __shfl_sync(fm, cr_c, rank, FLANES);
+        // backward: compose x -> (-mu)^np_r x + X_r + cr_r h_p0 right to left
+        T ba = pr, bb = c < cs ? xr + cr_c * (S.pwa[1] * (T(1) - pr * pr) * inv1m) : T(0);
+#pragma unroll
+        for (int dd = 1; dd < FLANES; dd <<= 1) {
+          const T pa = __shfl_down_sync(fm, ba, dd, FLANES);
+          const T pb = __shfl_down_sync(fm, bb, dd, FLANES);
+          if (c + dd < FLANES) {
+            bb = ba * pb + bb;
+            ba = ba * pa;
+          }
+        }
+        const T at2 = __shfl_sync(fm, ba, 0, FLANES);
+        const T xt = __shfl_sync(fm, bb, 0, FLANES);
         const bool last = rank + 1 >= cs;
-        const T ea = __shfl_sync(fm, sa, last ? 0 : rank + 1, FLANES);
-        const T eb = __shfl_sync(fm, sb, last ? 0 : rank + 1, FLANES);
-        const T x0 = xt / (T(1) - at);
-        d = last ? x0 : ea * x0 + eb;
+        const T da = __shfl_sync(fm, ba, last ? 0 : rank + 1, FLANES);
+        const T db = __shfl_sync(fm, bb, last ? 0 : rank + 1, FLANES);
+        const T x0 = xt / (T(1) - at2);
+        d = last ? x0 : da * x0 + db;
       }
       // this CTA's reads of the cluster's shared memory are done; it waits
       // for the others' before it exits (non-aligned forms: the wait follows
       // the divergent store loops)
       asm volatile("barrier.cluster.arrive;\n" ::: "memory");
-      T dv = d * S.pwa[max(nb - FCH, 0)];
 #pragma unroll
-      for (int i = FCH - 1; i >= 0; --i)
+      for (int i = 0; i < FCH; ++i)
         if (i < nb) {
-          dv *= mmu;  // d (-mu)^(nb - i)
-          v[i] += dv;
+          const T p1k = S.pwa[nb - i];            // (-mu)^(p1-k)
+          const T pk = S.pwa[c * FCH + i + 1];    // (-mu)^(k-p0+1)
+          v[i] += cr * (pk * (T(1) - p1k * p1k) * inv1m) + d * p1k;
         }
     }
     if (compat && p0 == 0) {
@@ -2023,8 +1967,7 @@ size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact, bool
   size_t el = fp64 ? 8 : 4;
   return FD_BYTES + 64 * sizeof(int) +
          (8 * (size_t)LPG + 32 + (exact ? (size_t)FPW + 2 * LPG : 0) +
-          (cell ? 2 : 1) * (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el +
-         (cell ? 8 + 2 * sizeof(double) * (size_t)FEDGE : 0);
+          (cell ? 2 : 1) * (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el;
 }
 
 int filter_segment_max(int J) { return filter_seg_max(J); }
