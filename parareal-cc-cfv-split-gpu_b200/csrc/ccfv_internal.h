@@ -201,6 +201,26 @@ inline size_t table_len(int L) {
 template <typename T>
 void fill_chunk_products(int L, T *tab);
 
+// Resident coarse propagator (coarse.cu): the whole G phase of one
+// delta-form Parareal iteration of an instance whose coarse field fits in one
+// SM's shared memory, one CTA per instance.  f: the instance's coarse sweep
+// descriptors of the iterations (x, y, x; filter-kernel constants filled).
+struct ResidentG {
+  SweepField f[3];
+  const double *F;  // F[0..S] fine results
+  double *U;        // U[0..S] slice states (updated)
+  double *norms;    // [2 (S + 1)]: sum dU^2, sum U^2 of every corrected slice
+  int inst;         // index into the launch's nlo array
+  int S, m, nx, ny, pitch;
+};
+// Dynamic shared memory of the resident kernel for an nx x ny field.
+size_t resident_g_smem_bytes(int nx, int ny, bool fp64, bool cell);
+// Whether an nx x ny coarse field can be resident (lines of at most 272
+// cells, the field in shared memory).
+bool resident_g_fits(int nx, int ny, bool fp64, bool cell);
+cudaError_t launch_resident_g(bool fp64, const ResidentG *d_rg, int n, size_t smem,
+                              const int *nlo, cudaStream_t st);
+
 // Counts kernel launches made by the library.
 void count_launch(uint64_t n = 1);
 uint64_t launches();

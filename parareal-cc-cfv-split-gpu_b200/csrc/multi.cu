@@ -88,6 +88,7 @@ __global__ void __launch_bounds__(BT)
     double *U = b.U + (long long)(n + 1) * b.NN;
     const double *Fv = b.F + (long long)(n + 1) * b.NN;
     double *Go = b.Gold ? b.Gold + (long long)(n + 1) * b.NN : nullptr;
+    if (b.pad) return;  // resident coarse propagator: corrected in its own kernel
     const bool zero_g = (b.form == CCFV_FORM_DELTA && n == lo);  // G(0) = 0
     // G is read from Wres; the new increment goes to W (elementwise, so the
     // two may be the same buffer)
@@ -268,6 +269,12 @@ int problem_setup(Problem &P, const ccfv_problem &p, std::string *err) {
 
 MultiEngine::~MultiEngine() {
   cudaSetDevice(device_);
+  if (side_) {
+    cudaStreamSynchronize(side_);
+    cudaStreamDestroy(side_);
+  }
+  for (cudaEvent_t e : side_ev_)
+    if (e) cudaEventDestroy(e);
   cudaStreamSynchronize(st_);
   for (auto &p : slots_)
     if (p && p->mem) cudaFreeAsync(p->mem, st_);
@@ -415,8 +422,15 @@ int MultiEngine::rebuild() {
     if (!live(P)) continue;
     const ccfv_grid &g = P->g;
     // coarse sequences start in W and end in W2 when 3m is odd
-    he[i] = BElem{P->U, P->F, P->Gold, P->W, ((3 * P->m) & 1) ? P->W2 : P->W, P->NN, P->S,
-                  P->o.form, P->g64 ? 1 : 0, 0, norms_d_.as<double>() + norm_off_[i]};
+    // resident coarse propagator: delta form, periodic, the coarse field in
+    // one SM's shared memory (CCFV_RESIDENT_G=0 keeps every problem in the
+    // shared launches)
+    const char *rge = std::getenv("CCFV_RESIDENT_G");
+    const bool want_rg = !P->prepared && !(rge && rge[0] == '0') &&
+                         P->o.form == CCFV_FORM_DELTA && g.bc == CCFV_BC_PERIODIC &&
+                         resident_g_fits(g.nx, g.ny, P->g64,
+                                         g.velocity == CCFV_VEL_SWIRL);
+    std::vector<PreparedField> rg_prep;  // its iterations' coarse fields, if resident
     for (int kind = 0; kind < 3 && !P->prepared; ++kind) {
       const int dir = kind == 1 ? 1 : 0;
       const int dsrc = (kind == 2 && g.scheme == CCFV_SCHEME_REFERENCE) ? 1 : 0;
@@ -463,7 +477,7 @@ int MultiEngine::rebuild() {
           return f;
         };
         const bool delta_src = g.source != CCFV_SRC_NONE && P->o.form == CCFV_FORM_DELTA;
-        if (P->g64 && !delta_src) {
+        if (P->g64 && !delta_src && !want_rg) {
           prepare_field(P->prep, kind, g, coarse_field(g, P->tab[2 + dir], 0), true, &P->ftab,
                         std::make_tuple(kind, 1, 1));
         } else {
@@ -474,11 +488,24 @@ int MultiEngine::rebuild() {
                         std::make_tuple(kind, 1, 1));
           ccfv_grid gh = g;
           if (P->o.form == CCFV_FORM_DELTA) gh.source = CCFV_SRC_NONE;
-          prepare_field(P->prep, kind, gh, coarse_field(gh, P->tab[2 + dir], 2), P->g64,
-                        &P->ftab, std::make_tuple(kind, 1, P->g64 ? 1 : 0));
+          prepare_field(want_rg ? rg_prep : P->prep, kind, gh, coarse_field(gh, P->tab[2 + dir], 2),
+                        P->g64, &P->ftab, std::make_tuple(kind, 1, P->g64 ? 1 : 0));
         }
       }
     }
+    if (want_rg) {
+      // resident only if every coarse sweep of the iterations runs a filter
+      // form (their constants mu and 1/c are then in the descriptors)
+      bool ok = rg_prep.size() == 3;
+      for (const PreparedField &pf : rg_prep) ok = ok && filter_variant(pf.G.variant);
+      if (ok) {
+        P->resident = true;
+        for (int k = 0; k < 3; ++k) P->rgf[k] = rg_prep[k].f;
+      } else {
+        for (const PreparedField &pf : rg_prep) P->prep.push_back(pf);
+      }
+    }
+    he[i].pad = P->resident ? 1 : 0;
     P->prepared = true;
     for (const PreparedField &pf : P->prep) place_field(pf.level == 0 ? fine_ : coarse_, pf, &pending);
   }
@@ -518,6 +545,37 @@ int MultiEngine::rebuild() {
   const int eb = 148;
   MCK(elems_.alloc(sizeof(BElem) * std::max(n, 1)));
   if (n) MCK(cudaMemcpyAsync(elems_.p, he.data(), sizeof(BElem) * n, cudaMemcpyHostToDevice, st_));
+  {
+    std::vector<ResidentG> hr[2];
+    for (int i = 0; i < n; ++i) {
+      Problem *P = slots_[i].get();
+      if (!live(P) || !P->resident) continue;
+      ResidentG r;
+      std::memset(&r, 0, sizeof(r));
+      for (int k = 0; k < 3; ++k) r.f[k] = P->rgf[k];
+      r.F = P->F;
+      r.U = P->U;
+      r.norms = norms_d_.as<double>() + norm_off_[i];
+      r.inst = i;
+      r.S = P->S;
+      r.m = P->m;
+      r.nx = P->g.nx;
+      r.ny = P->g.ny;
+      r.pitch = P->g.ny | 1;
+      const int q = P->g64 ? 1 : 0;
+      rgsmem_[q] = std::max(rgsmem_[q], resident_g_smem_bytes(P->g.nx, P->g.ny, P->g64,
+                                                              P->g.velocity == CCFV_VEL_SWIRL));
+      hr[q].push_back(r);
+    }
+    for (int q = 0; q < 2; ++q) {
+      rgn_[q] = (int)hr[q].size();
+      if (rgn_[q]) {
+        MCK(rgbuf_[q].alloc(sizeof(ResidentG) * hr[q].size()));
+        MCK(cudaMemcpyAsync(rgbuf_[q].p, hr[q].data(), sizeof(ResidentG) * hr[q].size(),
+                            cudaMemcpyHostToDevice, st_));
+      }
+    }
+  }
   MCK(nlo_d_.alloc(sizeof(int) * std::max(n, 1)));
   MCK(partial_.alloc(sizeof(double) * 2 * eb * (size_t)std::max(n, 1)));
   if (counters_.bytes < sizeof(unsigned) * std::max(n, 1)) {
@@ -546,6 +604,7 @@ bool MultiEngine::elem_active(int op, int n) const {
     const Problem *P = slots_[i].get();
     if (!P || P->state == Problem::DONE) continue;  // zeroed element: S = 0
     if (op == OP_LOAD_W_STD && P->o.form != CCFV_FORM_STANDARD) continue;
+    if (op == OP_CORRECT && P->resident) continue;
     if (n < P->S && n >= nlo_[i]) return true;
   }
   return false;
@@ -637,15 +696,19 @@ int MultiEngine::iterate(std::vector<int> *finished) {
   }
   // one Parareal iteration of every running problem; iteration k+1 leaves
   // slices < k untouched (already exact)
-  int Smax = 0, Jmax = 0, mmax = 0, running = 0;
+  int Smax = 0, Jmax = 0, mmax = 0, running = 0, resident = 0;
   bool any_std = false;
   for (int i = 0; i < n; ++i) {
     Problem *P = slots_[i].get();
     if (P && P->state == Problem::RUNNING) {
       nlo_[i] = P->k;
-      Smax = std::max(Smax, P->S);
+      if (P->resident) {
+        ++resident;
+      } else {
+        Smax = std::max(Smax, P->S);
+        mmax = std::max(mmax, P->m);
+      }
       Jmax = std::max(Jmax, P->J);
-      mmax = std::max(mmax, P->m);
       any_std |= P->o.form == CCFV_FORM_STANDARD;
       ++running;
       P->fine_cu += (double)(P->S - P->k) * P->J * P->NN;
@@ -662,12 +725,27 @@ int MultiEngine::iterate(std::vector<int> *finished) {
       for (int kind = 0; kind < 3; ++kind)
         if (int rc = sweeps(fine_, kind, j, 0)) return rc;
     MCK(cudaEventRecord(ef2, st_));
+    if (resident) {
+      // the resident problems' whole G phases, one CTA each, beside the
+      // shared coarse launches of the others
+      if (!side_) {
+        MCK(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+        MCK(cudaEventCreateWithFlags(&side_ev_[0], cudaEventDisableTiming));
+      }
+      MCK(cudaStreamWaitEvent(side_, ef2, 0));
+      for (int q = 0; q < 2; ++q)
+        if (rgn_[q])
+          MCK(launch_resident_g(q == 1, rgbuf_[q].as<ResidentG>(), rgn_[q], rgsmem_[q],
+                                nlo_d_.as<int>(), side_));
+      MCK(cudaEventRecord(side_ev_[0], side_));
+    }
     for (int s = 0; s < Smax; ++s) {
       int rc = any_std ? elem(OP_LOAD_W_STD, s) : CCFV_OK;
       if (!rc) rc = coarse_slice(s, mmax);
       if (!rc) rc = elem(OP_CORRECT, s);
       if (rc) return rc;
     }
+    if (resident) MCK(cudaStreamWaitEvent(st_, side_ev_[0], 0));
     MCK(cudaMemcpyAsync(hnorms_.data(), norms_d_.p, sizeof(double) * hnorms_.size(),
                         cudaMemcpyDeviceToHost, st_));
   }

@@ -61,6 +61,11 @@ struct Problem {
   FilterTables ftab;         // stencil tables of its filter-kernel fields
   std::vector<PreparedField> prep;  // its sweep descriptors (built at the first rebuild)
   bool prepared = false;
+  // resident coarse propagator (coarse.cu): its G phase runs in one CTA with
+  // the field in shared memory; rgf = its coarse sweep descriptors of the
+  // iterations (not placed in the launch classes)
+  bool resident = false;
+  SweepField rgf[3];
   enum { NEW, RUNNING, DONE } state = NEW;
   int k = 0;                 // iterations done
   int converged = 0;
@@ -148,6 +153,14 @@ class MultiEngine {
   std::vector<double> hnorms_;
   std::string err_;
   double ms_ = 0, fine_ms_ = 0;
+  // resident coarse propagators: descriptors per coarse precision (FP32,
+  // FP64), their shared memory, and the side stream they run on beside the
+  // shared coarse launches of the other problems
+  DevBuf rgbuf_[2];
+  int rgn_[2] = {0, 0};
+  size_t rgsmem_[2] = {0, 0};
+  cudaStream_t side_ = nullptr;
+  cudaEvent_t side_ev_[2] = {nullptr, nullptr};
   long long allocs_ = 0;  // problem allocations attempted (fault injection counts them)
 };
 

@@ -94,3 +94,36 @@ def test_batch_converges_per_instance(ccfv):
         assert st["converged"], st
         assert st["update"][-1] < p["tol"]
     assert stats[1]["iterations"] <= stats[0]["iterations"]
+
+
+def test_resident_coarse_propagator_matches_shared_launches(ccfv, monkeypatch):
+    """Small delta-form instances run their whole G phase in one CTA with the
+    coarse field in shared memory (uniform and per-cell velocity fields, FP32
+    and FP64 coarse steps, weak and stiff diffusion: the line's periodic
+    system closed exactly); the results equal those of the shared coarse
+    launches (CCFV_RESIDENT_G=0) within the FP64 parity tolerance."""
+    import torch
+    rng = np.random.default_rng(7)
+    specs = [  # N, velocity, params, K, prec
+        (64, 1, (1.0, -0.5), 1e-3, 1), (96, 2, (2 * np.pi, 0.5, 0.5), 1e-3, 0),
+        (120, 3, (1.5,), 5e-4, 1), (80, 3, (1.5,), 2e-3, 0), (200, 1, (0.4, 0.9), 1e-4, 1),
+        (72, 1, (0.6, -0.4), 5e-2, 1)]
+    def probs():
+        out = []
+        for N, vel, vp, K, prec in specs:
+            g = ccfv.make_grid(N, bc=1, velocity=vel, vel_params=vp, K=K, scheme=1)
+            C0 = dev(periodic_field(N, int(rng.integers(1000))))
+            out.append(dict(grid=g, C0=C0, C_T=torch.empty_like(C0), t0=0.0, t1=0.25,
+                            nt_fine=64, n_slices=8, coarse_ratio=2, tol=0.0, kmax=4,
+                            coarse_precision=prec, form=1,
+                            coarse_theta=ccfv.COARSE_THETA_AUTO))
+        return out
+    a = probs()
+    st_a = ccfv.batch_solve(a)
+    monkeypatch.setenv("CCFV_RESIDENT_G", "0")
+    b = [dict(p, C_T=torch.empty_like(p["C0"])) for p in a]
+    st_b = ccfv.batch_solve(b)
+    for p, q, x, y in zip(a, b, st_a, st_b):
+        assert x["iterations"] == y["iterations"] == 4
+        assert rel_l2(p["C_T"].cpu().numpy(), q["C_T"].cpu().numpy()) < 1e-12
+        np.testing.assert_allclose(x["update"], y["update"], rtol=1e-5, atol=1e-11)
