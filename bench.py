@@ -263,7 +263,7 @@ def measured_peak():
 # captures (dram__bytes_read.sum + dram__bytes_write.sum / cells) of a 4096^2
 # FP64 sweep of each kernel form; the commands and counters are in
 # profiles/sweep_filter_4096_fp64.md and profiles/sweep_filter_exact_4096_fp64.md.
-NCU_BYTES_PER_CELL_SWEEP = {"filter": 13.39, "filter_exact": 13.24}
+NCU_BYTES_PER_CELL_SWEEP = {"filter": 13.32, "filter_exact": 13.27}
 
 
 def ncu_traffic(N, variants=()):
