@@ -422,6 +422,8 @@ int MultiEngine::rebuild() {
     if (!live(P)) continue;
     const ccfv_grid &g = P->g;
     // coarse sequences start in W and end in W2 when 3m is odd
+    he[i] = BElem{P->U, P->F, P->Gold, P->W, ((3 * P->m) & 1) ? P->W2 : P->W, P->NN, P->S,
+                  P->o.form, P->g64 ? 1 : 0, 0, norms_d_.as<double>() + norm_off_[i]};
     // resident coarse propagator: delta form, periodic, the coarse field in
     // one SM's shared memory (CCFV_RESIDENT_G=0 keeps every problem in the
     // shared launches)
