@@ -1322,12 +1322,14 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
   const int cta = (int)blockIdx.x + group_base;
   FiltSmem<T> S = carve_filt<T, EXACT, CELL>(smem_raw, lc_max, H);
   {
-    // a field's CTAs start at cta0 = group0 * cs (cs is uniform over a launch)
-    const int lo = find_field(fields, g0idx, nfields, cta / cs);
+    // a field's CTAs start at cta0 = group0 * cs (cs is uniform over a launch);
+    // only the threads that copy the descriptor search for it
     constexpr int NW8 = (int)(sizeof(SweepField) / 8);
-    if (threadIdx.x < NW8)
+    if (threadIdx.x < NW8) {
+      const int lo = find_field(fields, g0idx, nfields, cta / cs);
       reinterpret_cast<long long *>(S.fd)[threadIdx.x] =
           __ldg(reinterpret_cast<const long long *>(&fields[lo]) + threadIdx.x);
+    }
   }
   __syncthreads();
   if (threadIdx.x == 0 && data_override) {
@@ -1371,50 +1373,60 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
   constexpr bool compat = CELL && COMPAT;
 
   // ---- stage rows p0-H .. p1+H-1 (periodic wrap) ----
-  if (xsweep) {
-    const int ln = lane & (LPG - 1);
-    const long long gl = line0 + ln;
-    T *dcol = S.C + ln;
-    const int row0 = warp * 2 + (lane >> 4);
-    if (gl < M) {
-      const T *gcol = gsrc + gl;
-      for (int row = row0; row < nrows; row += 2 * NW) {
-        int pos = p0 - H + row;
-        if (pos < 0 || pos >= L) {  // halo rows: periodic wrap, or zero (compat)
-          if (compat) {
-            dcol[row * PITCH] = T(0);
-            continue;
-          }
-          pos %= L;
-          if (pos < 0) pos += L;
-        }
-        const T *src = gcol + (long long)pos * s_pos;
-        if (sizeof(T) == 8) cp_async8(dcol + row * PITCH, src); else cp_async4(dcol + row * PITCH, src);
+  // Rows whose position lies inside the line ([rlo, rhi)) take pointer-stepped
+  // copies; only the halo rows outside it wrap (periodic) or are zero (compat).
+  {
+    const int rlo = max(0, H - p0), rhi = min(nrows, H - p0 + L);
+    auto halo_row = [&](T *dcol, const T *lbase, long long step, int row) {
+      int pos = p0 - H + row;
+      if (compat) {
+        dcol[row * PITCH] = T(0);
+        return;
       }
-    } else {
-      for (int row = row0; row < nrows; row += 2 * NW) dcol[row * PITCH] = T(0);
-    }
-  } else {
-    for (int ln = warp; ln < LPG; ln += NW) {
+      pos %= L;
+      if (pos < 0) pos += L;
+      const T *src = lbase + (long long)pos * step;
+      if (sizeof(T) == 8) cp_async8(dcol + row * PITCH, src); else cp_async4(dcol + row * PITCH, src);
+    };
+    if (xsweep) {
+      // a warp copies two rows of 16 consecutive values (128 B for FP64) per step
+      const int ln = lane & (LPG - 1);
       const long long gl = line0 + ln;
       T *dcol = S.C + ln;
+      int row = warp * 2 + (lane >> 4);
       if (gl < M) {
-        const T *lbase = gsrc + gl * s_line;
-        for (int row = lane; row < nrows; row += 32) {
-          int pos = p0 - H + row;
-          if (pos < 0 || pos >= L) {  // halo rows: periodic wrap, or zero (compat)
-            if (compat) {
-              dcol[row * PITCH] = T(0);
-              continue;
-            }
-            pos %= L;
-            if (pos < 0) pos += L;
-          }
-          if (sizeof(T) == 8) cp_async8(dcol + row * PITCH, lbase + pos);
-          else cp_async4(dcol + row * PITCH, lbase + pos);
+        const T *gcol = gsrc + gl;
+        for (; row < rlo; row += 2 * NW) halo_row(dcol, gcol, s_pos, row);
+        const T *src = gcol + (long long)(p0 - H + row) * s_pos;
+        T *dst = dcol + row * PITCH;
+        const long long gstep = 2LL * NW * s_pos;
+#pragma unroll 4
+        for (; row < rhi; row += 2 * NW, src += gstep, dst += 2 * NW * PITCH) {
+          if (sizeof(T) == 8) cp_async8(dst, src); else cp_async4(dst, src);
         }
+        for (; row < nrows; row += 2 * NW) halo_row(dcol, gcol, s_pos, row);
       } else {
-        for (int row = lane; row < nrows; row += 32) dcol[row * PITCH] = T(0);
+        for (; row < nrows; row += 2 * NW) dcol[row * PITCH] = T(0);
+      }
+    } else {
+      // a warp copies 32 consecutive values of one line per step
+      for (int ln = warp; ln < LPG; ln += NW) {
+        const long long gl = line0 + ln;
+        T *dcol = S.C + ln;
+        int row = lane;
+        if (gl < M) {
+          const T *lbase = gsrc + gl * s_line;
+          for (; row < rlo; row += 32) halo_row(dcol, lbase, 1, row);
+          const T *src = lbase + (p0 - H + row);
+          T *dst = dcol + row * PITCH;
+#pragma unroll 4
+          for (; row < rhi; row += 32, src += 32, dst += 32 * PITCH) {
+            if (sizeof(T) == 8) cp_async8(dst, src); else cp_async4(dst, src);
+          }
+          for (; row < nrows; row += 32) halo_row(dcol, lbase, 1, row);
+        } else {
+          for (; row < nrows; row += 32) dcol[row * PITCH] = T(0);
+        }
       }
     }
   }
