@@ -261,9 +261,9 @@ def measured_peak():
 
 # DRAM bytes per cell per sweep of the fine sweep kernel, from one-launch ncu
 # captures (dram__bytes_read.sum + dram__bytes_write.sum / cells) of a 4096^2
-# FP64 sweep of each kernel form; the commands and counters are in
-# profiles/sweep_filter_4096_fp64.md and profiles/sweep_filter_exact_4096_fp64.md.
-NCU_BYTES_PER_CELL_SWEEP = {"filter": 13.32, "filter_exact": 13.27}
+# FP64 sweep of each kernel form (warm-up form: the rotation field at
+# nu = 1e-3; cluster form: nu = 0.02).
+NCU_BYTES_PER_CELL_SWEEP = {"filter": 13.28, "filter_exact": 13.27}
 
 
 def ncu_traffic(N, variants=()):
