@@ -1453,8 +1453,17 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
       pk *= mmu;
     }
   }
-  if (EXACT)
-    for (int e = threadIdx.x; e < FPW; e += NTH) S.pwa[e] = T(powi(-F.sm_fac, e));
+  if (EXACT && warp == 0) {
+    // powers (-mu)^e, e < FPW, by doubling: [s, 2s) = [0, s) * (-mu)^s
+    T xs = T(-F.sm_fac);
+    if (lane == 0) S.pwa[0] = T(1);
+    __syncwarp();
+    for (int s = 1; s < FPW; s <<= 1) {
+      for (int t = lane; t < s && s + t < FPW; t += 32) S.pwa[s + t] = S.pwa[t] * xs;
+      __syncwarp();
+      xs *= xs;
+    }
+  }
   cp_async_wait_all_committed();
   __syncthreads();
   if (compat) {  // extrapolated ghost cells C_{-2}, C_{-1}, C_L, C_{L+1} (T2S4:275-286)
@@ -1792,13 +1801,28 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
       // for the others' before it exits (non-aligned forms: the wait follows
       // the divergent store loops)
       asm volatile("barrier.cluster.arrive;\n" ::: "memory");
+      // x_k += cr h_k + d (-mu)^(p1-k), with cr h_k = A (-mu)^(k-p0+1) -
+      // A (-mu)^(np+1) (-mu)^(p1-k), A = cr / (1 - mu^2): one power series
+      // rising from the segment start, one from its end (running products;
+      // positions from p1 on are not stored)
+      {
+        const T A = cr * inv1m;
+        const T Bc = d - A * S.pwa[np + 1];
+        T t1 = A * S.pwa[c * FCH + 1];  // A (-mu)^(k0-p0+1)
 #pragma unroll
-      for (int i = 0; i < FCH; ++i)
-        if (i < nb) {
-          const T p1k = S.pwa[nb - i];            // (-mu)^(p1-k)
-          const T pk = S.pwa[c * FCH + i + 1];    // (-mu)^(k-p0+1)
-          v[i] += cr * (pk * (T(1) - p1k * p1k) * inv1m) + d * p1k;
+        for (int i = 0; i < FCH; ++i) {
+          v[i] += t1;
+          t1 *= mmu;
         }
+        const int i0 = min(nb, FCH) - 1;  // this lane's last position before p1
+        T t3 = i0 >= 0 ? Bc * S.pwa[nb - i0] : T(0);
+#pragma unroll
+        for (int i = FCH - 1; i >= 0; --i)
+          if (i <= i0) {
+            v[i] += t3;
+            t3 *= mmu;
+          }
+      }
     }
     if (compat && p0 == 0) {
       // non-cyclic system: A = c (1 + mu S^-1)(1 + mu S) + c mu^2 e_0 e_0^T,
