@@ -1345,7 +1345,11 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
   const int q = cta - F.cta0;
   const int rank = q % cs;
   const long long line0 = (long long)(q / cs) * LPG;
-  const int Lc = (L + cs - 1) / cs;
+  // exact form: segments of a whole walk (FLANES * FCH cells) and a shorter
+  // last one when cs is the least count that covers the line (full segments
+  // need no masking, and their forward end is the scan's carry-out)
+  int Lc = (L + cs - 1) / cs;
+  if (EXACT && (cs - 1) * (FLANES * FCH) < L && cs * (FLANES * FCH) >= L) Lc = FLANES * FCH;
   const int p0 = min(L, rank * Lc);
   const int p1 = min(L, p0 + Lc);
   const int np = p1 - p0;
@@ -1668,6 +1672,7 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
         w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6; w6 = w7;
       }
     }
+    T fwd_out;  // exact form, full segment: the forward value at p1 - 1
     {
       // carries: chunk map x -> pw x + e_c, inclusive scan over the line's lanes
       T sa = pw, sb = v[FCH - 1];
@@ -1682,6 +1687,7 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
       }
       T cin = __shfl_up_sync(fm, sb, 1, FLANES);
       if (c == 0) cin = T(0);
+      fwd_out = __shfl_sync(fm, sb, FLANES - 1, FLANES);
       // + cin (-mu)^(i+1), the powers by a running product (no table loads)
 #pragma unroll
       for (int i = 0; i < FCH; ++i) {
@@ -1699,13 +1705,21 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
     T e_fwd = T(0);
     if (EXACT) {
       // forward end of the segment from a zero carry (position p1 - 1)
-      const int cend = (np - 1) / FCH, iend = (np - 1) - cend * FCH;
+      if (np == FLANES * FCH) {
+        e_fwd = fwd_out;
+      } else {
+        const int cend = (np - 1) / FCH, iend = (np - 1) - cend * FCH;
 #pragma unroll
-      for (int i = 0; i < FCH; ++i) e_fwd = (c == cend && i == iend) ? v[i] : e_fwd;
-      e_fwd = __shfl_sync(fm, e_fwd, cend, FLANES);
+        for (int i = 0; i < FCH; ++i) e_fwd = (c == cend && i == iend) ? v[i] : e_fwd;
+        e_fwd = __shfl_sync(fm, e_fwd, cend, FLANES);
+      }
     }
+    // zero from qb on; a backward range that covers every lane's positions
+    // needs none (uniform over the CTA)
+    if ((compat ? min(qb, L) : qb) - (p0 - J) < FLANES * FCH) {
 #pragma unroll
-    for (int i = 0; i < FCH; ++i) v[i] = (i < nb) ? v[i] : T(0);  // zero from qb on
+      for (int i = 0; i < FCH; ++i) v[i] = (i < nb) ? v[i] : T(0);
+    }
 
     // backward: x over [k0, qb), zero start at qb
     {
