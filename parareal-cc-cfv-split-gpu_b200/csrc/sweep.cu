@@ -1108,6 +1108,7 @@ struct FiltSmem {
   T *pwt;    // [32]       (-mu)^(i+1), i = 0 .. FCH-1
   T *pwa;    // exact form: [FPW] (-mu)^e
   T *ex;     // exact form: [2 * LPG] this segment's forward end / backward start per line
+  double *et;  // per-cell form: [FPW] sin^2(pi s) of the tile's edges (swirling field)
   int *n0;   // [LPG]
   SweepField *fd;
   int rows;
@@ -1130,6 +1131,11 @@ __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max
   s.C = p;
   s.rows = filter_tile_rows(lc_max, H);
   s.B = CELL ? p + (size_t)s.rows * PITCH : nullptr;
+  s.et = nullptr;
+  if (CELL) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(s.B + (size_t)s.rows * PITCH);
+    s.et = reinterpret_cast<double *>((a + 7) & ~uintptr_t(7));
+  }
   return s;
 }
 
@@ -1160,10 +1166,9 @@ struct CellEdge {
 };
 
 template <typename T>
-__device__ __forceinline__ CellEdge<T> cell_edge(const SweepField &F, const LineFeet &lf,
-                                                 const T *ccol, int rb, int nrows, int e,
-                                                 unsigned *status) {
-  const double f = lf.foot(F, e);
+__device__ __forceinline__ CellEdge<T> cell_edge_at(const SweepField &F, double f,
+                                                    const T *ccol, int rb, int nrows,
+                                                    unsigned *status) {
   const double u = (f - F.s_min) / F.h;
   const double fk = floor(u);
   CellEdge<T> r;
@@ -1192,6 +1197,13 @@ __device__ __forceinline__ CellEdge<T> cell_edge(const SweepField &F, const Line
                        (T(-8.0) * xi3 + T(6.0) * xi2 + T(18.0) * xi - T(1.0)) * cp1 +
                        (T(2.0) * xi3 - T(3.0) * xi) * cp2);
   return r;
+}
+
+template <typename T>
+__device__ __forceinline__ CellEdge<T> cell_edge(const SweepField &F, const LineFeet &lf,
+                                                 const T *ccol, int rb, int nrows, int e,
+                                                 unsigned *status) {
+  return cell_edge_at<T>(F, lf.foot(F, e), ccol, rb, nrows, status);
 }
 
 // b of the cell between edges l and l+1: remap + (1-theta) K Dt/h (D_r - D_l)
@@ -1508,9 +1520,74 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
       const int mm = (kw - kb + FLANES - 1) / FLANES;
       const int s0 = kb + c * mm, s1 = min(kw, s0 + mm);
       const double tau0 = F.t_min + F.ht * (double)gl;
-      const LineFeet lf(F, tau0, tau0 + F.ht, toff + F.ta_rel, toff + F.tb_rel);
       const T *ccol = S.C + ln;
       const T kbc = T(F.kb);
+      bool swirl_done = false;
+      if constexpr (sizeof(T) == 8 && !compat) {
+        if (F.vel == VEL_SWIRL) {
+          // Swirling field: the corner feet of the tile's LPG + 1 corner
+          // lines at the edges [kb, kw] once each (a corner is shared by the
+          // lines on either side), sin^2(pi s) of an edge shared by all of
+          // them (the LineFeet factorisation: g(tau) h(t) per corner line and
+          // time), into the second tile as [edge row][corner line]; then
+          // each line's edge feet (the mean of its two corners) in place,
+          // and the right-hand side below reads them back per edge.
+          double *cf = S.B;
+          const int ne = kw - kb + 1;
+          if (threadIdx.x <= LPG) {
+            const double sg = F.dir == 0 ? 1.0 : -1.0;
+            const double g =
+                sg * sinpi(2.0 * (F.t_min + F.ht * (double)(line0 + (long long)threadIdx.x)));
+            S.om[threadIdx.x] = g * cospi((toff + F.ta_rel) / F.vp[0]);
+            S.om[LPG + 1 + threadIdx.x] = g * cospi((toff + F.tb_rel) / F.vp[0]);
+          }
+          for (int i = threadIdx.x; i < ne; i += NTH) {
+            const double ss = sinpi(F.s_min + F.h * (kb + i));
+            S.et[i] = ss * ss;
+          }
+          __syncthreads();
+          for (int i = threadIdx.x; i < ne * (LPG + 1); i += NTH) {
+            const int ei = i / (LPG + 1), j = i - ei * (LPG + 1);
+            const double sp = F.s_min + F.h * (kb + ei);
+            const double w = S.om[LPG + 1 + j] * S.et[ei];  // speed at tb
+            const double q = sinpi(sp - F.Dt * w);
+            cf[(kb + ei + rb) * PITCH + j] = sp - 0.5 * F.Dt * (w + S.om[j] * q * q);
+          }
+          __syncthreads();
+          for (int i = threadIdx.x; i < ne; i += NTH) {
+            double *row = cf + (kb + i + rb) * PITCH;
+            double c0 = row[0];
+#pragma unroll
+            for (int j = 0; j < LPG; ++j) {
+              const double c1 = row[j + 1];
+              row[j] = 0.5 * (c0 + c1);
+              c0 = c1;
+            }
+          }
+          __syncthreads();
+          // lane c's last edge is the next lane's first: read before any write
+          const double fend = s0 < s1 ? cf[(s1 + rb) * PITCH + ln] : 0.0;
+          __syncwarp(fm);
+          T *bcol = S.B + ln;
+          if (s0 < s1) {
+            CellEdge<T> el{0, T(0), T(0)};
+            if (s0 < kv) el = cell_edge_at<T>(F, cf[(s0 + rb) * PITCH + ln], ccol, rb, nrows, status);
+            for (int k = s0; k < s1; ++k) {
+              T b = T(0);
+              if (k < kv) {
+                const double f1 = k + 1 < s1 ? cf[(k + 1 + rb) * PITCH + ln] : fend;
+                const CellEdge<T> er = cell_edge_at<T>(F, f1, ccol, rb, nrows, status);
+                b = cell_rhs<T>(el, er, ccol, rb, nrows, kbc, status);
+                el = er;
+              }
+              bcol[(k + rb) * PITCH] = b;
+            }
+          }
+          swirl_done = true;
+        }
+      }
+      if (!swirl_done) {
+      const LineFeet lf(F, tau0, tau0 + F.ht, toff + F.ta_rel, toff + F.tb_rel);
       if (!compat) {
         T *bcol = S.B + ln;
         if (s0 < s1) {
@@ -1625,6 +1702,7 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
             bcol[(k + rb) * PITCH] = b;
           }
         }
+      }
       }
       __syncwarp(fm);
     }
@@ -1911,7 +1989,8 @@ size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact, bool
   size_t el = fp64 ? 8 : 4;
   return FD_BYTES + 64 * sizeof(int) +
          (8 * (size_t)LPG + 32 + (exact ? (size_t)FPW + 2 * LPG : 0) +
-          (cell ? 2 : 1) * (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el;
+          (cell ? 2 : 1) * (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el +
+         (cell ? 8 * (size_t)FPW + 8 : 0);
 }
 
 int filter_segment_max(int J) { return filter_seg_max(J); }
