@@ -262,7 +262,14 @@ int ccfv_sweep_plan(ccfv_ctx *ctx, double dt, int precision, int variant[3], int
     const LaunchGeom G = step_geom(ctx->grid, dir, Dt, dsrc, precision == CCFV_FP64, false);
     if (variant)
       variant[kind] = (ctx->force_general && G.variant != SWEEP_GENERAL_SRC) ? SWEEP_GENERAL : G.variant;
-    if (segment) segment[kind] = G.lc_max;
+    if (segment) {
+      // the cluster form runs whole-walk segments (and a shorter last one)
+      // when its segment count is the least that covers the line
+      const int L = dir == 0 ? ctx->grid.nx : ctx->grid.ny, walk = filter_segment_max(0);
+      const bool whole = exact_filter_variant(G.variant) && (G.cs - 1) * walk < L &&
+                         G.cs * walk >= L;
+      segment[kind] = whole ? walk : G.lc_max;
+    }
   }
   return CCFV_OK;
 }
