@@ -1623,20 +1623,32 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
         if (!F.dsrc) {
           T *bcol = S.B + ln;
           if (uni) {
-            for (int k = s0; k < s1; ++k) {
+            // the lane's run in three ranges: the cells clear of the clamps
+            // and ghost selections [i0, i1) take the stencil with no
+            // per-cell branches, the others the reference's formulas (or 0
+            // outside the line)
+            auto edge_cell = [&](int k) {
               T b = T(0);
               if (k >= ka && k < kz) {
-                if (k >= klo && k <= khi) {
-                  const T *cp = S.C + (k + n0 - 2 + rb) * PITCH + ln;
-#pragma unroll
-                  for (int t = 0; t < 6; ++t) b += (wr[t] + wq[t]) * cp[t * PITCH];
-                } else {
-                  const double fa = lf.foot(F, k), fb = lf.foot(F, k + 1);
-                  b = remap_cell(F, vc, fa, fb) +
-                      kbc * (foot_derivative(F, vc, fb) - foot_derivative(F, vc, fa));
-                }
+                const double fa = lf.foot(F, k), fb = lf.foot(F, k + 1);
+                b = remap_cell(F, vc, fa, fb) +
+                    kbc * (foot_derivative(F, vc, fb) - foot_derivative(F, vc, fa));
               }
               bcol[(k + rb) * PITCH] = b;
+            };
+            const int i0 = max(s0, max(ka, klo)), i1 = max(i0, min(s1, min(kz, khi + 1)));
+            const int ia = min(i0, s1);
+            for (int k = i0; k < i1; ++k) {
+              const T *cp = S.C + (k + n0 - 2 + rb) * PITCH + ln;
+              T b = T(0);
+#pragma unroll
+              for (int t = 0; t < 6; ++t) b += (wr[t] + wq[t]) * cp[t * PITCH];
+              bcol[(k + rb) * PITCH] = b;
+            }
+            for (int k = s0; k < s1; ++k) {  // the rest, skipping [i0, i1)
+              if (k == ia) k = max(ia, i1);
+              if (k >= s1) break;
+              edge_cell(k);
             }
           } else {
             if (ka < kz) {
@@ -1661,16 +1673,22 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
           const int q0 = ra0 + c * m1, q1 = min(ra1, q0 + m1);
           T *rcol = S.B + ln;
           if (uni) {
-            for (int k = q0; k < q1; ++k) {
+            auto edge_remap = [&](int k) {
+              rcol[(k + rb) * PITCH] = remap_cell(F, vc, lf.foot(F, k), lf.foot(F, k + 1));
+            };
+            const int j0 = max(q0, klo), j1 = max(j0, min(q1, khi + 1));
+            const int ja = min(j0, q1);
+            for (int k = j0; k < j1; ++k) {
+              const T *cp = S.C + (k + n0 - 2 + rb) * PITCH + ln;
               T r = T(0);
-              if (k >= klo && k <= khi) {
-                const T *cp = S.C + (k + n0 - 2 + rb) * PITCH + ln;
 #pragma unroll
-                for (int t = 0; t < 6; ++t) r += wr[t] * cp[t * PITCH];
-              } else {
-                r = remap_cell(F, vc, lf.foot(F, k), lf.foot(F, k + 1));
-              }
+              for (int t = 0; t < 6; ++t) r += wr[t] * cp[t * PITCH];
               rcol[(k + rb) * PITCH] = r;
+            }
+            for (int k = q0; k < q1; ++k) {  // the rest, skipping [j0, j1)
+              if (k == ja) k = max(ja, j1);
+              if (k >= q1) break;
+              edge_remap(k);
             }
           } else if (q0 < q1) {
             CompatEdge<T> el = compat_edge<T>(F, lf, vc, vc, q0);
@@ -1685,21 +1703,29 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
           __syncwarp(fm);
           const LineView<T> vr{rcol, rb, nrows, status};
           T *bcol = S.C + ln;
-          for (int k = s0; k < s1; ++k) {
+          auto edge_cell = [&](int k) {
             T b = T(0);
             if (k >= ka && k < kz) {
-              if (uni && k >= klo && k <= khi) {
-                const T *rp = rcol + (k + n0 - 2 + rb) * PITCH;
-                T acc = T(0);
-#pragma unroll
-                for (int t = 0; t < 6; ++t) acc += wq[t] * rp[t * PITCH];
-                b = rcol[(k + rb) * PITCH] + acc;
-              } else {
-                const double fa = lf.foot(F, k), fb = lf.foot(F, k + 1);
-                b = vr(k) + kbc * (foot_derivative(F, vr, fb) - foot_derivative(F, vr, fa));
-              }
+              const double fa = lf.foot(F, k), fb = lf.foot(F, k + 1);
+              b = vr(k) + kbc * (foot_derivative(F, vr, fb) - foot_derivative(F, vr, fa));
             }
             bcol[(k + rb) * PITCH] = b;
+          };
+          // interior cells of a uniform displacement [i0, i1): the stencil
+          // (empty range for other fields: klo > khi)
+          const int i0 = max(s0, max(ka, klo)), i1 = max(i0, min(s1, min(kz, khi + 1)));
+          const int ia = min(i0, s1);
+          for (int k = i0; k < i1; ++k) {
+            const T *rp = rcol + (k + n0 - 2 + rb) * PITCH;
+            T acc = T(0);
+#pragma unroll
+            for (int t = 0; t < 6; ++t) acc += wq[t] * rp[t * PITCH];
+            bcol[(k + rb) * PITCH] = rcol[(k + rb) * PITCH] + acc;
+          }
+          for (int k = s0; k < s1; ++k) {  // the rest, skipping [i0, i1)
+            if (k == ia) k = max(ia, i1);
+            if (k >= s1) break;
+            edge_cell(k);
           }
         }
       }
