@@ -188,11 +188,13 @@ def test_periodic_filter_segments_match_oracle(oracle, ccfv, nx, K):
 
 
 @pytest.mark.parametrize("nx,ny,K", [(96, 96, 0.3), (300, 200, 0.2), (1000, 520, 0.05),
-                                     (2048, 64, 0.02)])
+                                     (2048, 64, 0.02), (544, 40, 0.05), (545, 40, 0.05)])
 def test_periodic_exact_filter_matches_oracle(oracle, ccfv, nx, ny, K):
     """Strong diffusion (diffusion numbers 6 - 14: the recurrence warm-up
     would exceed 64 cells): the filter kernel's cluster form, 1 to 8
-    segments per line, closes the periodic system exactly across them."""
+    segments per line, closes the periodic system exactly across them
+    (whole 272-cell segments and a shorter last one, down to a single cell:
+    544 = 2 x 272, 545 = 2 x 272 + 1)."""
     vp = (0.9, -1.7)
     dt = 0.8 / max(nx, ny) / 1.7
     C0 = periodic_field(nx, 23, ny=ny)
@@ -211,6 +213,7 @@ def test_periodic_exact_filter_matches_oracle(oracle, ccfv, nx, ny, K):
 @pytest.mark.parametrize("nx,ny,K,form", [(64, 64, 1e-3, "cell"), (300, 260, 1e-4, "cell"),
                                           (2048, 40, 1e-3, "cell"), (4096, 24, 1e-4, "cell"),
                                           (96, 96, 0.3, "cell_exact"),
+                                          (545, 40, 0.05, "cell_exact"),
                                           (1000, 520, 0.05, "cell_exact"),
                                           (2048, 64, 0.02, "cell_exact")])
 def test_periodic_cell_filter_matches_oracle(oracle, ccfv, nx, ny, K, form):
