@@ -53,6 +53,9 @@ struct SweepField {
   int cta0;              // filter kernel: first CTA of this field in the launch
                          // (a multiple of the launch's cluster size)
   int halo_f;            // filter kernel: staged halo (cells) of this field
+  int hyb;               // > 0: the line's segments are split between two launches,
+                         // those at least hyb cells from both ends run the stencil
+                         // form, the others the compat form; 0: one launch
   // Batched launches (all zero for single-instance launches):
   int inst;              // instance index into the launch's `nlo` array
   int slice;             // >= 0: fixed slice of this field; -1: the launch's slice

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -529,28 +530,70 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
       plan->groups_per_field[kind] = f.groups;
     }
     plan->geom[kind] = G;
+    // Compat lines, the first two sweeps of a step, out of place: segments at
+    // least a halo from both line ends see no boundary (no clamps or ghosts,
+    // and the non-cyclic correction has decayed within the warm-up), so they
+    // run the stencil form (one tile, four CTAs per SM) in a second launch
+    // and the compat form keeps the segments at the ends.
+    plan->hyb[kind] = false;
+    static const bool split_on = [] {
+      const char *e = std::getenv("CCFV_COMPAT_SPLIT");
+      return !(e && e[0] == '0');
+    }();
+    const bool uniform = g.velocity == CCFV_VEL_REF_ROT4 || g.velocity == CCFV_VEL_CONST ||
+                         g.velocity == CCFV_VEL_ROTATION;
+    int Jc = 0;
+    if (split_on && plan_pp && uniform && g.bc == CCFV_BC_COMPAT && !g.source && dsrc == 0 &&
+        G.variant == SWEEP_CELL_COMPAT && G.cs >= 3 &&
+        filter_params(g, dir, Dt, fp64, nullptr, nullptr, &Jc, theta) && Jc > 0) {
+      const int L = dir == 0 ? g.nx : g.ny;
+      LaunchGeom G2 = G;
+      G2.variant = SWEEP_FILTER;
+      G2.halo = Jc + shift_cells(g, dir, Dt) + 6;
+      if ((L + G.cs - 1) / G.cs >= G2.halo &&
+          sweep_filter_smem_bytes(G2.lc_max, G2.halo, fp64, false, false) <= 227 * 1024) {
+        plan->hyb[kind] = true;
+        plan->geom2[kind] = G2;
+        for (int i = 0; i < nf; ++i) h[(size_t)kind * nf + i].hyb = G2.halo;
+      }
+    }
   }
+  std::vector<SweepField> h2(h);  // the stencil launches' descriptors
+  for (int kind = 0; kind < 3; ++kind)
+    if (plan->hyb[kind])
+      for (int i = 0; i < nf; ++i) h2[(size_t)kind * nf + i].halo_f = plan->geom2[kind].halo;
   plan->nf = nf;
   plan->pp = nf > 0 && fields[0].B != nullptr;
   // filter sub-steps: one per-line stencil table per kind, shared by the
   // plan's fields (same grid and sub-step; the velocity fields of the filter
   // kernel do not depend on time)
   int lines[3] = {0, 0, 0};
+  bool any_hyb = false;
   for (int kind = 0; kind < 3 && nf > 0; ++kind) {
-    if (!stencil_filter_variant(plan->geom[kind].variant)) continue;
+    if (!stencil_filter_variant(plan->geom[kind].variant) && !plan->hyb[kind]) continue;
+    any_hyb = any_hyb || plan->hyb[kind];
     lines[kind] = h[(size_t)kind * nf].groups * LPG;
     CK(plan->wt[kind].alloc((fp64 ? 8 : 4) * 8 * (size_t)lines[kind]));
     CK(plan->nt[kind].alloc(sizeof(int) * (size_t)lines[kind]));
     for (int i = 0; i < nf; ++i) {
-      h[(size_t)kind * nf + i].wt = plan->wt[kind].p;
-      h[(size_t)kind * nf + i].nt = plan->nt[kind].as<int>();
+      for (std::vector<SweepField> *hv : {&h, &h2}) {
+        (*hv)[(size_t)kind * nf + i].wt = plan->wt[kind].p;
+        (*hv)[(size_t)kind * nf + i].nt = plan->nt[kind].as<int>();
+      }
     }
   }
   CK(plan->fields.alloc(sizeof(SweepField) * h.size()));
   CK(cudaMemcpy(plan->fields.p, h.data(), sizeof(SweepField) * h.size(), cudaMemcpyHostToDevice));
+  if (any_hyb) {
+    CK(plan->fields2.alloc(sizeof(SweepField) * h2.size()));
+    CK(cudaMemcpy(plan->fields2.p, h2.data(), sizeof(SweepField) * h2.size(),
+                  cudaMemcpyHostToDevice));
+  }
   for (int kind = 0; kind < 3; ++kind)
     if (lines[kind])
-      CK(launch_filter_weights(fp64, plan->fields.as<SweepField>() + (size_t)kind * nf,
+      CK(launch_filter_weights(fp64,
+                               (plan->hyb[kind] ? plan->fields2 : plan->fields).as<SweepField>() +
+                                   (size_t)kind * nf,
                                plan->wt[kind].p, plan->nt[kind].as<int>(), lines[kind], 0));
   CK(cudaStreamSynchronize(0));
   return CCFV_OK;
@@ -572,6 +615,17 @@ int run_step_plan(ccfv_ctx *ctx, const StepPlan &plan, bool fp64, int first, int
                                    G.lc_max, G.halo, toff, data_override, status, st, jstep,
                                    !plan.pp);
     CK(e);
+    if (plan.hyb[kind]) {  // the interior segments of compat lines: stencil form
+      const LaunchGeom &G2 = plan.geom2[kind];
+      const SweepField *f2 = plan.fields2.as<SweepField>() + (size_t)kind * plan.nf;
+      e = fp64 ? launch_sweep<double>(G2.variant, f2, plan.nf, first * gpf, count * gpf, G2.cs,
+                                      G2.lc_max, G2.halo, toff, data_override, status, st, jstep,
+                                      !plan.pp)
+               : launch_sweep<float>(G2.variant, f2, plan.nf, first * gpf, count * gpf, G2.cs,
+                                     G2.lc_max, G2.halo, toff, data_override, status, st, jstep,
+                                     !plan.pp);
+      CK(e);
+    }
   }
   return CCFV_OK;
 }

@@ -51,6 +51,11 @@ struct StepPlan {
   LaunchGeom geom[3];
   bool pp = false;        // out-of-place sequence (SweepField::pp)
   DevBuf wt[3], nt[3];    // filter kernel: per-line stencil tables per sub-step kind
+  // compat lines split between two launches (SweepField::hyb): the second
+  // launch's descriptors (stencil form) and geometry per sub-step kind
+  DevBuf fields2;         // SweepField[3][nf]
+  LaunchGeom geom2[3];
+  bool hyb[3] = {false, false, false};
 };
 
 // One field of a plan: swept in place on A (B == nullptr), or an out-of-place

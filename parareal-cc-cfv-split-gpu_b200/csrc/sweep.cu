@@ -1373,6 +1373,12 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
   const int p1 = min(L, p0 + Lc);
   const int np = p1 - p0;
   const int nrows = np + 2 * H;
+  // compat lines split between two launches (SweepField::hyb): each launch
+  // keeps its own segments (uniform over the CTA, before any barrier)
+  if (!EXACT && F.hyb > 0 && !clustered) {
+    const bool interior = p0 >= F.hyb && p1 + F.hyb <= L;
+    if (CELL ? interior : !interior) return;
+  }
   const int J = EXACT ? 0 : F.jf;
   const T mu = T(F.sm_fac), ic = T(F.sm_inv_den);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
