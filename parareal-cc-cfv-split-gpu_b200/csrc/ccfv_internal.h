@@ -125,12 +125,15 @@ constexpr size_t FD_BYTES = (sizeof(SweepField) + 63) & ~size_t(63);
 // per-cell right-hand side (feet that differ from edge to edge);
 // SWEEP_CELL_COMPAT: the per-cell form with the reference's boundaries
 // (non-cyclic system).
+// SWEEP_FILTER_WIDE: the stencil form with the 13-tap right-hand side of the
+// reference scheme's third sweep (interior segments of compat lines).
 enum { SWEEP_GENERAL = 0, SWEEP_FAST = 1, SWEEP_FILTER = 2, SWEEP_GENERAL_SRC = 3,
-       SWEEP_FILTER_EXACT = 4, SWEEP_CELL = 5, SWEEP_CELL_EXACT = 6, SWEEP_CELL_COMPAT = 7 };
+       SWEEP_FILTER_EXACT = 4, SWEEP_CELL = 5, SWEEP_CELL_EXACT = 6, SWEEP_CELL_COMPAT = 7,
+       SWEEP_FILTER_WIDE = 8 };
 // Variants run by the filter kernel (factored solve).
 inline bool filter_variant(int v) {
   return v == SWEEP_FILTER || v == SWEEP_FILTER_EXACT || v == SWEEP_CELL ||
-         v == SWEEP_CELL_EXACT || v == SWEEP_CELL_COMPAT;
+         v == SWEEP_CELL_EXACT || v == SWEEP_CELL_COMPAT || v == SWEEP_FILTER_WIDE;
 }
 // Warm-up (segmented) forms: lines longer than MAX_CLUSTER segments are
 // allowed out of place.
@@ -151,7 +154,7 @@ constexpr int FILTER_JMAX = 64;  // longest recurrence warm-up of the filter ker
 size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source = false);
 size_t sweep_fast_smem_bytes(int lc_max, int halo, bool fp64);
 size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact = false,
-                               bool cell = false);
+                               bool cell = false, bool wide = false);
 // Longest segment (cells per CTA along a line) of the filter kernel for a
 // recurrence warm-up of J cells.
 int filter_segment_max(int J);
@@ -159,7 +162,7 @@ int filter_segment_max(int J);
 // (device descriptor): wt = T[lines][8], nt = int[lines], lines = groups*LPG
 // (lines past M get zeros).
 cudaError_t launch_filter_weights(bool fp64, const SweepField *d_field, void *wt, int *nt,
-                                  int lines, cudaStream_t stream);
+                                  int lines, cudaStream_t stream, bool wide = false);
 
 // Launches one fused sweep over all fields of `d_fields` (device array,
 // sorted by group0; tiles group_base .. group_base+groups_total-1).  All fields share the cluster size `cs`, their

@@ -530,12 +530,15 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
       plan->groups_per_field[kind] = f.groups;
     }
     plan->geom[kind] = G;
-    // Compat lines, the first two sweeps of a step, out of place: segments at
-    // least a halo from both line ends see no boundary (no clamps or ghosts,
-    // and the non-cyclic correction has decayed within the warm-up), so they
-    // run the stencil form (one tile, four CTAs per SM) in a second launch
-    // and the compat form keeps the segments at the ends.
+    // Compat lines, out of place: segments at least a halo from both line
+    // ends see no boundary (no clamps or ghosts, and the non-cyclic
+    // correction has decayed within the warm-up), so they run the stencil
+    // form (one tile) in a second launch and the compat form keeps the
+    // segments at the ends.  The reference scheme's third sweep, which
+    // differentiates the remapped field, takes the 13-tap stencil form
+    // (displacements of at most two cells).
     plan->hyb[kind] = false;
+    plan->wide[kind] = false;
     static const bool split_on = [] {
       const char *e = std::getenv("CCFV_COMPAT_SPLIT");
       return !(e && e[0] == '0');
@@ -543,16 +546,19 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
     const bool uniform = g.velocity == CCFV_VEL_REF_ROT4 || g.velocity == CCFV_VEL_CONST ||
                          g.velocity == CCFV_VEL_ROTATION;
     int Jc = 0;
-    if (split_on && plan_pp && uniform && g.bc == CCFV_BC_COMPAT && !g.source && dsrc == 0 &&
-        G.variant == SWEEP_CELL_COMPAT && G.cs >= 3 &&
+    const int shc = shift_cells(g, dir, Dt);
+    if (split_on && plan_pp && uniform && g.bc == CCFV_BC_COMPAT && !g.source &&
+        G.variant == SWEEP_CELL_COMPAT && G.cs >= 3 && (dsrc == 0 || shc <= 2) &&
         filter_params(g, dir, Dt, fp64, nullptr, nullptr, &Jc, theta) && Jc > 0) {
       const int L = dir == 0 ? g.nx : g.ny;
+      const bool wide = dsrc != 0;
       LaunchGeom G2 = G;
-      G2.variant = SWEEP_FILTER;
-      G2.halo = Jc + shift_cells(g, dir, Dt) + 6;
+      G2.variant = wide ? SWEEP_FILTER_WIDE : SWEEP_FILTER;
+      G2.halo = wide ? Jc + 2 * shc + 12 : Jc + shc + 6;
       if ((L + G.cs - 1) / G.cs >= G2.halo &&
-          sweep_filter_smem_bytes(G2.lc_max, G2.halo, fp64, false, false) <= 227 * 1024) {
+          sweep_filter_smem_bytes(G2.lc_max, G2.halo, fp64, false, false, wide) <= 227 * 1024) {
         plan->hyb[kind] = true;
+        plan->wide[kind] = wide;
         plan->geom2[kind] = G2;
         for (int i = 0; i < nf; ++i) h[(size_t)kind * nf + i].hyb = G2.halo;
       }
@@ -573,7 +579,7 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
     if (!stencil_filter_variant(plan->geom[kind].variant) && !plan->hyb[kind]) continue;
     any_hyb = any_hyb || plan->hyb[kind];
     lines[kind] = h[(size_t)kind * nf].groups * LPG;
-    CK(plan->wt[kind].alloc((fp64 ? 8 : 4) * 8 * (size_t)lines[kind]));
+    CK(plan->wt[kind].alloc((fp64 ? 8 : 4) * (plan->wide[kind] ? 16 : 8) * (size_t)lines[kind]));
     CK(plan->nt[kind].alloc(sizeof(int) * (size_t)lines[kind]));
     for (int i = 0; i < nf; ++i) {
       for (std::vector<SweepField> *hv : {&h, &h2}) {
@@ -594,7 +600,8 @@ int build_step_plan(ccfv_ctx *ctx, StepPlan *plan, double dt, bool fp64,
       CK(launch_filter_weights(fp64,
                                (plan->hyb[kind] ? plan->fields2 : plan->fields).as<SweepField>() +
                                    (size_t)kind * nf,
-                               plan->wt[kind].p, plan->nt[kind].as<int>(), lines[kind], 0));
+                               plan->wt[kind].p, plan->nt[kind].as<int>(), lines[kind], 0,
+                               plan->wide[kind]));
   CK(cudaStreamSynchronize(0));
   return CCFV_OK;
 }

@@ -56,6 +56,7 @@ struct StepPlan {
   DevBuf fields2;         // SweepField[3][nf]
   LaunchGeom geom2[3];
   bool hyb[3] = {false, false, false};
+  bool wide[3] = {false, false, false};  // the stencil launch is the 13-tap form
 };
 
 // One field of a plan: swept in place on A (B == nullptr), or an out-of-place

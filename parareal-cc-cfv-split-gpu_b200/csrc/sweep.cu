@@ -1100,6 +1100,10 @@ __host__ __device__ inline int filter_tile_rows(int lc_max, int H) {
 // Exact (cluster) form: powers (-mu)^e for e = 0 .. FPW - 1 (a segment of at
 // most FLANES * FCH cells needs exponents up to FLANES * FCH).
 constexpr int FPW = FLANES * FCH + 8;
+// Wide stencil form (the reference scheme's third sweep, whose right-hand
+// side differentiates the remapped field): 13 taps, a table row of 16.
+constexpr int WIDE_TAPS = 13;
+constexpr int WIDE_TAPS_PAD = 16;
 
 template <typename T>
 struct FiltSmem {
@@ -1115,13 +1119,13 @@ struct FiltSmem {
   int rows;
 };
 
-template <typename T, bool EXACT, bool CELL>
+template <typename T, bool EXACT, bool CELL, bool WIDE>
 __device__ __forceinline__ FiltSmem<T> carve_filt(unsigned char *raw, int lc_max, int H) {
   FiltSmem<T> s;
   s.fd = reinterpret_cast<SweepField *>(raw);
   s.n0 = reinterpret_cast<int *>(raw + FD_BYTES);
   T *p = reinterpret_cast<T *>(raw + FD_BYTES + 64 * sizeof(int));
-  s.om = p; p += 8 * LPG;
+  s.om = p; p += (WIDE ? WIDE_TAPS_PAD : 8) * LPG;
   s.pwt = p; p += 32;
   s.pwa = nullptr;
   s.ex = nullptr;
@@ -1278,13 +1282,49 @@ __device__ __forceinline__ T compat_remap(const SweepField &F, const CompatEdge<
   return remap_cell(F, vc, l.f, r.f);
 }
 
-// The per-line stencil table of one field (one thread per line).
+// The per-line stencil table of one field (one thread per line).  Wide
+// (the reference scheme's third sweep, uniform displacement): b_k = R_k +
+// sum_t wq_t R_{k+n0-2+t} with R_j = sum_s wr_s C_{j+n0-2+s} (the compat
+// form's interior formulas) composes into 11 taps from C_{k+2n0-4}, valid for
+// n0 in [-3, 2]; with the mass matrix 13 taps from C_{k+2n0-5}, stored with
+// the shift 2n0-2 so that the kernel's first tap row is k + shift - 3.
 template <typename T>
 __global__ void filter_weights_kernel(const SweepField *__restrict__ f, T *__restrict__ wt,
-                                      int *__restrict__ nt, int lines) {
+                                      int *__restrict__ nt, int lines, int wide) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= lines) return;
   const SweepField F = *f;
+  if (wide) {
+    double om[WIDE_TAPS_PAD];
+    for (int m = 0; m < WIDE_TAPS_PAD; ++m) om[m] = 0.0;
+    int shift = 0;
+    if (l < F.M) {
+      const double tau0 = F.t_min + F.ht * (double)l;
+      const double f0 = edge_foot(F, 0, tau0, tau0 + F.ht, F.ta_rel, F.tb_rel);
+      double wr[6], wq[6];
+      int n0 = 0;
+      uniform_weights<double>(F, f0, wr, wq, &n0);
+      double bt[11];
+      for (int j = 0; j < 11; ++j) bt[j] = 0.0;
+      for (int sidx = 0; sidx < 6; ++sidx) {
+        const int j = sidx - n0 + 2;
+        if (j >= 0 && j < 11) bt[j] += wr[sidx];
+      }
+      for (int t = 0; t < 6; ++t)
+        for (int sidx = 0; sidx < 6; ++sidx) bt[t + sidx] += wq[t] * wr[sidx];
+      const double icw = F.sm_inv_den / 12.0;
+      for (int m = 0; m < WIDE_TAPS; ++m) {
+        const double bm = m < 11 ? bt[m] : 0.0;                       // b_{k-1}
+        const double bc = (m >= 1 && m < 12) ? bt[m - 1] : 0.0;       // b_k
+        const double bp = m >= 2 ? bt[m - 2] : 0.0;                   // b_{k+1}
+        om[m] = icw * (bm + 10.0 * bc + bp);
+      }
+      shift = 2 * n0 - 2;
+    }
+    for (int m = 0; m < WIDE_TAPS_PAD; ++m) wt[(size_t)l * WIDE_TAPS_PAD + m] = T(om[m]);
+    nt[l] = shift;
+    return;
+  }
   if (l < F.M) {
     T om[8];
     int n0 = 0;
@@ -1321,8 +1361,8 @@ __global__ void filter_weights_kernel(const SweepField *__restrict__ f, T *__res
 // and the per-edge arithmetic: two CTAs per SM.
 // COMPAT (per-cell form only): the reference's boundaries, a separate
 // instantiation so that the periodic per-cell form carries none of their code.
-template <typename T, bool EXACT, bool CELL, bool COMPAT>
-__global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
+template <typename T, bool EXACT, bool CELL, bool COMPAT, bool WIDE = false>
+__global__ void __launch_bounds__(NTH, (CELL || WIDE) ? 2 : 4)
     sweep_filter_kernel(const SweepField *__restrict__ fields, int nfields, int group_base,
                         double toff, void *data_override, int lc_max, int H, unsigned *status,
                         int jstep, int nslice, const int *nlo, int cs, int clustered,
@@ -1339,7 +1379,7 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
   // of different segment lengths share one launch (lc_max and H size the
   // shared memory only)
   const int cta = (int)blockIdx.x + group_base;
-  FiltSmem<T> S = carve_filt<T, EXACT, CELL>(smem_raw, lc_max, H);
+  FiltSmem<T> S = carve_filt<T, EXACT, CELL, WIDE>(smem_raw, lc_max, H);
   {
     // a field's CTAs start at cta0 = group0 * cs (cs is uniform over a launch);
     // only the threads that copy the descriptor search for it
@@ -1461,6 +1501,11 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
   }
   if (CELL) {
     // per-cell form: no per-line stencil (b is computed per cell below)
+  } else if (WIDE) {  // wide stencil rows (WIDE_TAPS_PAD per line) and shifts
+    static_assert(WIDE_TAPS_PAD * LPG == NTH, "one table entry per thread");
+    const T *src = reinterpret_cast<const T *>(F.wt) + line0 * WIDE_TAPS_PAD + threadIdx.x;
+    if (sizeof(T) == 8) cp_async8(S.om + threadIdx.x, src); else cp_async4(S.om + threadIdx.x, src);
+    if (threadIdx.x < LPG) cp_async4(S.n0 + threadIdx.x, F.nt + line0 + threadIdx.x);
   } else if (F.wt) {  // per-line stencil from the plan's table, copied with the cells
     if (threadIdx.x < 8 * LPG) {
       const T *src = reinterpret_cast<const T *>(F.wt) + line0 * 8 + threadIdx.x;
@@ -1471,7 +1516,7 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
     }
   }
   cp_async_commit();
-  if (!CELL && !F.wt && threadIdx.x < LPG) {
+  if (!CELL && !WIDE && !F.wt && threadIdx.x < LPG) {
     filter_line_stencil<T>(F, line0 + threadIdx.x, toff, S.om + 8 * threadIdx.x,
                            S.n0 + threadIdx.x);
   } else if (threadIdx.x == 9 * LPG) {
@@ -1752,7 +1797,7 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
     const int qb = p1 + J;
     const int k0 = p0 - J + c * FCH;
     const int r0 = CELL ? k0 - 1 + rb : k0 + S.n0[ln] - 3 + rb;  // row of the first tap
-    const bool ok = r0 >= 0 && r0 + FCH + (CELL ? 2 : 7) <= S.rows;
+    const bool ok = r0 >= 0 && r0 + FCH + (CELL ? 2 : WIDE ? WIDE_TAPS - 1 : 7) <= S.rows;
     if (!ok) atomicOr(status, STATUS_HALO);
     T v[FCH];
     if (CELL) {
@@ -1771,6 +1816,27 @@ __global__ void __launch_bounds__(NTH, CELL ? 2 : 4)
         v[i] = w;
         b0 = b1;
         b1 = b2;
+      }
+    } else if constexpr (WIDE) {
+      // w_k = sum of WIDE_TAPS taps of the cells from row r0 - mu w_{k-1}
+      const T *omp = S.om + WIDE_TAPS_PAD * ln;
+      T o[WIDE_TAPS], wv[WIDE_TAPS];
+#pragma unroll
+      for (int m = 0; m < WIDE_TAPS; ++m) o[m] = omp[m];
+      const T *cp = S.C + (ok ? r0 : 0) * PITCH + ln;
+#pragma unroll
+      for (int m = 0; m < WIDE_TAPS - 1; ++m) wv[m] = cp[m * PITCH];
+      T w = T(0);
+#pragma unroll
+      for (int i = 0; i < FCH; ++i) {
+        wv[WIDE_TAPS - 1] = cp[(WIDE_TAPS - 1 + i) * PITCH];
+        T mb = o[0] * wv[0];
+#pragma unroll
+        for (int m = 1; m < WIDE_TAPS; ++m) mb += o[m] * wv[m];
+        w = mb + mmu * w;
+        v[i] = w;
+#pragma unroll
+        for (int m = 0; m < WIDE_TAPS - 1; ++m) wv[m] = wv[m + 1];
       }
     } else {
       const T *omp = S.om + 8 * ln;
@@ -2024,10 +2090,11 @@ size_t sweep_smem_bytes(int lc_max, int halo, bool fp64, bool source) {
   return FD_BYTES + n * el;
 }
 
-size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact, bool cell) {
+size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact, bool cell,
+                               bool wide) {
   size_t el = fp64 ? 8 : 4;
   return FD_BYTES + 64 * sizeof(int) +
-         (8 * (size_t)LPG + 32 + (exact ? (size_t)FPW + 2 * LPG : 0) +
+         ((wide ? WIDE_TAPS_PAD : 8) * (size_t)LPG + 32 + (exact ? (size_t)FPW + 2 * LPG : 0) +
           (cell ? 2 : 1) * (size_t)filter_tile_rows(lc_max, halo) * PITCH) * el +
          (cell ? 8 * (size_t)FPW + 8 : 0);
 }
@@ -2035,15 +2102,15 @@ size_t sweep_filter_smem_bytes(int lc_max, int halo, bool fp64, bool exact, bool
 int filter_segment_max(int J) { return filter_seg_max(J); }
 
 cudaError_t launch_filter_weights(bool fp64, const SweepField *d_field, void *wt, int *nt,
-                                  int lines, cudaStream_t stream) {
+                                  int lines, cudaStream_t stream, bool wide) {
   const int bt = 128, grid = (lines + bt - 1) / bt;
   count_launch();
   if (fp64)
     filter_weights_kernel<double><<<grid, bt, 0, stream>>>(d_field, static_cast<double *>(wt), nt,
-                                                           lines);
+                                                           lines, wide ? 1 : 0);
   else
     filter_weights_kernel<float><<<grid, bt, 0, stream>>>(d_field, static_cast<float *>(wt), nt,
-                                                          lines);
+                                                          lines, wide ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -2066,6 +2133,7 @@ static FilterKernelT<T> filter_kernel_for(int variant) {
     case SWEEP_CELL: return sweep_filter_kernel<T, false, true, false>;
     case SWEEP_CELL_EXACT: return sweep_filter_kernel<T, true, true, false>;
     case SWEEP_CELL_COMPAT: return sweep_filter_kernel<T, false, true, true>;
+    case SWEEP_FILTER_WIDE: return sweep_filter_kernel<T, false, false, false, true>;
     default: return sweep_filter_kernel<T, false, false, false>;
   }
 }
@@ -2081,7 +2149,8 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
   const bool exact = exact_filter_variant(variant);
   const bool filt = filter_variant(variant);
   const bool src = (variant == SWEEP_GENERAL_SRC);
-  const size_t smem = filt ? sweep_filter_smem_bytes(lc_max, halo, sizeof(T) == 8, exact, cell)
+  const size_t smem = filt ? sweep_filter_smem_bytes(lc_max, halo, sizeof(T) == 8, exact, cell,
+                                                     variant == SWEEP_FILTER_WIDE)
                       : fast ? sweep_fast_smem_bytes(lc_max, halo, sizeof(T) == 8)
                              : sweep_smem_bytes(lc_max, halo, sizeof(T) == 8, src);
   {
@@ -2104,7 +2173,8 @@ static cudaError_t launch_impl(int variant, const SweepField *d_fields, int nfie
               (const void *)filter_kernel_for<T>(SWEEP_FILTER_EXACT),
               (const void *)filter_kernel_for<T>(SWEEP_CELL),
               (const void *)filter_kernel_for<T>(SWEEP_CELL_EXACT),
-              (const void *)filter_kernel_for<T>(SWEEP_CELL_COMPAT)}) {
+              (const void *)filter_kernel_for<T>(SWEEP_CELL_COMPAT),
+              (const void *)filter_kernel_for<T>(SWEEP_FILTER_WIDE)}) {
           err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      227 * 1024);
           if (err != cudaSuccess) return err;
